@@ -1,0 +1,177 @@
+/* usap-b200: C ABI of the B200 stochastic block partitioning path.
+ *
+ * Drop-in boundary for uSAP's entry point (chih-chun-chang/uSAP):
+ *   directed edge list in -> block assignment (+ evaluation scores) out.
+ * The reference exposes it as a header-only C++ class,
+ *   sgp::Graph_P<W>(FileName, num_threads)   include/graph_parallel.hpp:61-78
+ *   public parameters                         include/graph_parallel.hpp:40-52
+ *   void partition()                          include/graph_parallel.hpp:59, :322-512
+ *   const std::vector<size_t>& get_partitions()  include/graph_parallel.hpp:58
+ *   num_nodes(), num_edges()                  include/graph_parallel.hpp:56-57
+ * and scores through bf::evaluate(truth, given)   include/evaluate.hpp:18-266.
+ * include/usap/graph_p.hpp wraps this ABI in a class of that shape.
+ *
+ * Conventions: plain pointers and sizes, caller-owned buffers, int32 ids.
+ * Every call returns a usap_status (0 = ok, negative = error) and never
+ * exits the process (the reference calls std::exit on bad input files,
+ * graph_parallel.hpp:254-257); usap_last_error() gives a message for the
+ * calling thread.  One usap_ctx serves one caller at a time; different
+ * contexts may be used from different threads.
+ */
+#ifndef USAP_H
+#define USAP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t usap_status;
+#define USAP_OK 0
+#define USAP_ERR_INVALID (-1)   /* bad argument or graph */
+#define USAP_ERR_CUDA (-2)      /* CUDA runtime error */
+#define USAP_ERR_OOM (-3)       /* device or host allocation failed */
+#define USAP_ERR_LIMIT (-4)     /* input beyond a documented size limit */
+#define USAP_ERR_NO_DEVICE (-5) /* no usable sm_100 device */
+#define USAP_ERR_INTERNAL (-6)
+#define USAP_ERR_STATE (-7)     /* call out of order (e.g. no graph loaded) */
+
+/* A directed graph.  Edges are kept in the given order: a vertex's out- and
+ * in-neighbour lists are in edge order, as the reference builds them from
+ * the file (graph_parallel.hpp:285-290).  n = 0 takes the number of
+ * vertices from the largest source id, as the reference does
+ * (graph_parallel.hpp:276).  weight = NULL means unit weights (weights must
+ * be positive).  Limits: n < 2^31, total weight < 2^24. */
+typedef struct usap_graph {
+  int32_t n;
+  int64_t e;
+  const int32_t* src;
+  const int32_t* dst;
+  const int32_t* weight;
+  int32_t one_based;  /* 1: ids are 1-based like the reference's TSV files */
+} usap_graph;
+
+/* Parameters: the first group mirrors Graph_P's public members with the
+ * reference defaults (graph_parallel.hpp:40-52); `beta`, `verbose` and
+ * `t_block_num` are accepted and, as in the reference, not used. */
+typedef struct usap_params {
+  int32_t beta;                             /* 3 */
+  int32_t block_size;                       /* 1024 (the reference's dense/sparse switch) */
+  int32_t num_agg_proposals_per_block;      /* 10 */
+  float num_block_reduction_rate;           /* 0.5 */
+  int32_t max_num_nodal_itr;                /* 100 */
+  int32_t num_batch_nodal_update;           /* 4 */
+  double delta_entropy_threshold1;          /* 5e-4 */
+  double delta_entropy_threshold2;          /* 1e-4 */
+  int32_t delta_entropy_moving_avg_window;  /* 3 */
+  int32_t verbose;                          /* 0 */
+  int32_t dfs_depth;                        /* 20 */
+  int32_t t_block_num;                      /* 20 */
+  /* B200 build */
+  uint64_t seed;       /* Philox key of every proposal draw */
+  int32_t init_mode;   /* 0: SCC/DFS initial blocks (reference); 1: one block per vertex */
+  int32_t dense_max;   /* dense int32 tile for B <= dense_max (default 4096), sorted views above */
+  int32_t device;      /* CUDA device for usap_partition (ignored by contexts) */
+  int32_t stats;       /* 1: per-kernel CUDA-event timings and algorithmic byte counts */
+  int32_t reserved[6];
+} usap_params;
+
+typedef struct usap_result {
+  int32_t B;               /* number of blocks of the returned partition */
+  int32_t stages;          /* merge + nodal phases run */
+  double S;                /* description length of the result */
+  int64_t S_q;             /* the same in Q32 fixed point (exact) */
+  int64_t sweeps, batches;
+  int64_t nodal_proposals, nodal_moves;
+  int64_t near_threshold;  /* nodal proposals with |dS| <= 1e-9 */
+  int64_t merge_shortfall; /* merges the merge order could not supply */
+  int64_t edge_visits;     /* sum over proposing vertices of in+out degree */
+  double ms_total, ms_init, ms_merge, ms_nodal, ms_h2d, ms_d2h;
+  double ms_nodal_kernel;  /* stats: summed time of the nodal proposal kernel */
+  int64_t nodal_kernel_launches;
+  double nodal_kernel_bytes;  /* stats: algorithmic bytes of those launches */
+} usap_result;
+
+typedef struct usap_scores {
+  double accuracy;               /* optimal block matching (Hungarian); NaN if too many blocks */
+  double rand_index, adjusted_rand_index, adjusted_rand_index_exact;
+  double pairwise_recall, pairwise_precision;
+  double h_truth, h_given, h_truth_given, h_given_truth, mi;
+  double nmi, nmi_sqrt;          /* 2 MI / (H_t + H_g), MI / sqrt(H_t H_g) */
+  double missed_info, erroneous_info;
+  int64_t n, b_truth, b_given;
+} usap_scores;
+
+/* Trace events for replay harnesses: one after each merge application
+ * (kind 1), each nodal batch (kind 2) and each finished stage (kind 3),
+ * with checksums of the partition, of M's non-zeros and of the degrees. */
+typedef struct usap_trace_event {
+  int32_t kind, stage, itr, batch_beg, B;
+  int64_t S_q;
+  int32_t S_ninf;
+  int64_t cum_q;
+  int32_t cum_ninf;
+  int64_t moves;
+  uint64_t h_part, h_M, h_deg;
+} usap_trace_event;
+typedef void (*usap_trace_fn)(void* user, const usap_trace_event* ev);
+
+typedef struct usap_ctx usap_ctx;
+
+/* --- basics ------------------------------------------------------------- */
+const char* usap_version(void);
+const char* usap_last_error(void);
+void usap_params_default(usap_params* p);
+
+/* One-shot solve: Graph_P(file) + partition() + get_partitions()
+ * (graph_parallel.hpp:61-78, :322-512, :58).  out_assign[n] receives the
+ * 0-based block of every vertex. */
+usap_status usap_partition(const usap_graph* g, const usap_params* p, int32_t* out_assign,
+                           usap_result* out);
+
+/* Scores of bf::evaluate (evaluate.hpp:18-266) plus NMI, returned instead of
+ * printed.  Labels are 0-based; truth label -1 marks unknown vertices. */
+usap_status usap_evaluate(const int32_t* truth, const int32_t* given, int64_t n,
+                          usap_scores* out);
+
+/* --- resident contexts: the graph stays in HBM across solves ------------- */
+usap_status usap_ctx_create(int32_t device, usap_ctx** out);
+usap_status usap_ctx_destroy(usap_ctx* ctx);
+/* Graph_P constructor / load_graph_from_tsv (graph_parallel.hpp:251-317) */
+usap_status usap_ctx_load(usap_ctx* ctx, const usap_graph* g);
+usap_status usap_ctx_num_nodes(usap_ctx* ctx, int32_t* n, int64_t* e);
+/* partition() on the loaded graph; out_assign may be NULL */
+usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out_assign,
+                               usap_result* out);
+usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user);
+
+/* --- phase-level replay operations (host buffers in and out) ------------- */
+/* _scc (graph_parallel.hpp:514-603) */
+usap_status usap_op_scc(usap_ctx* ctx, int32_t dfs_depth, int32_t* part, int32_t* B);
+/* _initialize_edge_counts (:703-759): M (B*B row-major, may be NULL) and degrees */
+usap_status usap_op_build(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t dense_max,
+                          int32_t* M, int32_t* dout, int32_t* din);
+/* _compute_overall_entropy (:1281-1319), Q32 */
+usap_status usap_op_entropy(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t dense_max,
+                            int64_t* S_q);
+/* block_merge task (:349-368): K proposals per block; prop_* may be NULL */
+usap_status usap_op_merge_phase(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t K,
+                                int32_t stage, uint64_t seed, int32_t* best_s, int64_t* best_q,
+                                int32_t* prop_s, int64_t* prop_q);
+/* _carry_out_best_merges (:1225-1279); part is updated in place */
+usap_status usap_op_merge_apply(usap_ctx* ctx, int32_t* part, int32_t B, const int32_t* best_s,
+                                const int64_t* best_q, int32_t b_to_merge, int32_t* B_new,
+                                int32_t* merged);
+/* nodal_move + update tasks for one batch [beg, end) (:397-443); part is
+ * updated in place; prop_* (end-beg entries) may be NULL */
+usap_status usap_op_nodal_batch(usap_ctx* ctx, int32_t* part, int32_t B, int32_t dense_max,
+                                int32_t beg, int32_t end, int32_t itr, int32_t stage,
+                                uint64_t seed, int32_t* prop_s, int64_t* prop_q,
+                                int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
+                                int64_t* moves);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,97 @@
+"""C ABI checks that need no GPU: the library loads, exports every entry point
+include/usap.h declares, its host-side evaluation matches the oracle, and
+errors come back as status codes."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from usap_b200 import native as nat
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "usap.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)     # drop comments
+    return sorted(set(re.findall(r"\b(usap_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = nat.lib()
+    declared = _declared()
+    assert declared, "no declarations found"
+    for name in declared:
+        assert hasattr(L, name), name
+    assert sorted(nat.EXPORTS) == declared
+
+
+def test_version_and_defaults():
+    L = nat.lib()
+    assert b"sm_100a" in L.usap_version()
+    p = nat.default_params()
+    # the reference's defaults (graph_parallel.hpp:40-52)
+    assert p.beta == 3 and p.block_size == 1024 and p.num_agg_proposals_per_block == 10
+    assert abs(p.num_block_reduction_rate - 0.5) < 1e-7 and p.max_num_nodal_itr == 100
+    assert p.num_batch_nodal_update == 4 and p.delta_entropy_moving_avg_window == 3
+    assert p.delta_entropy_threshold1 == 5e-4 and p.delta_entropy_threshold2 == 1e-4
+    assert p.dfs_depth == 20 and p.t_block_num == 20
+
+
+def test_evaluate_matches_oracle(oracle):
+    rng = np.random.default_rng(5)
+    for n, b1, b2 in ((500, 7, 7), (1000, 11, 25), (300, 9, 3)):
+        truth = rng.integers(0, b1, n).astype(np.int32)
+        given = np.where(rng.random(n) < 0.7, truth % b2, rng.integers(0, b2, n)).astype(np.int32)
+        from usap_b200.api import evaluate
+        mine = evaluate(truth, given)
+        ref = oracle.evaluate(truth, given)
+        for k in ("rand_index", "adjusted_rand_index", "adjusted_rand_index_exact",
+                  "pairwise_recall", "pairwise_precision", "h_truth", "h_given",
+                  "h_truth_given", "h_given_truth", "mi", "nmi", "nmi_sqrt", "missed_info",
+                  "erroneous_info"):
+            assert abs(mine[k] - ref[k]) <= 1e-12 * max(1.0, abs(ref[k])), k
+        assert mine["n"] == ref["n"]
+
+
+def test_evaluate_accuracy_is_optimal_matching():
+    from usap_b200.api import evaluate
+    truth = np.array([0, 0, 0, 1, 1, 2, 2, 2, 2], np.int32)
+    given = np.array([2, 2, 1, 0, 0, 1, 1, 1, 2], np.int32)
+    s = evaluate(truth, given)
+    # best matching: 0->2 (2), 1->0 (2), 2->1 (3) = 7 of 9
+    assert abs(s["accuracy"] - 7 / 9) < 1e-12
+
+
+def test_evaluate_rejects_bad_input():
+    L = nat.lib()
+    t = np.zeros(1, np.int32)
+    rc = L.usap_evaluate(nat.p32(t), nat.p32(t), 1, C.byref(nat.Scores()))
+    assert rc == -1 and L.usap_last_error()
+    rc = L.usap_evaluate(None, nat.p32(t), 1, C.byref(nat.Scores()))
+    assert rc == -1
+
+
+def test_null_arguments_are_errors_not_crashes():
+    L = nat.lib()
+    assert L.usap_partition(None, None, None, None) == -1
+    assert L.usap_ctx_load(None, None) == -1
+    assert L.usap_ctx_partition(None, None, None, None) == -1
+    assert L.usap_op_build(None, None, 1, 0, None, None, None) == -1
+
+
+def test_no_device_is_reported(monkeypatch):
+    """Without a visible GPU the context refuses with USAP_ERR_NO_DEVICE or
+    USAP_ERR_CUDA (never a crash)."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is visible")
+    except ImportError:
+        pass
+    h = C.c_void_p()
+    rc = nat.lib().usap_ctx_create(0, C.byref(h))
+    assert rc in (-5, -2)
+    assert nat.lib().usap_last_error()

@@ -1,0 +1,213 @@
+// extern "C" entry points (include/usap.h).  Errors never escape as C++
+// exceptions: each call returns a status and records a message for the
+// calling thread.
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "../../include/usap.h"
+#include "job.h"
+
+struct usap_ctx {
+  std::unique_ptr<usap::Job> job;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <class F>
+usap_status guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return USAP_OK;
+  } catch (const usap::Error& e) {
+    g_last_error = e.what();
+    return e.code();
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return USAP_ERR_OOM;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return USAP_ERR_INTERNAL;
+  }
+}
+
+void check_ctx(usap_ctx* ctx) {
+  if (!ctx || !ctx->job) throw usap::Error(USAP_ERR_INVALID, "null context");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* usap_version(void) { return "usap-b200 0.1 (sm_100a)"; }
+
+const char* usap_last_error(void) { return g_last_error.c_str(); }
+
+void usap_params_default(usap_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->beta = 3;
+  p->block_size = 1024;
+  p->num_agg_proposals_per_block = 10;
+  p->num_block_reduction_rate = 0.5f;
+  p->max_num_nodal_itr = 100;
+  p->num_batch_nodal_update = 4;
+  p->delta_entropy_threshold1 = 5e-4;
+  p->delta_entropy_threshold2 = 1e-4;
+  p->delta_entropy_moving_avg_window = 3;
+  p->verbose = 0;
+  p->dfs_depth = 20;
+  p->t_block_num = 20;
+  p->seed = 0;
+  p->init_mode = 0;
+  p->dense_max = 4096;
+  p->device = 0;
+  p->stats = 0;
+}
+
+usap_status usap_partition(const usap_graph* g, const usap_params* p, int32_t* out_assign,
+                           usap_result* out) {
+  return guarded([&] {
+    if (!g || !out_assign || !out) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    usap_params def;
+    usap_params_default(&def);
+    const usap_params& prm = p ? *p : def;
+    usap::Job job(prm.device);
+    job.load(*g);
+    job.partition(prm, out_assign, out);
+    out->ms_h2d = job.last_h2d_ms();
+  });
+}
+
+usap_status usap_evaluate(const int32_t* truth, const int32_t* given, int64_t n, usap_scores* out) {
+  return guarded([&] {
+    if (!truth || !given || !out) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    usap::evaluate_host(truth, given, n, out);
+  });
+}
+
+usap_status usap_ctx_create(int32_t device, usap_ctx** out) {
+  return guarded([&] {
+    if (!out) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto ctx = std::make_unique<usap_ctx>();
+    ctx->job = std::make_unique<usap::Job>(device);
+    *out = ctx.release();
+  });
+}
+
+usap_status usap_ctx_destroy(usap_ctx* ctx) {
+  return guarded([&] { delete ctx; });
+}
+
+usap_status usap_ctx_load(usap_ctx* ctx, const usap_graph* g) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (!g) throw usap::Error(USAP_ERR_INVALID, "null graph");
+    ctx->job->load(*g);
+  });
+}
+
+usap_status usap_ctx_num_nodes(usap_ctx* ctx, int32_t* n, int64_t* e) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (n) *n = ctx->job->host_graph().n;
+    if (e) *e = ctx->job->host_graph().e;
+  });
+}
+
+usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out_assign,
+                               usap_result* out) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (!out) throw usap::Error(USAP_ERR_INVALID, "null result");
+    usap_params def;
+    usap_params_default(&def);
+    ctx->job->partition(p ? *p : def, out_assign, out);
+  });
+}
+
+usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user) {
+  return guarded([&] {
+    check_ctx(ctx);
+    ctx->job->set_trace(fn, user);
+  });
+}
+
+usap_status usap_op_scc(usap_ctx* ctx, int32_t dfs_depth, int32_t* part, int32_t* B) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (!part || !B) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    *B = ctx->job->op_scc(dfs_depth, part);
+  });
+}
+
+static void check_part(usap_ctx* ctx, const int32_t* part, int32_t B) {
+  if (!part) throw usap::Error(USAP_ERR_INVALID, "null partition");
+  const auto& hg = ctx->job->host_graph();
+  if (hg.n <= 0) throw usap::Error(USAP_ERR_STATE, "no graph loaded");
+  if (B < 1) throw usap::Error(USAP_ERR_INVALID, "B must be >= 1");
+  for (int32_t v = 0; v < hg.n; v++)
+    if (part[v] < 0 || part[v] >= B) throw usap::Error(USAP_ERR_INVALID, "block id out of range");
+}
+
+usap_status usap_op_build(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t dense_max,
+                          int32_t* M, int32_t* dout, int32_t* din) {
+  return guarded([&] {
+    check_ctx(ctx);
+    check_part(ctx, part, B);
+    if (!dout || !din) throw usap::Error(USAP_ERR_INVALID, "null degree buffer");
+    ctx->job->op_build(part, B, dense_max > 0 ? dense_max : 4096, M, dout, din);
+  });
+}
+
+usap_status usap_op_entropy(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t dense_max,
+                            int64_t* S_q) {
+  return guarded([&] {
+    check_ctx(ctx);
+    check_part(ctx, part, B);
+    if (!S_q) throw usap::Error(USAP_ERR_INVALID, "null output");
+    *S_q = ctx->job->op_entropy(part, B, dense_max > 0 ? dense_max : 4096);
+  });
+}
+
+usap_status usap_op_merge_phase(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t K,
+                                int32_t stage, uint64_t seed, int32_t* best_s, int64_t* best_q,
+                                int32_t* prop_s, int64_t* prop_q) {
+  return guarded([&] {
+    check_ctx(ctx);
+    check_part(ctx, part, B);
+    if (!best_s || !best_q) throw usap::Error(USAP_ERR_INVALID, "null output");
+    ctx->job->op_merge_phase(part, B, K, stage, seed, best_s, best_q, prop_s, prop_q);
+  });
+}
+
+usap_status usap_op_merge_apply(usap_ctx* ctx, int32_t* part, int32_t B, const int32_t* best_s,
+                                const int64_t* best_q, int32_t b_to_merge, int32_t* B_new,
+                                int32_t* merged) {
+  return guarded([&] {
+    check_ctx(ctx);
+    check_part(ctx, part, B);
+    if (!best_s || !best_q || !B_new || !merged) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    ctx->job->op_merge_apply(part, B, best_s, best_q, b_to_merge, B_new, merged);
+  });
+}
+
+usap_status usap_op_nodal_batch(usap_ctx* ctx, int32_t* part, int32_t B, int32_t dense_max,
+                                int32_t beg, int32_t end, int32_t itr, int32_t stage,
+                                uint64_t seed, int32_t* prop_s, int64_t* prop_q,
+                                int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
+                                int64_t* moves) {
+  return guarded([&] {
+    check_ctx(ctx);
+    check_part(ctx, part, B);
+    ctx->job->op_nodal_batch(part, B, dense_max > 0 ? dense_max : 4096, beg, end, itr, stage, seed,
+                             prop_s, prop_q, prop_ninf, cum_q, cum_ninf, moves);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,190 @@
+// Device state of one partitioning job and the launchers of its kernels.
+//
+// HBM layout (one job):
+//   graph   edge list src/dst[/w] (file order), CSR out/in (int32 offsets,
+//           file order inside each list), weighted degrees, log table
+//           log(k) for k <= total weight (FP64);
+//   state   four partition buffers (working + golden-section bracket),
+//           block degrees dout/din;
+//   blocks  either a dense int32 tile M and its transpose Mt (row stride
+//           ld = B rounded up to 4) when B <= dense_max, or sorted sparse
+//           views rebuilt from the edge list: CSR of M (row = source
+//           block), CSC of M, and the symmetric rows M[u,:]+M[:,u] with
+//           inclusive cumulative counts for block-order sampling;
+//   merge   K proposals per block, best target/dS, union-find scratch;
+//   nodal   per-vertex move target (-1 = stay), control block.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+namespace usap {
+
+class Error : public std::runtime_error {
+ public:
+  Error(int code, const std::string& msg) : std::runtime_error(msg), code_(code) {}
+  int code() const { return code_; }
+
+ private:
+  int code_;
+};
+
+void cuda_check(cudaError_t e, const char* what, const char* file, int line);
+#define USAP_CUDA(x) ::usap::cuda_check((x), #x, __FILE__, __LINE__)
+
+// Dense block matrix view: M[x*ld + y], transposed copy Mt[y*ld + x].
+struct DenseView {
+  const int* M;
+  const int* Mt;
+  int ld;
+};
+
+// Sorted sparse view built from the edge list.
+struct SortedView {
+  const int* rowptr;  // [B+1]
+  const int* col;     // [nnz] column (target block) of each M entry, row-major sorted
+  const int* val;
+  const int* colptr;  // [B+1] CSC of M (may be null when not built)
+  const int* row;
+  const int* cval;
+  const int* symptr;  // [B+1] rows of M[u,:]+M[:,u]
+  const int* symcol;
+  const int* symcum;  // global inclusive cumulative count
+};
+
+// Control block of a nodal phase, resident on the device so that batches
+// and sweeps can be queued without host round trips.
+struct NodalCtl {
+  int done;          // convergence reached: later batch kernels return at once
+  int S_ninf;
+  int cum_ninf;
+  int pad0;
+  long long S_q;     // running description length (Q32)
+  unsigned long long cum_q;   // accepted dS of the current sweep (Q32, two's complement)
+  unsigned long long moves;   // accepted moves (whole phase)
+  unsigned long long near;    // proposals with |dS| <= 1e-9
+  unsigned long long proposals;
+  unsigned long long edge_visits;
+  unsigned long long batches;
+  unsigned long long sweeps;
+  double mean;       // moving average of the previous sweeps' dS
+  unsigned long long entropy_acc;  // data term accumulator of the entropy kernel
+  unsigned long long bytes;        // algorithmic bytes of the nodal kernel (stats)
+};
+
+struct GraphDev {
+  int32_t n = 0;
+  int64_t e = 0;
+  int64_t wtot = 0;
+  bool unit = true;
+  int32_t *src = nullptr, *dst = nullptr, *w = nullptr;
+  int32_t *out_ptr = nullptr, *out_idx = nullptr, *out_w = nullptr;
+  int32_t *in_ptr = nullptr, *in_idx = nullptr, *in_w = nullptr;
+  int32_t *kout = nullptr, *kin = nullptr;
+  double* logk = nullptr;
+  // per-vertex global hash region for vertices too large for shared memory
+  int64_t* hi_off = nullptr;
+  int64_t hi_slots = 0;
+  int32_t *hkey = nullptr, *hwo = nullptr, *hwi = nullptr;
+};
+
+// Arguments of the nodal proposal kernel.
+struct NodalArgs {
+  const int32_t *out_ptr, *out_idx, *out_w, *in_ptr, *in_idx, *in_w, *kout, *kin;
+  const double* L;
+  int unit;
+  const int32_t* part;
+  int B;
+  const int32_t *dout, *din;
+  int beg, end;
+  uint32_t itr, stage;
+  uint64_t seed;
+  int32_t* move_to;
+  int32_t* prop_s;        // optional, [end-beg]
+  long long* prop_q;
+  int32_t* prop_ninf;
+  NodalCtl* ctl;
+  const int64_t* hi_off;
+  int32_t *hkey, *hwo, *hwi;
+  int stats;
+};
+
+struct MergeArgs {
+  const double* L;
+  int B, K;
+  uint32_t stage;
+  uint64_t seed;
+  const int32_t *dout, *din;
+  int32_t* prop_s;   // [B*K]
+  long long* prop_q;
+};
+
+// --- launchers (kernels_*.cu) -------------------------------------------------
+void launch_dense_build(const GraphDev& g, const int32_t* part, int B, int ld, int* M, int* Mt,
+                        cudaStream_t st);
+void launch_degrees(const GraphDev& g, const int32_t* part, int B, int32_t* dout, int32_t* din,
+                    cudaStream_t st);
+void launch_entropy_dense(const GraphDev& g, DenseView v, int B, const int32_t* dout,
+                          const int32_t* din, unsigned long long* acc, cudaStream_t st);
+void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, int64_t max_nnz,
+                           const int32_t* rowof, const int32_t* dout, const int32_t* din,
+                           unsigned long long* acc, cudaStream_t st);
+
+void launch_merge_propose(const GraphDev& g, SortedView v, const MergeArgs& a, cudaStream_t st);
+void launch_merge_argmin(int B, int K, const int32_t* prop_s, const long long* prop_q,
+                         int32_t* best_s, long long* best_q, cudaStream_t st);
+void launch_merge_union(int B, const int32_t* order, const int32_t* best_s, int btm,
+                        int32_t* work, int32_t* root, int32_t* merged, cudaStream_t st);
+void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int32_t* present,
+                          int32_t* newlabel, void* cub_tmp, size_t cub_bytes, cudaStream_t st);
+
+void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, cudaStream_t st);
+void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, cudaStream_t st);
+void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int beg,
+                              int end, int ld, int* M, int* Mt, int32_t* dout, int32_t* din,
+                              const NodalCtl* ctl, cudaStream_t st);
+void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
+                         int update_degrees, int32_t* dout, int32_t* din, const NodalCtl* ctl,
+                         cudaStream_t st);
+void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int W,
+                            const long long* ide_q, const int* ide_n, cudaStream_t st);
+void launch_ctl_batch_end(NodalCtl* ctl, int itr, int W, double thr, long long* ide_q,
+                          int* ide_n, long long batch_vertices, long long batch_edges,
+                          cudaStream_t st);
+void launch_merge_sort_keys(int B, const long long* best_q, unsigned long long* keys, int32_t* idx,
+                            cudaStream_t st);
+
+// Sort-based construction of the sparse views (CUB radix sort).
+class SortedBuilder {
+ public:
+  void reserve(int64_t e, int bmax);
+  void release();
+  // builds row view (+ optional CSC) and symmetric rows for partition `part`
+  void build(const GraphDev& g, const int32_t* part, int B, bool with_csc, bool with_sym,
+             cudaStream_t st);
+  SortedView view() const;
+  const int* nnz_dev() const { return nnz_; }
+  const int32_t* rowof() const { return rowof_; }
+  int64_t max_nnz() const { return e_; }
+
+ private:
+  void sort_reduce(int64_t count, int B, int kind, cudaStream_t st);
+  int64_t e_ = 0;
+  int bmax_ = 0;
+  unsigned long long *keys_ = nullptr, *keys_alt_ = nullptr, *ukeys_ = nullptr;
+  int *vals_ = nullptr, *vals_alt_ = nullptr, *uvals_ = nullptr;
+  int *nruns_ = nullptr;  // [3]: nnz of row view, CSC, sym
+  int *nnz_ = nullptr;
+  int *rowptr_ = nullptr, *col_ = nullptr, *val_ = nullptr, *rowof_ = nullptr;
+  int *colptr_ = nullptr, *crow_ = nullptr, *cval_ = nullptr;
+  int *symptr_ = nullptr, *symcol_ = nullptr, *symcum_ = nullptr;
+  void* tmp_ = nullptr;
+  size_t tmp_bytes_ = 0;
+  bool has_csc_ = false;
+};
+
+}  // namespace usap

@@ -1,0 +1,782 @@
+// Host orchestration of one partitioning job (Graph_P::partition,
+// graph_parallel.hpp:322-512): initial blocks, then stages of
+// merge phase -> merge application -> batched nodal sweeps -> description
+// length -> golden-section step, until the bracket closes.  All phases run
+// on the device; the host keeps the golden-section bracket (three partition
+// slots resident in HBM, swapped by index) and reads back one control block
+// per sweep.
+#include "job.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include <cub/cub.cuh>
+
+namespace usap {
+
+void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
+  if (e == cudaSuccess) return;
+  int code = (e == cudaErrorMemoryAllocation) ? USAP_ERR_OOM : USAP_ERR_CUDA;
+  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e) + " (" + file + ":" +
+                        std::to_string(line) + ")");
+}
+
+namespace {
+
+template <class T>
+void dalloc(T** p, size_t count) {
+  USAP_CUDA(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (count ? count : 1)));
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+inline uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+int hash_lg(int deg) {
+  int lg = 5;
+  while ((1 << lg) < 2 * deg) lg++;
+  return lg;
+}
+
+constexpr int kSharedHashSlots = 256;   // must match kernels_nodal.cu
+
+}  // namespace
+
+int32_t reduce_blocks(int32_t B, float rate) {
+  return static_cast<int32_t>(static_cast<float>(B) * rate);
+}
+
+double model_S(int64_t n, int64_t e, int32_t B) {
+  double x = static_cast<double>(B) * static_cast<double>(B) / static_cast<double>(e);
+  return static_cast<double>(e) * (1.0 + x) * std::log(1.0 + x) - x * std::log(x) +
+         static_cast<double>(n) * std::log(static_cast<double>(B));
+}
+
+long long q32_host(double t) { return std::llrint(t * 4294967296.0); }
+
+bool Golden::step(int32_t B, int64_t S, int32_t cur_slot, float rate, int32_t* restore_slot,
+                  int32_t* btm) {
+  GoldenPoint cur{B, S, true, cur_slot};
+  if (!med.finite || cur.S <= med.S) {
+    if (med.B > cur.B) large = med;
+    else small = med;
+    med = cur;
+  } else {
+    if (med.B > cur.B) small = cur;
+    else large = cur;
+  }
+  *restore_slot = -1;
+  *btm = 0;
+  if (!small.finite) {
+    *restore_slot = med.slot;
+    *btm = reduce_blocks(med.B, rate);
+    return *btm == 0;
+  }
+  // the reference would continue from an empty default state when the
+  // bracket has no upper end; the search stops at med
+  if (!large.finite) return true;
+  if (large.B - small.B == 2) return true;
+  if ((large.B - med.B) >= (med.B - small.B)) {
+    int32_t next_B = med.B + static_cast<int32_t>(std::round((large.B - med.B) * 0.618));
+    *restore_slot = large.slot;
+    *btm = large.B - next_B;
+  } else {
+    int32_t next_B = small.B + static_cast<int32_t>(std::round((med.B - small.B) * 0.618));
+    *restore_slot = med.slot;
+    *btm = med.B - next_B;
+  }
+  return false;
+}
+
+Job::Job(int device) : device_(device) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+    throw Error(USAP_ERR_NO_DEVICE, "no CUDA device available");
+  if (device < 0 || device >= count) throw Error(USAP_ERR_INVALID, "device index out of range");
+  USAP_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  USAP_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    throw Error(USAP_ERR_NO_DEVICE, std::string("device is not sm_100 class: ") + prop.name);
+  USAP_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  USAP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ctl_), sizeof(NodalCtl)));
+  dalloc(&ctl_, 1);
+}
+
+Job::~Job() {
+  cudaSetDevice(device_);
+  free_state();
+  free_graph();
+  dfree(ctl_);
+  if (h_ctl_) cudaFreeHost(h_ctl_);
+  for (auto e : ev_pool_) cudaEventDestroy(e);
+  if (st_) cudaStreamDestroy(st_);
+}
+
+void Job::free_graph() {
+  dfree(g_.src); dfree(g_.dst); dfree(g_.w);
+  dfree(g_.out_ptr); dfree(g_.out_idx); dfree(g_.out_w);
+  dfree(g_.in_ptr); dfree(g_.in_idx); dfree(g_.in_w);
+  dfree(g_.kout); dfree(g_.kin); dfree(g_.logk);
+  dfree(g_.hi_off); dfree(g_.hkey); dfree(g_.hwo); dfree(g_.hwi);
+  g_ = GraphDev{};
+}
+
+void Job::free_state() {
+  for (auto& s : slots_) dfree(s);
+  dfree(move_to_); dfree(dout_); dfree(din_);
+  dfree(M_); dfree(Mt_);
+  sb_.release();
+  dfree(prop_s_); dfree(prop_q_); dfree(best_s_); dfree(best_q_);
+  dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
+  dfree(union_work_); dfree(root_); dfree(present_); dfree(newlabel_); dfree(merged_dev_);
+  if (cub_tmp_) cudaFree(cub_tmp_);
+  cub_tmp_ = nullptr;
+  cub_bytes_ = 0;
+  dfree(ide_q_); dfree(ide_n_);
+  dfree(rp_s_); dfree(rp_n_); dfree(rp_q_);
+  bcap_ = kcap_ = dcap_ = icap_ = 0;
+}
+
+// --- graph load -----------------------------------------------------------------
+void Job::load(const usap_graph& in) {
+  USAP_CUDA(cudaSetDevice(device_));
+  if (in.e <= 0 || !in.src || !in.dst) throw Error(USAP_ERR_INVALID, "graph needs at least one edge");
+  if (in.e >= (1ll << 30)) throw Error(USAP_ERR_LIMIT, "more than 2^30 edges");
+  HostGraph h;
+  h.e = in.e;
+  const int32_t base = in.one_based ? 1 : 0;
+  h.src.resize(in.e);
+  h.dst.resize(in.e);
+  int64_t maxsrc = -1, maxid = -1;
+  for (int64_t i = 0; i < in.e; i++) {
+    int64_t a = static_cast<int64_t>(in.src[i]) - base, b = static_cast<int64_t>(in.dst[i]) - base;
+    if (a < 0 || b < 0) throw Error(USAP_ERR_INVALID, "negative vertex id at edge " + std::to_string(i));
+    maxsrc = std::max(maxsrc, a);
+    maxid = std::max(maxid, std::max(a, b));
+    h.src[i] = static_cast<int32_t>(a);
+    h.dst[i] = static_cast<int32_t>(b);
+  }
+  h.n = in.n > 0 ? in.n : static_cast<int32_t>(maxsrc + 1);
+  if (maxid >= h.n)
+    throw Error(USAP_ERR_INVALID, "vertex id " + std::to_string(maxid) + " >= n = " + std::to_string(h.n));
+  h.unit = true;
+  int64_t wtot = 0;
+  if (in.weight) {
+    h.w.resize(in.e);
+    for (int64_t i = 0; i < in.e; i++) {
+      if (in.weight[i] <= 0) throw Error(USAP_ERR_INVALID, "edge weights must be positive");
+      h.w[i] = in.weight[i];
+      wtot += in.weight[i];
+      if (in.weight[i] != 1) h.unit = false;
+    }
+    if (h.unit) h.w.clear();
+  } else {
+    wtot = in.e;
+  }
+  if (wtot >= (1ll << 24)) throw Error(USAP_ERR_LIMIT, "total edge weight must be below 2^24");
+  h.wtot = wtot;
+  const int32_t n = h.n;
+  h.out_ptr.assign(n + 1, 0);
+  h.in_ptr.assign(n + 1, 0);
+  h.kout.assign(n, 0);
+  h.kin.assign(n, 0);
+  for (int64_t i = 0; i < h.e; i++) {
+    int32_t ww = h.unit ? 1 : h.w[i];
+    h.out_ptr[h.src[i] + 1]++;
+    h.in_ptr[h.dst[i] + 1]++;
+    h.kout[h.src[i]] += ww;
+    h.kin[h.dst[i]] += ww;
+  }
+  for (int32_t v = 0; v < n; v++) {
+    h.out_ptr[v + 1] += h.out_ptr[v];
+    h.in_ptr[v + 1] += h.in_ptr[v];
+  }
+  h.out_idx.resize(h.e);
+  h.in_idx.resize(h.e);
+  if (!h.unit) {
+    h.out_w.resize(h.e);
+    h.in_w.resize(h.e);
+  }
+  {
+    std::vector<int32_t> fo(h.out_ptr.begin(), h.out_ptr.end() - 1), fi(h.in_ptr.begin(), h.in_ptr.end() - 1);
+    for (int64_t i = 0; i < h.e; i++) {   // stable: edge order within each list
+      int32_t po = fo[h.src[i]]++, pi = fi[h.dst[i]]++;
+      h.out_idx[po] = h.dst[i];
+      h.in_idx[pi] = h.src[i];
+      if (!h.unit) {
+        h.out_w[po] = h.w[i];
+        h.in_w[pi] = h.w[i];
+      }
+    }
+  }
+  // per-vertex global hash regions for degrees beyond the shared-memory table
+  std::vector<int64_t> hi_off(n, -1);
+  int64_t hi_slots = 0;
+  for (int32_t v = 0; v < n; v++) {
+    int deg = (h.out_ptr[v + 1] - h.out_ptr[v]) + (h.in_ptr[v + 1] - h.in_ptr[v]);
+    int cap = 1 << hash_lg(deg);
+    if (cap > kSharedHashSlots) {
+      hi_off[v] = hi_slots;
+      hi_slots += cap;
+    }
+  }
+  std::vector<double> logk(wtot + 1);
+  logk[0] = -INFINITY;
+  for (int64_t k = 1; k <= wtot; k++) logk[k] = std::log(static_cast<double>(k));
+
+  free_state();
+  free_graph();
+  cudaEvent_t e0, e1;
+  USAP_CUDA(cudaEventCreate(&e0));
+  USAP_CUDA(cudaEventCreate(&e1));
+  USAP_CUDA(cudaEventRecord(e0, st_));
+  GraphDev g;
+  g.n = n;
+  g.e = h.e;
+  g.wtot = wtot;
+  g.unit = h.unit;
+  auto up = [&](int32_t** d, const std::vector<int32_t>& v) {
+    dalloc(d, v.size());
+    if (!v.empty())
+      USAP_CUDA(cudaMemcpyAsync(*d, v.data(), sizeof(int32_t) * v.size(), cudaMemcpyHostToDevice, st_));
+  };
+  up(&g.src, h.src);
+  up(&g.dst, h.dst);
+  if (!h.unit) {
+    up(&g.w, h.w);
+    up(&g.out_w, h.out_w);
+    up(&g.in_w, h.in_w);
+  }
+  up(&g.out_ptr, h.out_ptr);
+  up(&g.out_idx, h.out_idx);
+  up(&g.in_ptr, h.in_ptr);
+  up(&g.in_idx, h.in_idx);
+  up(&g.kout, h.kout);
+  up(&g.kin, h.kin);
+  dalloc(&g.logk, logk.size());
+  USAP_CUDA(cudaMemcpyAsync(g.logk, logk.data(), sizeof(double) * logk.size(), cudaMemcpyHostToDevice, st_));
+  dalloc(&g.hi_off, n);
+  USAP_CUDA(cudaMemcpyAsync(g.hi_off, hi_off.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st_));
+  g.hi_slots = hi_slots;
+  dalloc(&g.hkey, hi_slots);
+  dalloc(&g.hwo, hi_slots);
+  dalloc(&g.hwi, hi_slots);
+  USAP_CUDA(cudaEventRecord(e1, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+  float ms = 0;
+  USAP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  h2d_ms_ = ms;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  g_ = g;
+  hg_ = std::move(h);
+}
+
+void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxitr) {
+  const int32_t n = hg_.n;
+  bool fresh = slots_[0] == nullptr;
+  if (fresh) {
+    for (auto& s : slots_) dalloc(&s, n);
+    dalloc(&move_to_, n);
+    USAP_CUDA(cudaMemsetAsync(move_to_, 0xff, sizeof(int32_t) * n, st_));
+    dalloc(&rp_s_, n);
+    dalloc(&rp_n_, n);
+    dalloc(&rp_q_, n);
+  }
+  if (B > bcap_) {
+    dfree(dout_); dfree(din_); dfree(best_s_); dfree(best_q_);
+    dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
+    dfree(union_work_); dfree(root_); dfree(present_); dfree(newlabel_); dfree(merged_dev_);
+    dalloc(&dout_, B);
+    dalloc(&din_, B);
+    dalloc(&best_s_, B);
+    dalloc(&best_q_, B);
+    dalloc(&skeys_, B);
+    dalloc(&skeys_alt_, B);
+    dalloc(&sidx_, B);
+    dalloc(&sidx_alt_, B);
+    dalloc(&union_work_, 8ll * B);
+    dalloc(&root_, B);
+    dalloc(&present_, B);
+    dalloc(&newlabel_, B);
+    dalloc(&merged_dev_, 1);
+    if (cub_tmp_) cudaFree(cub_tmp_);
+    size_t b1 = 0, b2 = 0;
+    USAP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, skeys_, skeys_alt_, sidx_, sidx_alt_, B));
+    USAP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b2, present_, newlabel_, B));
+    cub_bytes_ = std::max(b1, b2);
+    USAP_CUDA(cudaMalloc(&cub_tmp_, cub_bytes_));
+    sb_.reserve(hg_.e, B);
+    bcap_ = B;
+    kcap_ = 0;
+  }
+  if (static_cast<int64_t>(B) * K > static_cast<int64_t>(bcap_) * kcap_) {
+    dfree(prop_s_);
+    dfree(prop_q_);
+    dalloc(&prop_s_, static_cast<size_t>(bcap_) * K);
+    dalloc(&prop_q_, static_cast<size_t>(bcap_) * K);
+    kcap_ = K;
+  }
+  int32_t dneed = std::min(B, dense_max);
+  int32_t ld = (dneed + 3) & ~3;
+  if (ld > dcap_) {
+    dfree(M_);
+    dfree(Mt_);
+    dalloc(&M_, static_cast<size_t>(ld) * ld);
+    dalloc(&Mt_, static_cast<size_t>(ld) * ld);
+    dcap_ = ld;
+  }
+  if (maxitr > icap_) {
+    dfree(ide_q_);
+    dfree(ide_n_);
+    dalloc(&ide_q_, maxitr);
+    dalloc(&ide_n_, maxitr);
+    icap_ = maxitr;
+  }
+}
+
+// --- phases ---------------------------------------------------------------------
+void Job::prepare_nodal_blocks(const int32_t* part, int32_t B, bool dense) {
+  launch_degrees(g_, part, B, dout_, din_, st_);
+  if (dense) {
+    ld_ = (B + 3) & ~3;
+    launch_dense_build(g_, part, B, ld_, M_, Mt_, st_);
+  } else {
+    sb_.build(g_, part, B, false, true, st_);
+  }
+}
+
+void Job::merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage, uint64_t seed) {
+  launch_degrees(g_, part, B, dout_, din_, st_);
+  sb_.build(g_, part, B, true, true, st_);
+  MergeArgs a;
+  a.L = g_.logk;
+  a.B = B;
+  a.K = K;
+  a.stage = stage;
+  a.seed = seed;
+  a.dout = dout_;
+  a.din = din_;
+  a.prop_s = prop_s_;
+  a.prop_q = prop_q_;
+  launch_merge_propose(g_, sb_.view(), a, st_);
+  launch_merge_argmin(B, K, prop_s_, prop_q_, best_s_, best_q_, st_);
+}
+
+int32_t Job::merge_apply(int32_t* part, int32_t B, int32_t btm) {
+  launch_merge_sort_keys(B, best_q_, skeys_, sidx_, st_);
+  size_t bytes = cub_bytes_;
+  USAP_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_, bytes, skeys_, skeys_alt_, sidx_, sidx_alt_, B, 0,
+                                            64, st_));
+  launch_merge_union(B, sidx_alt_, best_s_, btm, union_work_, root_, merged_dev_, st_);
+  launch_merge_relabel(hg_.n, B, part, root_, present_, newlabel_, cub_tmp_, cub_bytes_, st_);
+  int32_t merged = 0;
+  USAP_CUDA(cudaMemcpyAsync(&h_ctl_->pad0, merged_dev_, sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+  merged = h_ctl_->pad0;
+  return merged;
+}
+
+void Job::entropy_launch(const int32_t* part, int32_t B, bool dense) {
+  USAP_CUDA(cudaMemsetAsync(&ctl_->entropy_acc, 0, sizeof(unsigned long long), st_));
+  if (dense) {
+    launch_entropy_dense(g_, dense_view(), B, dout_, din_, &ctl_->entropy_acc, st_);
+  } else {
+    launch_entropy_sorted(g_, sb_.view(), sb_.nnz_dev(), sb_.max_nnz(), sb_.rowof(), dout_, din_,
+                          &ctl_->entropy_acc, st_);
+  }
+}
+
+void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t itr,
+                      uint32_t stage, uint64_t seed, bool first_of_sweep, int stats) {
+  if (!dense && !first_of_sweep) sb_.build(g_, part, B, false, true, st_);
+  NodalArgs a;
+  a.out_ptr = g_.out_ptr;
+  a.out_idx = g_.out_idx;
+  a.out_w = g_.out_w;
+  a.in_ptr = g_.in_ptr;
+  a.in_idx = g_.in_idx;
+  a.in_w = g_.in_w;
+  a.kout = g_.kout;
+  a.kin = g_.kin;
+  a.L = g_.logk;
+  a.unit = g_.unit ? 1 : 0;
+  a.part = part;
+  a.B = B;
+  a.dout = dout_;
+  a.din = din_;
+  a.beg = beg;
+  a.end = end;
+  a.itr = itr;
+  a.stage = stage;
+  a.seed = seed;
+  a.move_to = move_to_;
+  a.prop_s = nullptr;
+  a.prop_q = nullptr;
+  a.prop_ninf = nullptr;
+  a.ctl = ctl_;
+  a.hi_off = g_.hi_off;
+  a.hkey = g_.hkey;
+  a.hwo = g_.hwo;
+  a.hwi = g_.hwi;
+  a.stats = stats;
+  if (stats == 2) {   // replay: per-vertex proposals
+    a.prop_s = rp_s_;
+    a.prop_q = rp_q_;
+    a.prop_ninf = rp_n_;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (stats == 1) {
+    while (ev_pool_.size() < ev_used_ + 2) {
+      cudaEvent_t e;
+      USAP_CUDA(cudaEventCreate(&e));
+      ev_pool_.push_back(e);
+    }
+    e0 = ev_pool_[ev_used_++];
+    e1 = ev_pool_[ev_used_++];
+    USAP_CUDA(cudaEventRecord(e0, st_));
+  }
+  if (dense) launch_nodal_propose_dense(a, dense_view(), st_);
+  else launch_nodal_propose_sorted(a, sb_.view(), st_);
+  if (stats == 1) USAP_CUDA(cudaEventRecord(e1, st_));
+  if (dense) launch_nodal_apply_dense(g_, part, move_to_, beg, end, ld_, M_, Mt_, dout_, din_, ctl_, st_);
+  launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, st_);
+}
+
+void Job::emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part, bool dense,
+                     long long S_q, int S_ninf, long long cum_q, int cum_ninf, long long moves) {
+  const int32_t n = hg_.n;
+  std::vector<int32_t> hp(n), hdo(B), hdi(B);
+  USAP_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaMemcpyAsync(hdo.data(), dout_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaMemcpyAsync(hdi.data(), din_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
+  uint64_t hM = 0;
+  if (dense) {
+    std::vector<int32_t> hm(static_cast<size_t>(ld_) * B);
+    USAP_CUDA(cudaMemcpyAsync(hm.data(), M_, sizeof(int32_t) * hm.size(), cudaMemcpyDeviceToHost, st_));
+    USAP_CUDA(cudaStreamSynchronize(st_));
+    for (int32_t i = 0; i < B; i++)
+      for (int32_t j = 0; j < B; j++) {
+        int32_t m = hm[static_cast<size_t>(i) * ld_ + j];
+        if (m) hM += mix64(mix64((static_cast<uint64_t>(i) << 32) | static_cast<uint32_t>(j)) ^ static_cast<uint64_t>(m));
+      }
+  } else {
+    sb_.build(g_, part, B, false, false, st_);
+    SortedView v = sb_.view();
+    int nnz = 0;
+    USAP_CUDA(cudaMemcpyAsync(&nnz, sb_.nnz_dev(), sizeof(int), cudaMemcpyDeviceToHost, st_));
+    USAP_CUDA(cudaStreamSynchronize(st_));
+    std::vector<int32_t> rp(B + 1), col(nnz), val(nnz);
+    USAP_CUDA(cudaMemcpyAsync(rp.data(), v.rowptr, sizeof(int32_t) * (B + 1), cudaMemcpyDeviceToHost, st_));
+    USAP_CUDA(cudaMemcpyAsync(col.data(), v.col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st_));
+    USAP_CUDA(cudaMemcpyAsync(val.data(), v.val, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st_));
+    USAP_CUDA(cudaStreamSynchronize(st_));
+    for (int32_t i = 0; i < B; i++)
+      for (int32_t p = rp[i]; p < rp[i + 1]; p++)
+        if (val[p]) hM += mix64(mix64((static_cast<uint64_t>(i) << 32) | static_cast<uint32_t>(col[p])) ^ static_cast<uint64_t>(val[p]));
+  }
+  uint64_t hpart = 1469598103934665603ull;
+  for (int32_t v = 0; v < n; v++) {
+    hpart ^= static_cast<uint32_t>(hp[v]);
+    hpart *= 1099511628211ull;
+  }
+  uint64_t hdeg = 0;
+  for (int32_t i = 0; i < B; i++)
+    hdeg += mix64(mix64(static_cast<uint64_t>(i)) ^ ((static_cast<uint64_t>(hdo[i]) << 32) ^ static_cast<uint64_t>(hdi[i])));
+  usap_trace_event ev;
+  std::memset(&ev, 0, sizeof(ev));
+  ev.kind = kind;
+  ev.stage = stage;
+  ev.itr = itr;
+  ev.batch_beg = beg;
+  ev.B = B;
+  ev.S_q = S_q;
+  ev.S_ninf = S_ninf;
+  ev.cum_q = cum_q;
+  ev.cum_ninf = cum_ninf;
+  ev.moves = moves;
+  ev.h_part = hpart;
+  ev.h_M = hM;
+  ev.h_deg = hdeg;
+  trace_(trace_user_, &ev);
+}
+
+// --- the whole solve ------------------------------------------------------------
+void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  USAP_CUDA(cudaSetDevice(device_));
+  if (p.num_agg_proposals_per_block < 1) throw Error(USAP_ERR_INVALID, "num_agg_proposals_per_block must be >= 1");
+  if (p.max_num_nodal_itr < 0) throw Error(USAP_ERR_INVALID, "max_num_nodal_itr must be >= 0");
+  if (p.num_batch_nodal_update < 1) throw Error(USAP_ERR_INVALID, "num_batch_nodal_update must be >= 1");
+  if (p.delta_entropy_moving_avg_window < 1) throw Error(USAP_ERR_INVALID, "moving average window must be >= 1");
+  if (!(p.num_block_reduction_rate > 0.0f && p.num_block_reduction_rate < 1.0f))
+    throw Error(USAP_ERR_INVALID, "num_block_reduction_rate must be in (0, 1)");
+  const int dense_max = p.dense_max > 0 ? p.dense_max : 4096;
+  auto t_start = std::chrono::steady_clock::now();
+  std::memset(res, 0, sizeof(*res));
+  const int32_t n = hg_.n;
+  const int32_t K = p.num_agg_proposals_per_block;
+  const int32_t W = p.delta_entropy_moving_avg_window;
+  const int32_t maxitr = p.max_num_nodal_itr;
+  int32_t bs = n / p.num_batch_nodal_update;
+  if (bs < 1) bs = 1;
+  const int stats = p.stats ? 1 : 0;
+  ev_used_ = 0;
+
+  // initial blocks (host): depth-limited DFS on the transpose, or identity
+  std::vector<int32_t> part0(n);
+  int32_t B;
+  if (p.init_mode == 1) {
+    for (int32_t v = 0; v < n; v++) part0[v] = v;
+    B = n;
+  } else {
+    B = scc_host(hg_, p.dfs_depth, part0.data());
+  }
+  ensure_capacity(B, K, dense_max, std::max(maxitr, 1));
+  int32_t work = 0;
+  USAP_CUDA(cudaMemcpyAsync(slots_[work], part0.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+  auto t_init = std::chrono::steady_clock::now();
+  res->ms_init = std::chrono::duration<double, std::milli>(t_init - t_start).count();
+
+  int32_t btm = reduce_blocks(B, p.num_block_reduction_rate);
+  Golden gs;
+  uint32_t stage = 0;
+  const uint64_t seed = p.seed;
+  double ms_merge = 0, ms_nodal = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kernel_events;
+  for (;;) {
+    if (stage > 100000u) throw Error(USAP_ERR_INTERNAL, "golden-section search did not close");
+    int32_t* part = slots_[work];
+    auto tm0 = std::chrono::steady_clock::now();
+    // merge phase and its application
+    merge_phase(part, B, K, stage, seed);
+    int32_t merged = merge_apply(part, B, btm);
+    if (merged < btm) res->merge_shortfall += btm - merged;
+    B -= merged;
+    auto tm1 = std::chrono::steady_clock::now();
+    ms_merge += std::chrono::duration<double, std::milli>(tm1 - tm0).count();
+
+    // batched nodal sweeps
+    const bool dense = B <= dense_max;
+    prepare_nodal_blocks(part, B, dense);
+    if (trace_) emit_trace(1, stage, 0, 0, B, part, dense, 0, 0, 0, 0, 0);
+    USAP_CUDA(cudaMemsetAsync(ctl_, 0, sizeof(NodalCtl), st_));
+    USAP_CUDA(cudaMemsetAsync(ide_q_, 0, sizeof(long long) * std::max(maxitr, 1), st_));
+    USAP_CUDA(cudaMemsetAsync(ide_n_, 0, sizeof(int) * std::max(maxitr, 1), st_));
+    const bool isf = gs.large.finite && gs.med.finite && gs.small.finite;
+    const double thr = isf ? p.delta_entropy_threshold2 : p.delta_entropy_threshold1;
+    const long long model_q = q32_host(model_S(n, hg_.e, B));
+    trace_prev_moves_ = 0;
+    for (int32_t itr = 0; itr < maxitr; itr++) {
+      if (!dense) sb_.build(g_, part, B, false, true, st_);
+      entropy_launch(part, B, dense);
+      launch_ctl_sweep_start(ctl_, model_q, itr, W, ide_q_, ide_n_, st_);
+      size_t ev_mark = ev_used_;
+      for (int32_t beg = 0; beg < n; beg += bs) {
+        const int32_t end = beg + bs < n ? beg + bs : n;
+        nodal_batch(part, B, dense, beg, end, itr, stage, seed, beg == 0, stats);
+        const long long edges = (static_cast<long long>(hg_.out_ptr[end]) - hg_.out_ptr[beg]) +
+                                (static_cast<long long>(hg_.in_ptr[end]) - hg_.in_ptr[beg]);
+        launch_ctl_batch_end(ctl_, itr, W, thr, ide_q_, ide_n_, end - beg, edges, st_);
+        if (trace_) {
+          USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+          USAP_CUDA(cudaStreamSynchronize(st_));
+          NodalCtl c = *h_ctl_;
+          emit_trace(2, stage, itr, beg, B, part, dense, c.S_q, c.S_ninf, static_cast<long long>(c.cum_q),
+                     c.cum_ninf, static_cast<long long>(c.moves) - trace_prev_moves_);
+          trace_prev_moves_ = static_cast<long long>(c.moves);
+          if (c.done) break;
+        }
+      }
+      USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+      USAP_CUDA(cudaStreamSynchronize(st_));
+      if (stats) {
+        for (size_t i = ev_mark; i + 1 < ev_used_; i += 2) {
+          float ms = 0;
+          USAP_CUDA(cudaEventElapsedTime(&ms, ev_pool_[i], ev_pool_[i + 1]));
+          res->ms_nodal_kernel += ms;
+          res->nodal_kernel_launches++;
+        }
+        ev_used_ = ev_mark;
+      }
+      if (h_ctl_->done) break;
+    }
+    // the control block was read after the last sweep
+    res->sweeps += static_cast<int64_t>(h_ctl_->sweeps);
+    res->batches += static_cast<int64_t>(h_ctl_->batches);
+    res->nodal_proposals += static_cast<int64_t>(h_ctl_->proposals);
+    res->nodal_moves += static_cast<int64_t>(h_ctl_->moves);
+    res->near_threshold += static_cast<int64_t>(h_ctl_->near);
+    res->edge_visits += static_cast<int64_t>(h_ctl_->edge_visits);
+    res->nodal_kernel_bytes += static_cast<double>(h_ctl_->bytes);
+    // description length of the finished stage
+    if (!dense) sb_.build(g_, part, B, false, true, st_);
+    entropy_launch(part, B, dense);
+    USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+    USAP_CUDA(cudaStreamSynchronize(st_));
+    const long long S_fin = model_q - static_cast<long long>(h_ctl_->entropy_acc);
+    auto tn1 = std::chrono::steady_clock::now();
+    ms_nodal += std::chrono::duration<double, std::milli>(tn1 - tm1).count();
+    if (trace_) emit_trace(3, stage, 0, 0, B, part, dense, S_fin, 0, 0, 0, 0);
+    res->stages++;
+    stage++;
+
+    int32_t restore = -1;
+    bool done = gs.step(B, S_fin, work, p.num_block_reduction_rate, &restore, &btm);
+    if (done) {
+      auto td0 = std::chrono::steady_clock::now();
+      if (out_assign)
+        USAP_CUDA(cudaMemcpyAsync(out_assign, slots_[gs.med.slot], sizeof(int32_t) * n,
+                                  cudaMemcpyDeviceToHost, st_));
+      USAP_CUDA(cudaStreamSynchronize(st_));
+      auto td1 = std::chrono::steady_clock::now();
+      res->ms_d2h = std::chrono::duration<double, std::milli>(td1 - td0).count();
+      res->B = gs.med.B;
+      res->S_q = gs.med.S;
+      res->S = static_cast<double>(gs.med.S) / 4294967296.0;
+      break;
+    }
+    // continue from a bracket point: copy it into a slot outside the bracket
+    bool used[4] = {false, false, false, false};
+    for (const GoldenPoint* gp : {&gs.large, &gs.med, &gs.small})
+      if (gp->finite) used[gp->slot] = true;
+    int32_t next = -1;
+    for (int i = 0; i < 4; i++)
+      if (!used[i]) {
+        next = i;
+        break;
+      }
+    if (next < 0 || restore < 0) throw Error(USAP_ERR_INTERNAL, "golden-section slot bookkeeping");
+    USAP_CUDA(cudaMemcpyAsync(slots_[next], slots_[restore], sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st_));
+    B = restore == gs.large.slot ? gs.large.B : gs.med.B;
+    work = next;
+  }
+  res->ms_merge = ms_merge;
+  res->ms_nodal = ms_nodal;
+  res->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+}
+
+// --- phase-level operations -------------------------------------------------------
+int32_t Job::op_scc(int32_t depth, int32_t* part) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  return scc_host(hg_, depth, part);
+}
+
+void Job::op_build(const int32_t* part, int32_t B, int32_t dense_max, int32_t* M, int32_t* dout,
+                   int32_t* din) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  USAP_CUDA(cudaSetDevice(device_));
+  ensure_capacity(B, 1, dense_max, 1);
+  const int32_t n = hg_.n;
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st_));
+  const bool dense = B <= dense_max;
+  prepare_nodal_blocks(slots_[0], B, dense);
+  USAP_CUDA(cudaMemcpyAsync(dout, dout_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaMemcpyAsync(din, din_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
+  if (M) {
+    if (dense) {
+      USAP_CUDA(cudaMemcpy2DAsync(M, sizeof(int32_t) * B, M_, sizeof(int32_t) * ld_, sizeof(int32_t) * B, B,
+                                  cudaMemcpyDeviceToHost, st_));
+      USAP_CUDA(cudaStreamSynchronize(st_));
+    } else {
+      SortedView v = sb_.view();
+      int nnz = 0;
+      USAP_CUDA(cudaMemcpyAsync(&nnz, sb_.nnz_dev(), sizeof(int), cudaMemcpyDeviceToHost, st_));
+      USAP_CUDA(cudaStreamSynchronize(st_));
+      std::vector<int32_t> rp(B + 1), col(nnz), val(nnz);
+      USAP_CUDA(cudaMemcpyAsync(rp.data(), v.rowptr, sizeof(int32_t) * (B + 1), cudaMemcpyDeviceToHost, st_));
+      USAP_CUDA(cudaMemcpyAsync(col.data(), v.col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st_));
+      USAP_CUDA(cudaMemcpyAsync(val.data(), v.val, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st_));
+      USAP_CUDA(cudaStreamSynchronize(st_));
+      std::memset(M, 0, sizeof(int32_t) * static_cast<size_t>(B) * B);
+      for (int32_t i = 0; i < B; i++)
+        for (int32_t q = rp[i]; q < rp[i + 1]; q++) M[static_cast<size_t>(i) * B + col[q]] = val[q];
+    }
+  }
+  USAP_CUDA(cudaStreamSynchronize(st_));
+}
+
+int64_t Job::op_entropy(const int32_t* part, int32_t B, int32_t dense_max) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  USAP_CUDA(cudaSetDevice(device_));
+  ensure_capacity(B, 1, dense_max, 1);
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  const bool dense = B <= dense_max;
+  prepare_nodal_blocks(slots_[0], B, dense);
+  entropy_launch(slots_[0], B, dense);
+  USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+  return q32_host(model_S(hg_.n, hg_.e, B)) - static_cast<long long>(h_ctl_->entropy_acc);
+}
+
+void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
+                         int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  if (K < 1) throw Error(USAP_ERR_INVALID, "K must be >= 1");
+  USAP_CUDA(cudaSetDevice(device_));
+  ensure_capacity(B, K, 1, 1);
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  merge_phase(slots_[0], B, K, static_cast<uint32_t>(stage), seed);
+  USAP_CUDA(cudaMemcpyAsync(best_s, best_s_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaMemcpyAsync(best_q, best_q_, sizeof(int64_t) * B, cudaMemcpyDeviceToHost, st_));
+  if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, prop_s_, sizeof(int32_t) * B * K, cudaMemcpyDeviceToHost, st_));
+  if (prop_q) USAP_CUDA(cudaMemcpyAsync(prop_q, prop_q_, sizeof(int64_t) * B * K, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+}
+
+void Job::op_merge_apply(int32_t* part, int32_t B, const int32_t* best_s, const int64_t* best_q,
+                         int32_t btm, int32_t* B_new, int32_t* merged) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  USAP_CUDA(cudaSetDevice(device_));
+  for (int32_t i = 0; i < B; i++)
+    if (best_s[i] < 0 || best_s[i] >= B) throw Error(USAP_ERR_INVALID, "best merge target out of range");
+  ensure_capacity(B, 1, 1, 1);
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaMemcpyAsync(best_s_, best_s, sizeof(int32_t) * B, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaMemcpyAsync(best_q_, best_q, sizeof(int64_t) * B, cudaMemcpyHostToDevice, st_));
+  int32_t m = merge_apply(slots_[0], B, btm);
+  USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_.n, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+  *merged = m;
+  *B_new = B - m;
+}
+
+void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t beg, int32_t end,
+                         int32_t itr, int32_t stage, uint64_t seed, int32_t* prop_s, int64_t* prop_q,
+                         int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  if (beg < 0 || end > hg_.n || beg > end) throw Error(USAP_ERR_INVALID, "batch range out of bounds");
+  USAP_CUDA(cudaSetDevice(device_));
+  ensure_capacity(B, 1, dense_max, 1);
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  const bool dense = B <= dense_max;
+  prepare_nodal_blocks(slots_[0], B, dense);
+  USAP_CUDA(cudaMemsetAsync(ctl_, 0, sizeof(NodalCtl), st_));
+  nodal_batch(slots_[0], B, dense, beg, end, static_cast<uint32_t>(itr), static_cast<uint32_t>(stage), seed,
+              true, 2);
+  const int32_t cnt = end - beg;
+  USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_.n, cudaMemcpyDeviceToHost, st_));
+  if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, rp_s_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));
+  if (prop_q) USAP_CUDA(cudaMemcpyAsync(prop_q, rp_q_, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost, st_));
+  if (prop_ninf) USAP_CUDA(cudaMemcpyAsync(prop_ninf, rp_n_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+  if (cum_q) *cum_q = static_cast<int64_t>(h_ctl_->cum_q);
+  if (cum_ninf) *cum_ninf = h_ctl_->cum_ninf;
+  if (moves) *moves = static_cast<int64_t>(h_ctl_->moves);
+}
+
+}  // namespace usap

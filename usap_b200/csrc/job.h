@@ -1,0 +1,132 @@
+// One partitioning job: a graph resident in HBM plus the state of a solve.
+#pragma once
+
+#include <chrono>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/usap.h"
+#include "engine.h"
+
+namespace usap {
+
+struct HostGraph {
+  int32_t n = 0;
+  int64_t e = 0;
+  int64_t wtot = 0;
+  bool unit = true;
+  std::vector<int32_t> src, dst, w;
+  std::vector<int32_t> out_ptr, out_idx, out_w, in_ptr, in_idx, in_w, kout, kin;
+};
+
+// _scc + _dfs_itr (graph_parallel.hpp:514-603), host side
+int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part);
+
+// host evaluation (evaluate.hpp:18-266 scores + NMI + Hungarian accuracy)
+void evaluate_host(const int32_t* truth, const int32_t* given, int64_t n, usap_scores* out);
+
+// _prepare_for_partition_next (graph_parallel.hpp:1322-1365) on slot ids
+struct GoldenPoint {
+  int32_t B = 0;
+  int64_t S = 0;
+  bool finite = false;
+  int32_t slot = -1;
+};
+
+struct Golden {
+  GoldenPoint large, med, small;
+  // returns true when the search is over (answer: med)
+  bool step(int32_t B, int64_t S, int32_t cur_slot, float rate, int32_t* restore_slot,
+            int32_t* btm);
+};
+
+int32_t reduce_blocks(int32_t B, float rate);   // (size_t)_P.B * rate, :340
+double model_S(int64_t n, int64_t e, int32_t B);   // :1314-1316
+long long q32_host(double t);
+
+class Job {
+ public:
+  explicit Job(int device);
+  ~Job();
+  Job(const Job&) = delete;
+  Job& operator=(const Job&) = delete;
+
+  void load(const usap_graph& g);
+  bool loaded() const { return hg_.n > 0; }
+  const HostGraph& host_graph() const { return hg_; }
+  void set_trace(usap_trace_fn fn, void* user) {
+    trace_ = fn;
+    trace_user_ = user;
+  }
+  void partition(const usap_params& p, int32_t* out_assign, usap_result* res);
+
+  // phase-level operations on host buffers
+  int32_t op_scc(int32_t depth, int32_t* part);
+  void op_build(const int32_t* part, int32_t B, int32_t dense_max, int32_t* M, int32_t* dout,
+                int32_t* din);
+  int64_t op_entropy(const int32_t* part, int32_t B, int32_t dense_max);
+  void op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
+                      int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q);
+  void op_merge_apply(int32_t* part, int32_t B, const int32_t* best_s, const int64_t* best_q,
+                      int32_t btm, int32_t* B_new, int32_t* merged);
+  void op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t beg, int32_t end,
+                      int32_t itr, int32_t stage, uint64_t seed, int32_t* prop_s, int64_t* prop_q,
+                      int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves);
+
+  double last_h2d_ms() const { return h2d_ms_; }
+
+ private:
+  void free_graph();
+  void free_state();
+  void ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxitr);
+  // block structures for a nodal phase / batch
+  void prepare_nodal_blocks(const int32_t* part, int32_t B, bool dense);
+  void merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage, uint64_t seed);
+  int32_t merge_apply(int32_t* part, int32_t B, int32_t btm);
+  void entropy_launch(const int32_t* part, int32_t B, bool dense);
+  void nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t itr,
+                   uint32_t stage, uint64_t seed, bool first_of_sweep, int stats);
+  void emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part,
+                  bool dense, long long S_q, int S_ninf, long long cum_q, int cum_ninf,
+                  long long moves);
+  DenseView dense_view() const { return DenseView{M_, Mt_, ld_}; }
+
+  int device_;
+  cudaStream_t st_ = nullptr;
+  HostGraph hg_;
+  GraphDev g_;
+  double h2d_ms_ = 0;
+  // state
+  int32_t bcap_ = 0, kcap_ = 0, dcap_ = 0, icap_ = 0;
+  int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
+  int32_t* move_to_ = nullptr;
+  int32_t *dout_ = nullptr, *din_ = nullptr;
+  int *M_ = nullptr, *Mt_ = nullptr;
+  int ld_ = 0;
+  SortedBuilder sb_;
+  int32_t* prop_s_ = nullptr;
+  long long* prop_q_ = nullptr;
+  int32_t* best_s_ = nullptr;
+  long long* best_q_ = nullptr;
+  unsigned long long *skeys_ = nullptr, *skeys_alt_ = nullptr;
+  int32_t *sidx_ = nullptr, *sidx_alt_ = nullptr;
+  int32_t *union_work_ = nullptr, *root_ = nullptr, *present_ = nullptr, *newlabel_ = nullptr;
+  int32_t* merged_dev_ = nullptr;
+  void* cub_tmp_ = nullptr;
+  size_t cub_bytes_ = 0;
+  NodalCtl* ctl_ = nullptr;
+  NodalCtl* h_ctl_ = nullptr;   // pinned
+  long long* ide_q_ = nullptr;
+  int* ide_n_ = nullptr;
+  int32_t *rp_s_ = nullptr, *rp_n_ = nullptr;   // replay proposal buffers [n]
+  long long* rp_q_ = nullptr;
+  // stats
+  std::vector<cudaEvent_t> ev_pool_;
+  size_t ev_used_ = 0;
+  // trace
+  usap_trace_fn trace_ = nullptr;
+  void* trace_user_ = nullptr;
+  long long trace_prev_moves_ = 0;
+};
+
+}  // namespace usap

@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark: stochastic block partitioning solve of the N=50,000 DC-SBM graph
+(44 planted blocks, within-block fraction 0.5, Dirichlet alpha 1, ~780k
+edges), batch = 10% of N, K = 10 merge proposals per block, on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one full solve (Graph_P::partition: initial blocks, merges,
+batched nodal sweeps, golden-section search) of one graph.  Multi-GPU runs
+are replicas: every rank solves its own graph of the same shape (seed =
+rank); there is no collective on the data path.  Rank 0 prints one JSON
+line.
+
+value  solve time in seconds with the graph already resident in HBM
+       (usap_ctx_partition), timed with CUDA events around the blocking
+       call, L2 flushed (256 MiB write) before every step, max over ranks;
+e2e    the same metric through the one-shot C ABI call usap_partition with
+       host edge arrays in and the host assignment out (CSR build, host to
+       device copies and the device to host read inside the timed region);
+roofline  the nodal proposal kernels (warp-per-vertex + CTA-per-hub), the
+       dominant kernels: algorithmic bytes (per proposing vertex
+       8 + 8 deg + 48 |distinct neighbour blocks| + 48 + 8 * sampled
+       entries) over their CUDA-event time, against the measured copy
+       bandwidth of this B200 pool;
+cpu_baseline  the reference's own partition() (compiled from its sources
+       against the Taskflow-API shim, oracle/_ref/ref_main) on the same
+       graph with all host threads, one full solve.
+
+--impl reference times that reference binary alone (rank 0), K full solves.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SBP solve time at N=50k & MCMC edge-visits/s; batched vs plain at matched NMI"
+WORKLOAD = "dcsbm N=50000 B*=44 within=0.5 alpha=1 (~780k edges), batch 0.1N, K=10"
+REF_MAIN = os.path.join(ROOT, "oracle", "_ref", "ref_main")
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "nodal_propose_c2_traffic.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def graph_for(rank: int):
+    from usap_b200 import generator as gen
+    return gen.generate(gen.config_c2(seed=rank))
+
+
+def solver_params(seed: int = 0, stats: int = 0):
+    from usap_b200 import native as nat
+    return nat.default_params(num_batch_nodal_update=10, seed=seed, stats=stats)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def measured_traffic():
+    try:
+        with open(TRAFFIC) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def reference_solve(G, threads: int, timeout: float = 600.0):
+    """The reference's own partition() on G; returns (seconds, B, partition)."""
+    if not os.path.exists(REF_MAIN):
+        raise FileNotFoundError(f"{REF_MAIN} is not built (make -C oracle ref)")
+    import numpy as np
+    with tempfile.TemporaryDirectory() as td:
+        base = os.path.join(td, "g")
+        G.write_tsv(base)
+        out = os.path.join(td, "p.txt")
+        p = subprocess.run([REF_MAIN, base, str(threads), "10", out], capture_output=True,
+                           text=True, timeout=timeout)
+        if p.returncode != 0:
+            raise RuntimeError(f"ref_main failed: {p.stderr[:300]}")
+        j = json.loads(p.stdout.strip().splitlines()[-1])
+        part = np.loadtxt(out, dtype=np.int64)
+    return j["ms"] / 1000.0, j["B"], part
+
+
+def run_reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return
+    from usap_b200 import generator as gen
+    from usap_b200.api import evaluate
+    threads = os.cpu_count() or 1
+    G = graph_for(0)
+    Gw = gen.generate(gen.config_c1())
+    for _ in range(args.warmup):      # warm the binary and page cache (untimed, N=5000)
+        reference_solve(Gw, threads)
+    times, B, nmi = [], None, None
+    for k in range(args.steps):
+        t, B, part = reference_solve(G, threads)
+        times.append(t)
+        log(f"reference step {k}: {t:.2f} s, B={B}")
+    nmi = evaluate(G.truth, part)["nmi"]
+    v = statistics.mean(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded DC-SBM generator)",
+        "config": {"workload": WORKLOAD, "graph_seed": 0, "num_batch_nodal_update": 10,
+                   "threads": threads},
+        "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference",
+                         "sample": "full partition() of the N=50k graph per step (timed as "
+                                   "main.cpp:54-60 does), reference sources + Taskflow-API shim"},
+        "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "B": B, "nmi": nmi, "step_seconds": times,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local_rank: int):
+    import numpy as np
+    import torch
+    from usap_b200 import api, native as nat
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    G = graph_for(rank)
+    ctx = api.Context(local_rank)
+    ctx.load(G.src, G.dst, None, G.n)
+    params = solver_params(seed=0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        ctx.partition(params, want_assign=False)
+    # --- timed: device-resident solves
+    clocks = ClockSampler(local_rank)
+    barrier()
+    clocks.start()
+    step_ms, results = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, res = ctx.partition(params, want_assign=False)
+        e1.record()
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        results.append(res)
+    barrier()
+    clk = clocks.stop()
+    total_ms = float(sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = total_ms / args.steps / 1000.0
+    res = results[-1]
+    launches = int(sum(r["kernel_launches"] for r in results))
+    visits_per_s = res["edge_visits"] / (statistics.mean(step_ms) / 1000.0)
+
+    # --- end to end through the one-shot C ABI (host arrays in and out)
+    e2e_ms = []
+    e2e_res = None
+    barrier()
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        part, e2e_res = api.partition(G.src, G.dst, None, G.n,
+                                      params=nat.default_params(num_batch_nodal_update=10, seed=0,
+                                                                device=local_rank))
+        e1.record()
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    barrier()
+    e2e_total = float(sum(e2e_ms))
+    if dist is not None:
+        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = e2e_total / args.steps / 1000.0
+    nmi = api.evaluate(G.truth, part)["nmi"]
+
+    # --- roofline of the nodal proposal kernels (instrumented, untimed solve)
+    _, rs = ctx.partition(solver_params(seed=0, stats=1), want_assign=False)
+    peak, peak_kind = hbm_peak()
+    kernel_s = rs["ms_nodal_kernel"] / 1000.0
+    achieved = rs["nodal_kernel_bytes"] / kernel_s / 1e9 if kernel_s > 0 else None
+    per_launch = rs["nodal_kernel_bytes"] / max(1, rs["nodal_kernel_launches"])
+    tr = measured_traffic()
+    traffic = None
+    if tr and "dram_bytes_per_launch" in tr:
+        traffic = tr["dram_bytes_per_launch"]
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "peak_source": peak_kind, "kernel": "nodal propose (warp-per-vertex + hub CTA)",
+                "algorithmic_bytes_per_launch": per_launch,
+                "avg_launch_us": rs["ms_nodal_kernel"] * 1000 / max(1, rs["nodal_kernel_launches"]),
+                "kernel_share_of_solve": rs["ms_nodal_kernel"] / max(1e-9, rs["ms_total"])}
+    ctx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        try:
+            t, B_ref, part_ref = reference_solve(G, threads)
+            cpu = {"value": t, "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": "one full partition() of the same N=50k graph (reference sources "
+                             "+ Taskflow-API shim, timed as main.cpp:54-60)",
+                   "B": int(B_ref), "nmi": api.evaluate(G.truth, part_ref)["nmi"]}
+        except Exception as e:   # reported, not fatal
+            cpu = {"value": None, "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1000, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32 counts, f64 entropy (Q32 sums)",
+        "data": "synthetic (seeded DC-SBM generator)",
+        "config": {"workload": WORKLOAD, "graph_seed": "rank", "num_batch_nodal_update": 10,
+                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before each step",
+                   "init": "SCC/DFS initial blocks (dfs_depth 20)"},
+        "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": int(e2e_res["h2d_bytes"]),
+                "d2h_bytes_per_step": int(e2e_res["d2h_bytes"])},
+        "gpu_launches": launches,
+        "cub_calls": int(sum(r["cub_calls"] for r in results)),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "mcmc_edge_visits_per_s": visits_per_s,
+        "B": res["B"], "S": res["S"], "nmi": nmi, "sweeps": res["sweeps"], "stages": res["stages"],
+        "near_threshold_decisions": res["near_threshold"],
+        "phase_ms": {"init": res["ms_init"], "merge": res["ms_merge"], "nodal": res["ms_nodal"]},
+        "step_ms": step_ms,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="one untimed solve of the workload (for ncu launch lists), no output")
+    args = ap.parse_args()
+    if args.profile:
+        from usap_b200 import api
+        G = graph_for(0)
+        ctx = api.Context(0)
+        ctx.load(G.src, G.dst, None, G.n)
+        ctx.partition(solver_params(seed=0), want_assign=False)
+        ctx.close()
+        return
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and "WORLD_SIZE" in os.environ:
+        log(f"note: WORLD_SIZE={world} overrides --gpus {args.gpus}")
+    if world > 1 and "RANK" not in os.environ:
+        raise SystemExit("--gpus > 1 runs under torchrun (one process per GPU)")
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -91,6 +91,9 @@ typedef struct usap_result {
   double ms_nodal_kernel;  /* stats: summed time of the nodal proposal kernel */
   int64_t nodal_kernel_launches;
   double nodal_kernel_bytes;  /* stats: algorithmic bytes of those launches */
+  int64_t kernel_launches;    /* launches of this library's kernels during the call */
+  int64_t cub_calls;          /* CUB sort/scan/reduce calls during the call */
+  int64_t h2d_bytes, d2h_bytes;  /* host<->device traffic of the call */
 } usap_result;
 
 typedef struct usap_scores {

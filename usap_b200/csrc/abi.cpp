@@ -77,9 +77,13 @@ usap_status usap_partition(const usap_graph* g, const usap_params* p, int32_t* o
     usap_params_default(&def);
     const usap_params& prm = p ? *p : def;
     usap::Job job(prm.device);
+    const auto lc0 = usap::launch_count();
     job.load(*g);
     job.partition(prm, out_assign, out);
     out->ms_h2d = job.last_h2d_ms();
+    out->h2d_bytes += job.last_h2d_bytes();
+    out->kernel_launches = usap::launch_count().kernels - lc0.kernels;
+    out->cub_calls = usap::launch_count().cub - lc0.cub;
   });
 }
 

@@ -36,11 +36,47 @@ class Error : public std::runtime_error {
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
 #define USAP_CUDA(x) ::usap::cuda_check((x), #x, __FILE__, __LINE__)
 
-// Dense block matrix view: M[x*ld + y], transposed copy Mt[y*ld + x].
+// launches of this library's own kernels and of CUB primitives on the
+// calling thread (reported per solve)
+struct LaunchCount {
+  long long kernels = 0;
+  long long cub = 0;
+};
+LaunchCount& launch_count();
+// after each kernel launch of this library: error check + count
+#define USAP_LAUNCHED()                          \
+  do {                                           \
+    USAP_CUDA(cudaGetLastError());               \
+    ::usap::launch_count().kernels++;            \
+  } while (0)
+#define USAP_CUB(x)                              \
+  do {                                           \
+    USAP_CUDA(x);                                \
+    ::usap::launch_count().cub++;                \
+  } while (0)
+
+// Vertices whose degree exceeds kHubDegree are proposed by a whole CTA;
+// its neighbour-block hash holds up to kHubSmemSlots entries in shared
+// memory (3 ints per slot), larger ones use the vertex's global region.
+constexpr int kHubDegree = 128;
+constexpr int kHubSmemSlots = 16384;
+
+// Dense block matrix view: M[x*ld + y], transposed copy Mt[y*ld + x], and
+// per-row chunk sums CS[u*cld + c] of M[u,i]+M[i,u] over blocks
+// i in [128c, 128c+128).
 struct DenseView {
   const int* M;
   const int* Mt;
   int ld;
+  const int* CS;
+  int cld;
+};
+
+// hub vertices of one batch: ids[lo, hi), hash capacity in shared memory
+struct HubList {
+  const int32_t* ids;
+  int lo, hi;
+  int smem_cap;
 };
 
 // Sorted sparse view built from the edge list.
@@ -142,10 +178,14 @@ void launch_merge_union(int B, const int32_t* order, const int32_t* best_s, int 
 void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int32_t* present,
                           int32_t* newlabel, void* cub_tmp, size_t cub_bytes, cudaStream_t st);
 
-void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, cudaStream_t st);
-void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, cudaStream_t st);
+void nodal_configure();
+void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
+                                cudaStream_t st);
+void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,
+                                 cudaStream_t st);
+void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st);
 void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int beg,
-                              int end, int ld, int* M, int* Mt, int32_t* dout, int32_t* din,
+                              int end, int ld, int* M, int* Mt, int cld, int* CS,
                               const NodalCtl* ctl, cudaStream_t st);
 void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
                          int update_degrees, int32_t* dout, int32_t* din, const NodalCtl* ctl,

@@ -16,6 +16,11 @@
 
 namespace usap {
 
+LaunchCount& launch_count() {
+  static thread_local LaunchCount c;
+  return c;
+}
+
 void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
   if (e == cudaSuccess) return;
   int code = (e == cudaErrorMemoryAllocation) ? USAP_ERR_OOM : USAP_ERR_CUDA;
@@ -48,8 +53,6 @@ int hash_lg(int deg) {
   while ((1 << lg) < 2 * deg) lg++;
   return lg;
 }
-
-constexpr int kSharedHashSlots = 256;   // must match kernels_nodal.cu
 
 }  // namespace
 
@@ -110,6 +113,7 @@ Job::Job(int device) : device_(device) {
   if (prop.major < 10)
     throw Error(USAP_ERR_NO_DEVICE, std::string("device is not sm_100 class: ") + prop.name);
   USAP_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  nodal_configure();
   USAP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ctl_), sizeof(NodalCtl)));
   dalloc(&ctl_, 1);
 }
@@ -130,13 +134,15 @@ void Job::free_graph() {
   dfree(g_.in_ptr); dfree(g_.in_idx); dfree(g_.in_w);
   dfree(g_.kout); dfree(g_.kin); dfree(g_.logk);
   dfree(g_.hi_off); dfree(g_.hkey); dfree(g_.hwo); dfree(g_.hwi);
+  dfree(hubs_dev_);
+  hub_ids_.clear();
   g_ = GraphDev{};
 }
 
 void Job::free_state() {
   for (auto& s : slots_) dfree(s);
   dfree(move_to_); dfree(dout_); dfree(din_);
-  dfree(M_); dfree(Mt_);
+  dfree(M_); dfree(Mt_); dfree(CS_);
   sb_.release();
   dfree(prop_s_); dfree(prop_q_); dfree(best_s_); dfree(best_q_);
   dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
@@ -223,13 +229,17 @@ void Job::load(const usap_graph& in) {
   }
   // per-vertex global hash regions for degrees beyond the shared-memory table
   std::vector<int64_t> hi_off(n, -1);
+  std::vector<int32_t> hubs;
   int64_t hi_slots = 0;
   for (int32_t v = 0; v < n; v++) {
     int deg = (h.out_ptr[v + 1] - h.out_ptr[v]) + (h.in_ptr[v + 1] - h.in_ptr[v]);
-    int cap = 1 << hash_lg(deg);
-    if (cap > kSharedHashSlots) {
-      hi_off[v] = hi_slots;
-      hi_slots += cap;
+    if (deg > kHubDegree) {
+      hubs.push_back(v);
+      int cap = 1 << hash_lg(deg);
+      if (cap > kHubSmemSlots) {
+        hi_off[v] = hi_slots;
+        hi_slots += cap;
+      }
     }
   }
   std::vector<double> logk(wtot + 1);
@@ -247,10 +257,12 @@ void Job::load(const usap_graph& in) {
   g.e = h.e;
   g.wtot = wtot;
   g.unit = h.unit;
+  long long up_bytes = 0;
   auto up = [&](int32_t** d, const std::vector<int32_t>& v) {
     dalloc(d, v.size());
     if (!v.empty())
       USAP_CUDA(cudaMemcpyAsync(*d, v.data(), sizeof(int32_t) * v.size(), cudaMemcpyHostToDevice, st_));
+    up_bytes += static_cast<long long>(sizeof(int32_t) * v.size());
   };
   up(&g.src, h.src);
   up(&g.dst, h.dst);
@@ -269,19 +281,42 @@ void Job::load(const usap_graph& in) {
   USAP_CUDA(cudaMemcpyAsync(g.logk, logk.data(), sizeof(double) * logk.size(), cudaMemcpyHostToDevice, st_));
   dalloc(&g.hi_off, n);
   USAP_CUDA(cudaMemcpyAsync(g.hi_off, hi_off.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st_));
+  up_bytes += static_cast<long long>(sizeof(double) * logk.size() + sizeof(int64_t) * n +
+                                     sizeof(int32_t) * hubs.size());
   g.hi_slots = hi_slots;
   dalloc(&g.hkey, hi_slots);
   dalloc(&g.hwo, hi_slots);
   dalloc(&g.hwi, hi_slots);
+  dalloc(&hubs_dev_, hubs.size());
+  if (!hubs.empty())
+    USAP_CUDA(cudaMemcpyAsync(hubs_dev_, hubs.data(), sizeof(int32_t) * hubs.size(), cudaMemcpyHostToDevice, st_));
   USAP_CUDA(cudaEventRecord(e1, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
   float ms = 0;
   USAP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
   h2d_ms_ = ms;
+  h2d_bytes_ = up_bytes;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   g_ = g;
   hg_ = std::move(h);
+  hub_ids_ = std::move(hubs);
+}
+
+HubList Job::hubs_for(int32_t beg, int32_t end, int32_t B) const {
+  HubList hl;
+  hl.ids = hubs_dev_;
+  hl.lo = static_cast<int>(std::lower_bound(hub_ids_.begin(), hub_ids_.end(), beg) - hub_ids_.begin());
+  hl.hi = static_cast<int>(std::lower_bound(hub_ids_.begin(), hub_ids_.end(), end) - hub_ids_.begin());
+  int cap = 32;
+  for (int i = hl.lo; i < hl.hi; i++) {
+    const int32_t v = hub_ids_[i];
+    int deg = (hg_.out_ptr[v + 1] - hg_.out_ptr[v]) + (hg_.in_ptr[v + 1] - hg_.in_ptr[v]);
+    int c = 1 << hash_lg(std::min(deg, B));
+    cap = std::max(cap, c);
+  }
+  hl.smem_cap = std::min(cap, kHubSmemSlots);
+  return hl;
 }
 
 void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxitr) {
@@ -334,8 +369,11 @@ void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxit
   if (ld > dcap_) {
     dfree(M_);
     dfree(Mt_);
+    dfree(CS_);
     dalloc(&M_, static_cast<size_t>(ld) * ld);
     dalloc(&Mt_, static_cast<size_t>(ld) * ld);
+    const int cld = (ld + 127) / 128;
+    dalloc(&CS_, static_cast<size_t>(ld) * cld);
     dcap_ = ld;
   }
   if (maxitr > icap_) {
@@ -352,7 +390,9 @@ void Job::prepare_nodal_blocks(const int32_t* part, int32_t B, bool dense) {
   launch_degrees(g_, part, B, dout_, din_, st_);
   if (dense) {
     ld_ = (B + 3) & ~3;
+    cld_ = (B + 127) / 128;
     launch_dense_build(g_, part, B, ld_, M_, Mt_, st_);
+    launch_chunk_sums(B, dense_view(), CS_, st_);
   } else {
     sb_.build(g_, part, B, false, true, st_);
   }
@@ -378,8 +418,8 @@ void Job::merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage,
 int32_t Job::merge_apply(int32_t* part, int32_t B, int32_t btm) {
   launch_merge_sort_keys(B, best_q_, skeys_, sidx_, st_);
   size_t bytes = cub_bytes_;
-  USAP_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_, bytes, skeys_, skeys_alt_, sidx_, sidx_alt_, B, 0,
-                                            64, st_));
+  USAP_CUB(cub::DeviceRadixSort::SortPairs(cub_tmp_, bytes, skeys_, skeys_alt_, sidx_, sidx_alt_, B, 0,
+                                           64, st_));
   launch_merge_union(B, sidx_alt_, best_s_, btm, union_work_, root_, merged_dev_, st_);
   launch_merge_relabel(hg_.n, B, part, root_, present_, newlabel_, cub_tmp_, cub_bytes_, st_);
   int32_t merged = 0;
@@ -448,10 +488,12 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
     e1 = ev_pool_[ev_used_++];
     USAP_CUDA(cudaEventRecord(e0, st_));
   }
-  if (dense) launch_nodal_propose_dense(a, dense_view(), st_);
-  else launch_nodal_propose_sorted(a, sb_.view(), st_);
+  const HubList hubs = hubs_for(beg, end, B);
+  if (dense) launch_nodal_propose_dense(a, dense_view(), hubs, st_);
+  else launch_nodal_propose_sorted(a, sb_.view(), hubs, st_);
   if (stats == 1) USAP_CUDA(cudaEventRecord(e1, st_));
-  if (dense) launch_nodal_apply_dense(g_, part, move_to_, beg, end, ld_, M_, Mt_, dout_, din_, ctl_, st_);
+  if (dense)
+    launch_nodal_apply_dense(g_, part, move_to_, beg, end, ld_, M_, Mt_, cld_, CS_, ctl_, st_);
   launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, st_);
 }
 
@@ -534,6 +576,8 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   if (bs < 1) bs = 1;
   const int stats = p.stats ? 1 : 0;
   ev_used_ = 0;
+  const LaunchCount lc0 = launch_count();
+  long long d2h = 0;
 
   // initial blocks (host): depth-limited DFS on the transpose, or identity
   std::vector<int32_t> part0(n);
@@ -564,6 +608,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     // merge phase and its application
     merge_phase(part, B, K, stage, seed);
     int32_t merged = merge_apply(part, B, btm);
+    d2h += sizeof(int32_t);
     if (merged < btm) res->merge_shortfall += btm - merged;
     B -= merged;
     auto tm1 = std::chrono::steady_clock::now();
@@ -603,6 +648,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       }
       USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
       USAP_CUDA(cudaStreamSynchronize(st_));
+      d2h += sizeof(NodalCtl);
       if (stats) {
         for (size_t i = ev_mark; i + 1 < ev_used_; i += 2) {
           float ms = 0;
@@ -628,6 +674,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
     USAP_CUDA(cudaStreamSynchronize(st_));
     const long long S_fin = model_q - static_cast<long long>(h_ctl_->entropy_acc);
+    d2h += sizeof(NodalCtl);
     auto tn1 = std::chrono::steady_clock::now();
     ms_nodal += std::chrono::duration<double, std::milli>(tn1 - tm1).count();
     if (trace_) emit_trace(3, stage, 0, 0, B, part, dense, S_fin, 0, 0, 0, 0);
@@ -644,6 +691,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       USAP_CUDA(cudaStreamSynchronize(st_));
       auto td1 = std::chrono::steady_clock::now();
       res->ms_d2h = std::chrono::duration<double, std::milli>(td1 - td0).count();
+      if (out_assign) d2h += static_cast<long long>(sizeof(int32_t)) * n;
       res->B = gs.med.B;
       res->S_q = gs.med.S;
       res->S = static_cast<double>(gs.med.S) / 4294967296.0;
@@ -666,6 +714,10 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   }
   res->ms_merge = ms_merge;
   res->ms_nodal = ms_nodal;
+  res->kernel_launches = launch_count().kernels - lc0.kernels;
+  res->cub_calls = launch_count().cub - lc0.cub;
+  res->h2d_bytes = static_cast<long long>(sizeof(int32_t)) * n;   // initial partition
+  res->d2h_bytes = d2h;
   res->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
 }
 

@@ -74,6 +74,7 @@ class Job {
                       int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves);
 
   double last_h2d_ms() const { return h2d_ms_; }
+  long long last_h2d_bytes() const { return h2d_bytes_; }
 
  private:
   void free_graph();
@@ -89,20 +90,24 @@ class Job {
   void emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part,
                   bool dense, long long S_q, int S_ninf, long long cum_q, int cum_ninf,
                   long long moves);
-  DenseView dense_view() const { return DenseView{M_, Mt_, ld_}; }
+  DenseView dense_view() const { return DenseView{M_, Mt_, ld_, CS_, cld_}; }
+  HubList hubs_for(int32_t beg, int32_t end, int32_t B) const;
 
   int device_;
   cudaStream_t st_ = nullptr;
   HostGraph hg_;
   GraphDev g_;
   double h2d_ms_ = 0;
+  long long h2d_bytes_ = 0;   // bytes uploaded by load()
   // state
   int32_t bcap_ = 0, kcap_ = 0, dcap_ = 0, icap_ = 0;
   int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t* move_to_ = nullptr;
   int32_t *dout_ = nullptr, *din_ = nullptr;
-  int *M_ = nullptr, *Mt_ = nullptr;
-  int ld_ = 0;
+  int *M_ = nullptr, *Mt_ = nullptr, *CS_ = nullptr;
+  int ld_ = 0, cld_ = 0;
+  std::vector<int32_t> hub_ids_;      // vertices of degree > kHubDegree, ascending
+  int32_t* hubs_dev_ = nullptr;
   SortedBuilder sb_;
   int32_t* prop_s_ = nullptr;
   long long* prop_q_ = nullptr;

@@ -185,7 +185,7 @@ void launch_dense_build(const GraphDev& g, const int32_t* part, int B, int ld, i
   USAP_CUDA(cudaMemsetAsync(M, 0, bytes, st));
   USAP_CUDA(cudaMemsetAsync(Mt, 0, bytes, st));
   k_dense_build<<<grid_for(g.e, kThreads), kThreads, 0, st>>>(g.e, g.src, g.dst, g.w, part, ld, M, Mt);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_degrees(const GraphDev& g, const int32_t* part, int B, int32_t* dout, int32_t* din,
@@ -193,14 +193,14 @@ void launch_degrees(const GraphDev& g, const int32_t* part, int B, int32_t* dout
   USAP_CUDA(cudaMemsetAsync(dout, 0, sizeof(int32_t) * B, st));
   USAP_CUDA(cudaMemsetAsync(din, 0, sizeof(int32_t) * B, st));
   k_degrees<<<grid_for(g.n, kThreads), kThreads, 0, st>>>(g.n, part, g.kout, g.kin, dout, din);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_entropy_dense(const GraphDev& g, DenseView v, int B, const int32_t* dout,
                           const int32_t* din, unsigned long long* acc, cudaStream_t st) {
   int64_t cells = static_cast<int64_t>(B) * B;
   k_entropy_dense<<<grid_for(cells, kThreads), kThreads, 0, st>>>(g.logk, v.M, v.ld, B, dout, din, acc);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, int64_t max_nnz,
@@ -208,7 +208,7 @@ void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, 
                            unsigned long long* acc, cudaStream_t st) {
   k_entropy_sorted<<<grid_for(max_nnz, kThreads), kThreads, 0, st>>>(g.logk, nnz_dev, rowof, v.col,
                                                                       v.val, dout, din, acc);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 // --- SortedBuilder --------------------------------------------------------------
@@ -262,11 +262,11 @@ void SortedBuilder::sort_reduce(int64_t count, int B, int kind, cudaStream_t st)
   int n = static_cast<int>(count);
   int bits = key_bits(B);
   size_t bytes = tmp_bytes_;
-  USAP_CUDA(cub::DeviceRadixSort::SortPairs(tmp_, bytes, keys_, keys_alt_, vals_, vals_alt_, n, 0,
-                                            bits, st));
+  USAP_CUB(cub::DeviceRadixSort::SortPairs(tmp_, bytes, keys_, keys_alt_, vals_, vals_alt_, n, 0,
+                                           bits, st));
   bytes = tmp_bytes_;
-  USAP_CUDA(cub::DeviceReduce::ReduceByKey(tmp_, bytes, keys_alt_, ukeys_, vals_alt_, uvals_,
-                                           nruns_ + kind, cuda::std::plus<int>{}, n, st));
+  USAP_CUB(cub::DeviceReduce::ReduceByKey(tmp_, bytes, keys_alt_, ukeys_, vals_alt_, uvals_,
+                                          nruns_ + kind, cuda::std::plus<int>{}, n, st));
 }
 
 void SortedBuilder::build(const GraphDev& g, const int32_t* part, int B, bool with_csc, bool with_sym,
@@ -276,25 +276,28 @@ void SortedBuilder::build(const GraphDev& g, const int32_t* part, int B, bool wi
   int ogrid = grid_for(2 * g.e, kThreads);
   // row view
   k_make_keys<<<grid, kThreads, 0, st>>>(g.e, g.src, g.dst, g.w, part, B, 0, keys_, vals_);
+  USAP_LAUNCHED();
   sort_reduce(g.e, B, 0, st);
   k_offsets<<<grid, kThreads, 0, st>>>(ukeys_, uvals_, nruns_ + 0, B, rowptr_, col_, val_, rowof_, nnz_ + 0);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
   has_csc_ = with_csc;
   if (with_csc) {
     k_make_keys<<<grid, kThreads, 0, st>>>(g.e, g.src, g.dst, g.w, part, B, 1, keys_, vals_);
+    USAP_LAUNCHED();
     sort_reduce(g.e, B, 1, st);
     k_offsets<<<grid, kThreads, 0, st>>>(ukeys_, uvals_, nruns_ + 1, B, colptr_, crow_, cval_,
                                          nullptr, nnz_ + 1);
-    USAP_CUDA(cudaGetLastError());
+    USAP_LAUNCHED();
   }
   if (with_sym) {
     k_make_keys<<<grid, kThreads, 0, st>>>(g.e, g.src, g.dst, g.w, part, B, 2, keys_, vals_);
+    USAP_LAUNCHED();
     sort_reduce(2 * g.e, B, 2, st);
     k_offsets<<<ogrid, kThreads, 0, st>>>(ukeys_, uvals_, nruns_ + 2, B, symptr_, symcol_, nullptr,
                                           nullptr, nnz_ + 2);
-    USAP_CUDA(cudaGetLastError());
+    USAP_LAUNCHED();
     size_t bytes = tmp_bytes_;
-    USAP_CUDA(cub::DeviceScan::InclusiveSum(tmp_, bytes, uvals_, symcum_, static_cast<int>(2 * g.e), st));
+    USAP_CUB(cub::DeviceScan::InclusiveSum(tmp_, bytes, uvals_, symcum_, static_cast<int>(2 * g.e), st));
   }
 }
 

@@ -289,19 +289,19 @@ void launch_merge_propose(const GraphDev& g, SortedView v, const MergeArgs& a, c
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (blocks < 1) blocks = 1;
   k_merge_propose<<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_merge_argmin(int B, int K, const int32_t* prop_s, const long long* prop_q, int32_t* best_s,
                          long long* best_q, cudaStream_t st) {
   k_merge_argmin<<<(B + 255) / 256, 256, 0, st>>>(B, K, prop_s, prop_q, best_s, best_q);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_merge_union(int B, const int32_t* order, const int32_t* best_s, int btm, int32_t* work,
                         int32_t* root, int32_t* merged, cudaStream_t st) {
   k_merge_union<<<1, 1024, 0, st>>>(B, order, best_s, btm, work, root, merged);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int32_t* present,
@@ -310,18 +310,18 @@ void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int3
   int grid = (n + 255) / 256;
   if (grid > 148 * 8) grid = 148 * 8;
   k_present<<<grid, 256, 0, st>>>(n, part, root, present);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
   size_t bytes = cub_bytes;
-  USAP_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp, bytes, present, newlabel, B, st));
+  USAP_CUB(cub::DeviceScan::ExclusiveSum(cub_tmp, bytes, present, newlabel, B, st));
   k_relabel<<<grid, 256, 0, st>>>(n, part, root, newlabel);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 // exposed for the engine: keys for the stable (dS, block) sort
 void launch_merge_sort_keys(int B, const long long* best_q, unsigned long long* keys, int32_t* idx,
                             cudaStream_t st) {
   k_sort_keys<<<(B + 255) / 256, 256, 0, st>>>(B, best_q, keys, idx);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 }  // namespace usap

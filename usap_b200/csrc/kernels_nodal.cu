@@ -6,19 +6,23 @@
 // scratch rows are cleared and scanned); the update task (:433-458) applies
 // the buffered moves, rebuilds M from scratch and tests convergence.
 //
-// Here one warp proposes for one vertex.  Its neighbour blocks are
-// aggregated in a per-warp open-addressed hash in shared memory (or, for
-// vertices whose degree does not fit, in a per-vertex region of global
-// memory), so dS costs O(deg) lookups: each distinct neighbour block b gives
-// the changed entries M[r,b], M[s,b] (out-neighbours) or M[b,r], M[b,s]
-// (in-neighbours); the entries a move leaves unchanged contribute
-// count * (log new degree - log old degree), with the counts known exactly
-// from the degrees.  The reference's rule that in-edges from blocks r and s
-// do not adjust the 2x2 row entries (the adjustment is commented out at
-// :1135-1142) and that column sums skip i in {r,s} is kept.  Accepted moves
-// are written to move_to[]; a second kernel applies them to the dense tile
-// by +/-w deltas (exact integers, so order does not matter), a third commits
-// the partition.  The convergence bookkeeping of the update task runs in a
+// Here one warp proposes for one vertex (one CTA for vertices of degree
+// above kHubDegree, so a hub does not set the batch's tail).  The target is
+// drawn in block-id order: on the dense tile through per-row chunk sums of
+// M[u,:]+M[:,u] (chunks of 128 blocks, kept current by the same delta
+// updates as M), on the sparse views by binary search of cumulative counts.
+// The vertex's neighbour blocks are aggregated in an open-addressed hash in
+// shared memory (global memory for the largest hubs), so dS costs O(deg)
+// lookups: each distinct neighbour block b gives the changed entries
+// M[r,b], M[s,b] (out-neighbours) or M[b,r], M[b,s] (in-neighbours); the
+// entries a move leaves unchanged contribute count * (log new degree - log
+// old degree), with the counts known exactly from the degrees.  The
+// reference's rule that in-edges from blocks r and s do not adjust the 2x2
+// row entries (the adjustment is commented out at :1135-1142) and that
+// column sums skip i in {r,s} is kept.  Accepted moves are written to
+// move_to[]; a second kernel applies them to the dense tile by +/-w deltas
+// (exact integers, so order does not matter), a third commits the
+// partition.  The convergence bookkeeping of the update task runs in a
 // one-thread kernel so batches and sweeps queue without host round trips.
 #include <cmath>
 
@@ -31,7 +35,8 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kHCap = 256;   // shared-memory hash slots per warp
+constexpr int kHCap = 256;          // shared-memory hash slots per warp
+constexpr int kChunk = 128;         // blocks per chunk sum of a dense row
 
 struct DenseOps {
   DenseView v;
@@ -39,25 +44,50 @@ struct DenseOps {
   __device__ __forceinline__ int get(int x, int y) const {
     return __ldg(v.M + static_cast<long long>(x) * v.ld + y);
   }
-  // first block i (block-id order) whose cumulative M[u,i]+M[i,u] exceeds t
+  // first block i (block-id order) whose cumulative M[u,i]+M[i,u] exceeds t:
+  // a warp scan over the row's chunk sums, then over the 128 entries of the
+  // chosen chunk (4 per lane, 16-byte loads; rows are padded to ld, a
+  // multiple of 4, with zeros)
   __device__ __forceinline__ int sym_sample(int u, long long t, int lane, int* scanned) const {
-    const int* rowM = v.M + static_cast<long long>(u) * v.ld;
-    const int* rowT = v.Mt + static_cast<long long>(u) * v.ld;
+    const int nch = (B + kChunk - 1) / kChunk;
+    const int* cs = v.CS + static_cast<long long>(u) * v.cld;
     long long run = 0;
-    for (int base = 0; base < B; base += 32) {
-      int i = base + lane;
-      int val = i < B ? __ldg(rowM + i) + __ldg(rowT + i) : 0;
-      int incl = warp_incl_scan(val, lane);
-      int total = __shfl_sync(0xffffffffu, incl, 31);
+    int c = nch - 1;
+    for (int base = 0; base < nch; base += 32) {
+      const int cc = base + lane;
+      const int val = cc < nch ? __ldg(cs + cc) : 0;
+      const int incl = warp_incl_scan(val, lane);
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
       if (run + total > t) {
-        unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
-        *scanned += base + 32;
-        return base + __ffs(m) - 1;
+        const unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
+        const int l = __ffs(m) - 1;
+        c = base + l;
+        run += __shfl_sync(0xffffffffu, incl - val, l);
+        break;
       }
       run += total;
     }
-    *scanned += B;
-    return B - 1;
+    const int i0 = c * kChunk + lane * 4;
+    int p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+    if (i0 < B) {
+      const int4 a = __ldg(reinterpret_cast<const int4*>(v.M + static_cast<long long>(u) * v.ld + i0));
+      const int4 b = __ldg(reinterpret_cast<const int4*>(v.Mt + static_cast<long long>(u) * v.ld + i0));
+      p0 = a.x + b.x;
+      p1 = p0 + a.y + b.y;
+      p2 = p1 + a.z + b.z;
+      p3 = p2 + a.w + b.w;
+    }
+    const int incl = warp_incl_scan(p3, lane);
+    const long long before = run + incl - p3;
+    const unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
+    const int l = m ? __ffs(m) - 1 : 31;
+    int k = 3;
+    if (before + p0 > t) k = 0;
+    else if (before + p1 > t) k = 1;
+    else if (before + p2 > t) k = 2;
+    *scanned += nch + kChunk;
+    int i = c * kChunk + l * 4 + __shfl_sync(0xffffffffu, k, l);
+    return i < B ? i : B - 1;
   }
 };
 
@@ -93,6 +123,159 @@ __device__ __forceinline__ int table_lookup_wo(const int* key, const int* wo, in
   }
 }
 
+__device__ __forceinline__ void table_insert(int* key, int* two, int* twi, int cap, int lg, int b,
+                                             int ww, bool is_out) {
+  unsigned h = hash_slot(b, lg);
+  while (true) {
+    int prev = atomicCAS(key + h, -1, b);
+    if (prev == -1 || prev == b) break;
+    h = (h + 1) & (cap - 1);
+  }
+  atomicAdd(is_out ? two + h : twi + h, ww);
+}
+
+struct VertexInfo {
+  int r;
+  long long kout, kin;
+  int o0, dego, i0, degi;
+};
+
+__device__ __forceinline__ VertexInfo vertex_info(const NodalArgs& a, int v) {
+  VertexInfo vi;
+  vi.r = __ldg(a.part + v);
+  vi.kout = __ldg(a.kout + v);
+  vi.kin = __ldg(a.kin + v);
+  vi.o0 = __ldg(a.out_ptr + v);
+  vi.dego = __ldg(a.out_ptr + v + 1) - vi.o0;
+  vi.i0 = __ldg(a.in_ptr + v);
+  vi.degi = __ldg(a.in_ptr + v + 1) - vi.i0;
+  return vi;
+}
+
+// target block of the proposal for v (warp-collective: all 32 lanes)
+template <class Ops>
+__device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops, int v,
+                                              const VertexInfo& vi, int lane, int* scanned) {
+  const int B = a.B;
+  const Draws x = philox(static_cast<uint32_t>(v), a.itr, a.stage, kTagNodal, a.seed);
+  const long long k = vi.kout + vi.kin;
+  if (k == 0) return static_cast<int>(draw_below(x.x2, B));
+  const long long t = draw_below(x.x0, k);
+  const int deg = vi.dego + vi.degi;
+  int j;
+  if (a.unit) {
+    j = static_cast<int>(t);
+  } else {   // weighted: first neighbour whose cumulative weight exceeds t
+    long long run = 0;
+    j = deg - 1;
+    for (int base = 0; base < deg; base += 32) {
+      const int jj = base + lane;
+      long long ww = 0;
+      if (jj < deg) ww = jj < vi.dego ? __ldg(a.out_w + vi.o0 + jj) : __ldg(a.in_w + vi.i0 + jj - vi.dego);
+      const long long incl = warp_incl_scan_ll(ww, lane);
+      const long long total = __shfl_sync(0xffffffffu, incl, 31);
+      if (run + total > t) {
+        const unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
+        j = base + __ffs(m) - 1;
+        break;
+      }
+      run += total;
+    }
+  }
+  const int nbr = j < vi.dego ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
+  const int u = __ldg(a.part + nbr);
+  const long long dau = static_cast<long long>(__ldg(a.dout + u)) + __ldg(a.din + u);
+  if (accept_uniform(x.x1, dau, B)) return static_cast<int>(draw_below(x.x2, B));
+  return ops.sym_sample(u, draw_below(x.x2, dau), lane, scanned);
+}
+
+struct TermSums {
+  long long acc;
+  int sXR, sXS, sYR, sYS, nb;
+};
+
+// dS terms of one aggregated neighbour block b (b not in {r, s})
+template <class Ops>
+__device__ __forceinline__ void slot_terms(const NodalArgs& a, const Ops& ops, int r, int s, int b,
+                                           int wo, int wi, long long dr_out, long long ds_out,
+                                           long long dr_in, long long ds_in, long long dr_out_n,
+                                           long long ds_out_n, long long dr_in_n, long long ds_in_n,
+                                           TermSums& ts) {
+  if (wo > 0) {
+    const int R = ops.get(r, b), S = ops.get(s, b);
+    const long long dinb = __ldg(a.din + b);
+    ts.acc += q32(g_term(a.L, R, dinb, dr_out));
+    ts.acc += q32(g_term(a.L, S, dinb, ds_out));
+    ts.acc -= q32(g_term(a.L, R - wo, dinb, dr_out_n));
+    ts.acc -= q32(g_term(a.L, S + wo, dinb, ds_out_n));
+    ts.sXR += R;
+    ts.sXS += S;
+  }
+  if (wi > 0) {
+    const int Rc = ops.get(b, r), Sc = ops.get(b, s);
+    const long long doutb = __ldg(a.dout + b);
+    ts.acc += q32(g_term(a.L, Rc, dr_in, doutb));
+    ts.acc += q32(g_term(a.L, Sc, ds_in, doutb));
+    ts.acc -= q32(g_term(a.L, Rc - wi, dr_in_n, doutb));
+    ts.acc -= q32(g_term(a.L, Sc + wi, ds_in_n, doutb));
+    ts.sYR += Rc;
+    ts.sYS += Sc;
+  }
+}
+
+// 2x2 and unchanged-entry terms, the accept rule (dS < 0, -inf included)
+// and the outputs; one thread
+template <class Ops>
+__device__ __forceinline__ void finalize(const NodalArgs& a, const Ops& ops, int v, int r, int s,
+                                         const VertexInfo& vi, TermSums ts, long long wor,
+                                         long long wos, long long Rr, long long Rs, long long Sr,
+                                         long long Ss, int scanned, unsigned long long* my_bytes) {
+  const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
+  const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
+  const long long dr_out_n = dr_out - vi.kout, ds_out_n = ds_out + vi.kout;
+  const long long dr_in_n = dr_in - vi.kin, ds_in_n = ds_in + vi.kin;
+  long long acc = ts.acc;
+  acc += q32(g_term(a.L, Rr, dr_in, dr_out));
+  acc += q32(g_term(a.L, Rs, ds_in, dr_out));
+  acc += q32(g_term(a.L, Sr, dr_in, ds_out));
+  acc += q32(g_term(a.L, Ss, ds_in, ds_out));
+  int ninf = 0;
+  const double nt[4] = {g_term(a.L, Rr - wor, dr_in_n, dr_out_n), g_term(a.L, Rs - wos, ds_in_n, dr_out_n),
+                        g_term(a.L, Sr + wor, dr_in_n, ds_out_n), g_term(a.L, Ss + wos, ds_in_n, ds_out_n)};
+#pragma unroll
+  for (int t = 0; t < 4; t++) {
+    if (isinf(nt[t])) ninf = 1;
+    else acc -= q32(nt[t]);
+  }
+  acc += q32(coef_term(a.L, dr_out - Rr - Rs - ts.sXR, dr_out_n, dr_out));
+  acc += q32(coef_term(a.L, ds_out - Sr - Ss - ts.sXS, ds_out_n, ds_out));
+  acc += q32(coef_term(a.L, dr_in - Rr - Sr - ts.sYR, dr_in_n, dr_in));
+  acc += q32(coef_term(a.L, ds_in - Rs - Ss - ts.sYS, ds_in_n, ds_in));
+  const bool accept = ninf || acc < 0;
+  if (a.prop_s) {
+    a.prop_s[v - a.beg] = s;
+    a.prop_q[v - a.beg] = acc;
+    a.prop_ninf[v - a.beg] = ninf;
+  }
+  if (accept) {
+    a.move_to[v] = s;
+    if (ninf) atomicOr(&a.ctl->cum_ninf, 1);
+    else atomicAdd(&a.ctl->cum_q, static_cast<unsigned long long>(acc));
+    atomicAdd(&a.ctl->moves, 1ull);
+  }
+  if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&a.ctl->near, 1ull);
+  if (a.stats) *my_bytes += 8 + 8ull * (vi.dego + vi.degi) + 48ull * ts.nb + 48 + 8ull * scanned;
+}
+
+__device__ __forceinline__ void record_stay(const NodalArgs& a, int v) {
+  if (a.prop_s) {
+    a.prop_s[v - a.beg] = -1;
+    a.prop_q[v - a.beg] = 0;
+    a.prop_ninf[v - a.beg] = 0;
+  }
+}
+
+// one warp per vertex of degree <= kHubDegree
 template <class Ops>
 __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops) {
   __shared__ int s_key[kWarps][kHCap];
@@ -101,75 +284,27 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
   if (*reinterpret_cast<volatile int*>(&a.ctl->done)) return;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nwarps = gridDim.x * kWarps;
-  const int B = a.B;
   unsigned long long my_bytes = 0;
   for (int v = a.beg + blockIdx.x * kWarps + wib; v < a.end; v += nwarps) {
-    const int r = __ldg(a.part + v);
-    const long long kout = __ldg(a.kout + v), kin = __ldg(a.kin + v);
-    const long long k = kout + kin;
-    const int o0 = __ldg(a.out_ptr + v), dego = __ldg(a.out_ptr + v + 1) - o0;
-    const int i0 = __ldg(a.in_ptr + v), degi = __ldg(a.in_ptr + v + 1) - i0;
-    const int deg = dego + degi;
-    Draws x = philox(static_cast<uint32_t>(v), a.itr, a.stage, kTagNodal, a.seed);
-    int s;
+    const VertexInfo vi = vertex_info(a, v);
+    const int deg = vi.dego + vi.degi;
+    if (deg > kHubDegree) continue;   // handled by k_nodal_propose_hub
     int scanned = 0;
-    if (k == 0) {
-      s = static_cast<int>(draw_below(x.x2, B));
-    } else {
-      long long t = draw_below(x.x0, k);
-      int j;
-      if (a.unit) {
-        j = static_cast<int>(t);
-      } else {   // weighted: first neighbour whose cumulative weight exceeds t
-        long long run = 0;
-        j = deg - 1;
-        for (int base = 0; base < deg; base += 32) {
-          int jj = base + lane;
-          long long ww = 0;
-          if (jj < deg) ww = jj < dego ? __ldg(a.out_w + o0 + jj) : __ldg(a.in_w + i0 + jj - dego);
-          long long incl = warp_incl_scan_ll(ww, lane);
-          long long total = __shfl_sync(0xffffffffu, incl, 31);
-          if (run + total > t) {
-            unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
-            j = base + __ffs(m) - 1;
-            break;
-          }
-          run += total;
-        }
-      }
-      const int nbr = j < dego ? __ldg(a.out_idx + o0 + j) : __ldg(a.in_idx + i0 + j - dego);
-      const int u = __ldg(a.part + nbr);
-      const long long dau = static_cast<long long>(__ldg(a.dout + u)) + __ldg(a.din + u);
-      if (accept_uniform(x.x1, dau, B)) {
-        s = static_cast<int>(draw_below(x.x2, B));
-      } else {
-        s = ops.sym_sample(u, draw_below(x.x2, dau), lane, &scanned);
-      }
-    }
+    const int r = vi.r;
+    const int s = propose_target(a, ops, v, vi, lane, &scanned);
     if (s == r) {
-      if (a.prop_s && lane == 0) {
-        a.prop_s[v - a.beg] = -1;
-        a.prop_q[v - a.beg] = 0;
-        a.prop_ninf[v - a.beg] = 0;
+      if (lane == 0) {
+        record_stay(a, v);
+        if (a.stats) my_bytes += 8 + 8ull * deg + 8ull * scanned;
       }
-      if (a.stats && lane == 0) my_bytes += 8 + 8ull * deg + 8ull * scanned;
       continue;
     }
-    // --- aggregate the neighbour blocks: wo[b] (out-edges), wi[b] (in-edges)
     int lg = 5;
     while ((1 << lg) < 2 * deg) lg++;
-    const int cap = 1 << lg;
-    int *key, *two, *twi;
-    if (cap <= kHCap) {
-      key = s_key[wib];
-      two = s_wo[wib];
-      twi = s_wi[wib];
-    } else {
-      long long off = __ldg(a.hi_off + v);
-      key = a.hkey + off;
-      two = a.hwo + off;
-      twi = a.hwi + off;
-    }
+    const int cap = 1 << lg;   // <= kHCap since deg <= kHubDegree
+    int* key = s_key[wib];
+    int* two = s_wo[wib];
+    int* twi = s_wi[wib];
     for (int i = lane; i < cap; i += 32) {
       key[i] = -1;
       two[i] = 0;
@@ -177,60 +312,29 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
     }
     __syncwarp();
     for (int j = lane; j < deg; j += 32) {
-      const bool is_out = j < dego;
-      const int nb = is_out ? __ldg(a.out_idx + o0 + j) : __ldg(a.in_idx + i0 + j - dego);
-      const int ww = a.unit ? 1 : (is_out ? __ldg(a.out_w + o0 + j) : __ldg(a.in_w + i0 + j - dego));
-      const int b = __ldg(a.part + nb);
-      unsigned h = hash_slot(b, lg);
-      while (true) {
-        int prev = atomicCAS(key + h, -1, b);
-        if (prev == -1 || prev == b) break;
-        h = (h + 1) & (cap - 1);
-      }
-      atomicAdd(is_out ? two + h : twi + h, ww);
+      const bool is_out = j < vi.dego;
+      const int nb = is_out ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
+      const int ww = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
+      table_insert(key, two, twi, cap, lg, __ldg(a.part + nb), ww, is_out);
     }
     __syncwarp();
-    // --- dS terms over the distinct neighbour blocks other than r and s
     const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
     const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
-    const long long dr_out_n = dr_out - kout, ds_out_n = ds_out + kout;
-    const long long dr_in_n = dr_in - kin, ds_in_n = ds_in + kin;
-    long long acc = 0;
-    int sXR = 0, sXS = 0, sYR = 0, sYS = 0, nb_distinct = 0;
+    TermSums ts{0, 0, 0, 0, 0, 0};
     for (int i = lane; i < cap; i += 32) {
       const int b = key[i];
       if (b < 0) continue;
-      nb_distinct++;
+      ts.nb++;
       if (b == r || b == s) continue;
-      const int wo = two[i], wi = twi[i];
-      if (wo > 0) {
-        const int R = ops.get(r, b), S = ops.get(s, b);
-        const long long dinb = __ldg(a.din + b);
-        acc += q32(g_term(a.L, R, dinb, dr_out));
-        acc += q32(g_term(a.L, S, dinb, ds_out));
-        acc -= q32(g_term(a.L, R - wo, dinb, dr_out_n));
-        acc -= q32(g_term(a.L, S + wo, dinb, ds_out_n));
-        sXR += R;
-        sXS += S;
-      }
-      if (wi > 0) {
-        const int Rc = ops.get(b, r), Sc = ops.get(b, s);
-        const long long doutb = __ldg(a.dout + b);
-        acc += q32(g_term(a.L, Rc, dr_in, doutb));
-        acc += q32(g_term(a.L, Sc, ds_in, doutb));
-        acc -= q32(g_term(a.L, Rc - wi, dr_in_n, doutb));
-        acc -= q32(g_term(a.L, Sc + wi, ds_in_n, doutb));
-        sYR += Rc;
-        sYS += Sc;
-      }
+      slot_terms(a, ops, r, s, b, two[i], twi[i], dr_out, ds_out, dr_in, ds_in, dr_out - vi.kout,
+                 ds_out + vi.kout, dr_in - vi.kin, ds_in + vi.kin, ts);
     }
-    acc = warp_sum_ll(acc);
-    sXR = warp_sum_i(sXR);
-    sXS = warp_sum_i(sXS);
-    sYR = warp_sum_i(sYR);
-    sYS = warp_sum_i(sYS);
-    nb_distinct = warp_sum_i(nb_distinct);
-    // 2x2 entries, fetched by four lanes
+    ts.acc = warp_sum_ll(ts.acc);
+    ts.sXR = warp_sum_i(ts.sXR);
+    ts.sXS = warp_sum_i(ts.sXS);
+    ts.sYR = warp_sum_i(ts.sYR);
+    ts.sYS = warp_sum_i(ts.sYS);
+    ts.nb = warp_sum_i(ts.nb);
     int e4 = 0;
     if (lane < 4) e4 = ops.get(lane < 2 ? r : s, (lane & 1) ? s : r);
     const long long Rr = __shfl_sync(0xffffffffu, e4, 0), Rs = __shfl_sync(0xffffffffu, e4, 1);
@@ -238,40 +342,152 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
     if (lane == 0) {
       const long long wor = table_lookup_wo(key, two, cap, lg, r);
       const long long wos = table_lookup_wo(key, two, cap, lg, s);
-      acc += q32(g_term(a.L, Rr, dr_in, dr_out));
-      acc += q32(g_term(a.L, Rs, ds_in, dr_out));
-      acc += q32(g_term(a.L, Sr, dr_in, ds_out));
-      acc += q32(g_term(a.L, Ss, ds_in, ds_out));
-      int ninf = 0;
-      const double nt[4] = {g_term(a.L, Rr - wor, dr_in_n, dr_out_n), g_term(a.L, Rs - wos, ds_in_n, dr_out_n),
-                            g_term(a.L, Sr + wor, dr_in_n, ds_out_n), g_term(a.L, Ss + wos, ds_in_n, ds_out_n)};
-#pragma unroll
-      for (int t = 0; t < 4; t++) {
-        if (isinf(nt[t])) ninf = 1;
-        else acc -= q32(nt[t]);
-      }
-      acc += q32(coef_term(a.L, dr_out - Rr - Rs - sXR, dr_out_n, dr_out));
-      acc += q32(coef_term(a.L, ds_out - Sr - Ss - sXS, ds_out_n, ds_out));
-      acc += q32(coef_term(a.L, dr_in - Rr - Sr - sYR, dr_in_n, dr_in));
-      acc += q32(coef_term(a.L, ds_in - Rs - Ss - sYS, ds_in_n, ds_in));
-      const bool accept = ninf || acc < 0;
-      if (a.prop_s) {
-        a.prop_s[v - a.beg] = s;
-        a.prop_q[v - a.beg] = acc;
-        a.prop_ninf[v - a.beg] = ninf;
-      }
-      if (accept) {
-        a.move_to[v] = s;
-        if (ninf) atomicOr(&a.ctl->cum_ninf, 1);
-        else atomicAdd(&a.ctl->cum_q, static_cast<unsigned long long>(acc));
-        atomicAdd(&a.ctl->moves, 1ull);
-      }
-      if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&a.ctl->near, 1ull);
-      if (a.stats) my_bytes += 8 + 8ull * deg + 48ull * nb_distinct + 48 + 8ull * scanned;
+      finalize(a, ops, v, r, s, vi, ts, wor, wos, Rr, Rs, Sr, Ss, scanned, &my_bytes);
     }
     __syncwarp();
   }
   if (a.stats && lane == 0 && my_bytes) atomicAdd(&a.ctl->bytes, my_bytes);
+}
+
+// one CTA per vertex of degree > kHubDegree; the hash holds at most
+// min(deg, B) distinct blocks and lives in dynamic shared memory
+// (`smem_cap` slots) or, beyond that, in the vertex's global region
+template <class Ops>
+__global__ void __launch_bounds__(kThreads) k_nodal_propose_hub(NodalArgs a, Ops ops, const int32_t* hubs,
+                                                               int hub_lo, int hub_hi, int smem_cap) {
+  extern __shared__ int dyn[];
+  __shared__ long long s_acc[kWarps];
+  __shared__ int s_sum[5][kWarps];
+  __shared__ int s_target, s_scanned;
+  if (*reinterpret_cast<volatile int*>(&a.ctl->done)) return;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  unsigned long long my_bytes = 0;
+  for (int h = hub_lo + blockIdx.x; h < hub_hi; h += gridDim.x) {
+    const int v = __ldg(hubs + h);
+    const VertexInfo vi = vertex_info(a, v);
+    const int deg = vi.dego + vi.degi;
+    const int r = vi.r;
+    if (wib == 0) {
+      int scanned = 0;
+      const int s = propose_target(a, ops, v, vi, lane, &scanned);
+      if (lane == 0) {
+        s_target = s;
+        s_scanned = scanned;
+      }
+    }
+    __syncthreads();
+    const int s = s_target;
+    if (s == r) {
+      if (threadIdx.x == 0) {
+        record_stay(a, v);
+        if (a.stats) my_bytes += 8 + 8ull * deg + 8ull * s_scanned;
+      }
+      __syncthreads();
+      continue;
+    }
+    const int distinct_max = deg < a.B ? deg : a.B;
+    int lg = 5;
+    while ((1 << lg) < 2 * distinct_max) lg++;
+    const int cap = 1 << lg;
+    int *key, *two, *twi;
+    if (cap <= smem_cap) {
+      key = dyn;
+      two = dyn + smem_cap;
+      twi = dyn + 2 * smem_cap;
+    } else {
+      const long long off = __ldg(a.hi_off + v);
+      key = a.hkey + off;
+      two = a.hwo + off;
+      twi = a.hwi + off;
+    }
+    for (int i = threadIdx.x; i < cap; i += kThreads) {
+      key[i] = -1;
+      two[i] = 0;
+      twi[i] = 0;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < deg; j += kThreads) {
+      const bool is_out = j < vi.dego;
+      const int nb = is_out ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
+      const int ww = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
+      table_insert(key, two, twi, cap, lg, __ldg(a.part + nb), ww, is_out);
+    }
+    __syncthreads();
+    const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
+    const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
+    TermSums ts{0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < cap; i += kThreads) {
+      const int b = key[i];
+      if (b < 0) continue;
+      ts.nb++;
+      if (b == r || b == s) continue;
+      slot_terms(a, ops, r, s, b, two[i], twi[i], dr_out, ds_out, dr_in, ds_in, dr_out - vi.kout,
+                 ds_out + vi.kout, dr_in - vi.kin, ds_in + vi.kin, ts);
+    }
+    ts.acc = warp_sum_ll(ts.acc);
+    ts.sXR = warp_sum_i(ts.sXR);
+    ts.sXS = warp_sum_i(ts.sXS);
+    ts.sYR = warp_sum_i(ts.sYR);
+    ts.sYS = warp_sum_i(ts.sYS);
+    ts.nb = warp_sum_i(ts.nb);
+    if (lane == 0) {
+      s_acc[wib] = ts.acc;
+      s_sum[0][wib] = ts.sXR;
+      s_sum[1][wib] = ts.sXS;
+      s_sum[2][wib] = ts.sYR;
+      s_sum[3][wib] = ts.sYS;
+      s_sum[4][wib] = ts.nb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      TermSums tot{0, 0, 0, 0, 0, 0};
+      for (int w = 0; w < kWarps; w++) {
+        tot.acc += s_acc[w];
+        tot.sXR += s_sum[0][w];
+        tot.sXS += s_sum[1][w];
+        tot.sYR += s_sum[2][w];
+        tot.sYS += s_sum[3][w];
+        tot.nb += s_sum[4][w];
+      }
+      const long long Rr = ops.get(r, r), Rs = ops.get(r, s), Sr = ops.get(s, r), Ss = ops.get(s, s);
+      const long long wor = table_lookup_wo(key, two, cap, lg, r);
+      const long long wos = table_lookup_wo(key, two, cap, lg, s);
+      finalize(a, ops, v, r, s, vi, tot, wor, wos, Rr, Rs, Sr, Ss, s_scanned, &my_bytes);
+    }
+    __syncthreads();
+  }
+  if (a.stats && threadIdx.x == 0 && my_bytes) atomicAdd(&a.ctl->bytes, my_bytes);
+}
+
+// chunk sums CS[u][c] = sum over the chunk's blocks i of M[u,i] + M[i,u]
+__global__ void __launch_bounds__(kThreads) k_chunk_sums(int B, int ld, const int* __restrict__ M,
+                                                        const int* __restrict__ Mt, int cld,
+                                                        int* __restrict__ CS) {
+  const int lane = threadIdx.x & 31;
+  const int nch = (B + kChunk - 1) / kChunk;
+  const long long items = static_cast<long long>(B) * nch;
+  const long long nwarps = static_cast<long long>(gridDim.x) * kWarps;
+  for (long long it = static_cast<long long>(blockIdx.x) * kWarps + (threadIdx.x >> 5); it < items;
+       it += nwarps) {
+    const int u = static_cast<int>(it / nch), c = static_cast<int>(it - static_cast<long long>(u) * nch);
+    const int i0 = c * kChunk + lane * 4;
+    int sum = 0;
+    if (i0 < B) {
+      const int4 a = *reinterpret_cast<const int4*>(M + static_cast<long long>(u) * ld + i0);
+      const int4 b = *reinterpret_cast<const int4*>(Mt + static_cast<long long>(u) * ld + i0);
+      sum = a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;
+    }
+    sum = warp_sum_i(sum);
+    if (lane == 0) CS[static_cast<long long>(u) * cld + c] = sum;
+  }
+}
+
+// M[x,y] += w, keeping Mt and the chunk sums of rows x and y in step
+__device__ __forceinline__ void dense_add(int* M, int* Mt, int* CS, int ld, int cld, int x, int y, int w) {
+  atomicAdd(M + static_cast<long long>(x) * ld + y, w);
+  atomicAdd(Mt + static_cast<long long>(y) * ld + x, w);
+  atomicAdd(CS + static_cast<long long>(x) * cld + y / kChunk, w);
+  atomicAdd(CS + static_cast<long long>(y) * cld + x / kChunk, w);
 }
 
 // Apply accepted moves of [beg, end) to the dense tile by deltas.  An edge
@@ -281,7 +497,7 @@ __global__ void __launch_bounds__(kThreads) k_nodal_apply_dense(
     const int32_t* __restrict__ out_w, const int32_t* __restrict__ in_ptr,
     const int32_t* __restrict__ in_idx, const int32_t* __restrict__ in_w,
     const int32_t* __restrict__ part, const int32_t* __restrict__ move_to, int beg, int end, int ld,
-    int* __restrict__ M, int* __restrict__ Mt, const NodalCtl* ctl) {
+    int* __restrict__ M, int* __restrict__ Mt, int cld, int* __restrict__ CS, const NodalCtl* ctl) {
   const int lane = threadIdx.x & 31;
   const int nwarps = gridDim.x * kWarps;
   for (int v = beg + blockIdx.x * kWarps + (threadIdx.x >> 5); v < end; v += nwarps) {
@@ -295,10 +511,8 @@ __global__ void __launch_bounds__(kThreads) k_nodal_apply_dense(
       const int oy = part[y];
       const int my = move_to[y];
       const int ny = my >= 0 ? my : oy;
-      atomicAdd(M + static_cast<long long>(r) * ld + oy, -w);
-      atomicAdd(Mt + static_cast<long long>(oy) * ld + r, -w);
-      atomicAdd(M + static_cast<long long>(s) * ld + ny, w);
-      atomicAdd(Mt + static_cast<long long>(ny) * ld + s, w);
+      dense_add(M, Mt, CS, ld, cld, r, oy, -w);
+      dense_add(M, Mt, CS, ld, cld, s, ny, w);
     }
     const int i0 = in_ptr[v], i1 = in_ptr[v + 1];
     for (int p = i0 + lane; p < i1; p += 32) {
@@ -306,10 +520,8 @@ __global__ void __launch_bounds__(kThreads) k_nodal_apply_dense(
       if (move_to[y] >= 0) continue;
       const int w = in_w ? in_w[p] : 1;
       const int oy = part[y];
-      atomicAdd(M + static_cast<long long>(oy) * ld + r, -w);
-      atomicAdd(Mt + static_cast<long long>(r) * ld + oy, -w);
-      atomicAdd(M + static_cast<long long>(oy) * ld + s, w);
-      atomicAdd(Mt + static_cast<long long>(s) * ld + oy, w);
+      dense_add(M, Mt, CS, ld, cld, oy, r, -w);
+      dense_add(M, Mt, CS, ld, cld, oy, s, w);
     }
   }
 }
@@ -378,35 +590,63 @@ __global__ void k_ctl_batch_end(NodalCtl* ctl, int itr, int W, double thr, long 
 }
 
 template <class Ops>
-void launch_propose(const NodalArgs& a, Ops ops, cudaStream_t st) {
-  int count = a.end - a.beg;
+void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, cudaStream_t st) {
+  const int count = a.end - a.beg;
   if (count <= 0) return;
   int blocks = (count + kWarps - 1) / kWarps;
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_nodal_propose<Ops><<<blocks, kThreads, 0, st>>>(a, ops);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
+  if (hubs.hi > hubs.lo) {
+    const size_t smem = sizeof(int) * 3 * static_cast<size_t>(hubs.smem_cap);
+    k_nodal_propose_hub<Ops><<<hubs.hi - hubs.lo, kThreads, smem, st>>>(a, ops, hubs.ids, hubs.lo,
+                                                                        hubs.hi, hubs.smem_cap);
+    USAP_LAUNCHED();
+  }
 }
 
 }  // namespace
 
-void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, cudaStream_t st) {
-  launch_propose(a, DenseOps{v, a.B}, st);
+void nodal_configure() {
+  static bool done = false;
+  if (done) return;
+  const int smem = static_cast<int>(sizeof(int) * 3 * kHubSmemSlots);
+  USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<DenseOps>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<SortedOps>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  done = true;
 }
 
-void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, cudaStream_t st) {
-  launch_propose(a, SortedOps{v, a.B}, st);
+void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs, cudaStream_t st) {
+  launch_propose(a, DenseOps{v, a.B}, hubs, st);
+}
+
+void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs, cudaStream_t st) {
+  launch_propose(a, SortedOps{v, a.B}, hubs, st);
+}
+
+void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st) {
+  const int nch = (B + kChunk - 1) / kChunk;
+  long long items = static_cast<long long>(B) * nch;
+  long long blocks = (items + kWarps - 1) / kWarps;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  if (blocks < 1) blocks = 1;
+  k_chunk_sums<<<static_cast<int>(blocks), kThreads, 0, st>>>(B, v.ld, v.M, v.Mt, v.cld, CS);
+  USAP_LAUNCHED();
 }
 
 void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int beg,
-                              int end, int ld, int* M, int* Mt, int32_t* dout, int32_t* din,
-                              const NodalCtl* ctl, cudaStream_t st) {
+                              int end, int ld, int* M, int* Mt, int cld, int* CS, const NodalCtl* ctl,
+                              cudaStream_t st) {
   int count = end - beg;
   if (count <= 0) return;
   int blocks = (count + kWarps - 1) / kWarps;
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_nodal_apply_dense<<<blocks, kThreads, 0, st>>>(g.out_ptr, g.out_idx, g.out_w, g.in_ptr, g.in_idx,
-                                                  g.in_w, part, move_to, beg, end, ld, M, Mt, ctl);
-  USAP_CUDA(cudaGetLastError());
+                                                  g.in_w, part, move_to, beg, end, ld, M, Mt, cld, CS,
+                                                  ctl);
+  USAP_LAUNCHED();
 }
 
 void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
@@ -418,19 +658,19 @@ void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_nodal_commit<<<blocks, 256, 0, st>>>(part, move_to, g.kout, g.kin, beg, end, update_degrees, dout,
                                          din);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int W, const long long* ide_q,
                             const int* ide_n, cudaStream_t st) {
   k_ctl_sweep_start<<<1, 1, 0, st>>>(ctl, model_q, itr, W, ide_q, ide_n);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 void launch_ctl_batch_end(NodalCtl* ctl, int itr, int W, double thr, long long* ide_q, int* ide_n,
                           long long batch_vertices, long long batch_edges, cudaStream_t st) {
   k_ctl_batch_end<<<1, 1, 0, st>>>(ctl, itr, W, thr, ide_q, ide_n, batch_vertices, batch_edges);
-  USAP_CUDA(cudaGetLastError());
+  USAP_LAUNCHED();
 }
 
 }  // namespace usap

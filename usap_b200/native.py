@@ -53,7 +53,8 @@ class Result(C.Structure):
                 ("ms_total", C.c_double), ("ms_init", C.c_double), ("ms_merge", C.c_double),
                 ("ms_nodal", C.c_double), ("ms_h2d", C.c_double), ("ms_d2h", C.c_double),
                 ("ms_nodal_kernel", C.c_double), ("nodal_kernel_launches", C.c_int64),
-                ("nodal_kernel_bytes", C.c_double)]
+                ("nodal_kernel_bytes", C.c_double), ("kernel_launches", C.c_int64),
+                ("cub_calls", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
 
 
 class Scores(C.Structure):

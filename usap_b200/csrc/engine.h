@@ -79,6 +79,22 @@ struct HubList {
   int smem_cap;
 };
 
+// main stream plus a side stream for kernels that overlap it
+struct StreamPair {
+  cudaStream_t main, side;
+  cudaEvent_t fork, join;
+};
+
+// batch-end bookkeeping, run by the commit kernel (active = 1)
+struct CtlArgs {
+  int active;
+  int itr, W;
+  double thr;
+  long long* ide_q;
+  int* ide_n;
+  long long batch_vertices, batch_edges;
+};
+
 // Sorted sparse view built from the edge list.
 struct SortedView {
   const int* rowptr;  // [B+1]
@@ -120,6 +136,7 @@ struct GraphDev {
   int32_t *src = nullptr, *dst = nullptr, *w = nullptr;
   int32_t *out_ptr = nullptr, *out_idx = nullptr, *out_w = nullptr;
   int32_t *in_ptr = nullptr, *in_idx = nullptr, *in_w = nullptr;
+  int32_t *out_src = nullptr, *in_dst = nullptr;   // owner vertex of each CSR position
   int32_t *kout = nullptr, *kin = nullptr;
   double* logk = nullptr;
   // per-vertex global hash region for vertices too large for shared memory
@@ -180,21 +197,18 @@ void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int3
 
 void nodal_configure();
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
-                                cudaStream_t st);
+                                const StreamPair& sp);
 void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,
-                                 cudaStream_t st);
+                                 const StreamPair& sp);
 void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st);
-void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int beg,
-                              int end, int ld, int* M, int* Mt, int cld, int* CS,
-                              const NodalCtl* ctl, cudaStream_t st);
+void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int o0,
+                              int n_out, int i0, int n_in, int ld, int* M, int* Mt, int cld, int* CS,
+                              cudaStream_t st);
 void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
-                         int update_degrees, int32_t* dout, int32_t* din, const NodalCtl* ctl,
-                         cudaStream_t st);
+                         int update_degrees, int32_t* dout, int32_t* din, NodalCtl* ctl,
+                         const CtlArgs& c, cudaStream_t st);
 void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int W,
                             const long long* ide_q, const int* ide_n, cudaStream_t st);
-void launch_ctl_batch_end(NodalCtl* ctl, int itr, int W, double thr, long long* ide_q,
-                          int* ide_n, long long batch_vertices, long long batch_edges,
-                          cudaStream_t st);
 void launch_merge_sort_keys(int B, const long long* best_q, unsigned long long* keys, int32_t* idx,
                             cudaStream_t st);
 

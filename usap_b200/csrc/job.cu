@@ -113,6 +113,9 @@ Job::Job(int device) : device_(device) {
   if (prop.major < 10)
     throw Error(USAP_ERR_NO_DEVICE, std::string("device is not sm_100 class: ") + prop.name);
   USAP_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  USAP_CUDA(cudaStreamCreateWithFlags(&st_side_, cudaStreamNonBlocking));
+  USAP_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+  USAP_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
   nodal_configure();
   USAP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ctl_), sizeof(NodalCtl)));
   dalloc(&ctl_, 1);
@@ -125,6 +128,9 @@ Job::~Job() {
   dfree(ctl_);
   if (h_ctl_) cudaFreeHost(h_ctl_);
   for (auto e : ev_pool_) cudaEventDestroy(e);
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
+  if (st_side_) cudaStreamDestroy(st_side_);
   if (st_) cudaStreamDestroy(st_);
 }
 
@@ -132,6 +138,7 @@ void Job::free_graph() {
   dfree(g_.src); dfree(g_.dst); dfree(g_.w);
   dfree(g_.out_ptr); dfree(g_.out_idx); dfree(g_.out_w);
   dfree(g_.in_ptr); dfree(g_.in_idx); dfree(g_.in_w);
+  dfree(g_.out_src); dfree(g_.in_dst);
   dfree(g_.kout); dfree(g_.kin); dfree(g_.logk);
   dfree(g_.hi_off); dfree(g_.hkey); dfree(g_.hwo); dfree(g_.hwi);
   dfree(hubs_dev_);
@@ -277,6 +284,15 @@ void Job::load(const usap_graph& in) {
   up(&g.in_idx, h.in_idx);
   up(&g.kout, h.kout);
   up(&g.kin, h.kin);
+  {
+    std::vector<int32_t> osrc(h.e), idst(h.e);
+    for (int32_t v = 0; v < n; v++) {
+      for (int32_t p = h.out_ptr[v]; p < h.out_ptr[v + 1]; p++) osrc[p] = v;
+      for (int32_t p = h.in_ptr[v]; p < h.in_ptr[v + 1]; p++) idst[p] = v;
+    }
+    up(&g.out_src, osrc);
+    up(&g.in_dst, idst);
+  }
   dalloc(&g.logk, logk.size());
   USAP_CUDA(cudaMemcpyAsync(g.logk, logk.data(), sizeof(double) * logk.size(), cudaMemcpyHostToDevice, st_));
   dalloc(&g.hi_off, n);
@@ -440,7 +456,8 @@ void Job::entropy_launch(const int32_t* part, int32_t B, bool dense) {
 }
 
 void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t itr,
-                      uint32_t stage, uint64_t seed, bool first_of_sweep, int stats) {
+                      uint32_t stage, uint64_t seed, bool first_of_sweep, int stats,
+                      const CtlArgs& ctl_args) {
   if (!dense && !first_of_sweep) sb_.build(g_, part, B, false, true, st_);
   NodalArgs a;
   a.out_ptr = g_.out_ptr;
@@ -489,12 +506,15 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
     USAP_CUDA(cudaEventRecord(e0, st_));
   }
   const HubList hubs = hubs_for(beg, end, B);
-  if (dense) launch_nodal_propose_dense(a, dense_view(), hubs, st_);
-  else launch_nodal_propose_sorted(a, sb_.view(), hubs, st_);
+  if (dense) launch_nodal_propose_dense(a, dense_view(), hubs, streams());
+  else launch_nodal_propose_sorted(a, sb_.view(), hubs, streams());
   if (stats == 1) USAP_CUDA(cudaEventRecord(e1, st_));
-  if (dense)
-    launch_nodal_apply_dense(g_, part, move_to_, beg, end, ld_, M_, Mt_, cld_, CS_, ctl_, st_);
-  launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, st_);
+  if (dense) {
+    const int o0 = hg_.out_ptr[beg], i0 = hg_.in_ptr[beg];
+    launch_nodal_apply_dense(g_, part, move_to_, o0, hg_.out_ptr[end] - o0, i0, hg_.in_ptr[end] - i0, ld_,
+                             M_, Mt_, cld_, CS_, st_);
+  }
+  launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, ctl_args, st_);
 }
 
 void Job::emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part, bool dense,
@@ -632,10 +652,10 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       size_t ev_mark = ev_used_;
       for (int32_t beg = 0; beg < n; beg += bs) {
         const int32_t end = beg + bs < n ? beg + bs : n;
-        nodal_batch(part, B, dense, beg, end, itr, stage, seed, beg == 0, stats);
         const long long edges = (static_cast<long long>(hg_.out_ptr[end]) - hg_.out_ptr[beg]) +
                                 (static_cast<long long>(hg_.in_ptr[end]) - hg_.in_ptr[beg]);
-        launch_ctl_batch_end(ctl_, itr, W, thr, ide_q_, ide_n_, end - beg, edges, st_);
+        const CtlArgs ca{1, itr, W, thr, ide_q_, ide_n_, end - beg, edges};
+        nodal_batch(part, B, dense, beg, end, itr, stage, seed, beg == 0, stats, ca);
         if (trace_) {
           USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
           USAP_CUDA(cudaStreamSynchronize(st_));
@@ -817,8 +837,9 @@ void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t be
   const bool dense = B <= dense_max;
   prepare_nodal_blocks(slots_[0], B, dense);
   USAP_CUDA(cudaMemsetAsync(ctl_, 0, sizeof(NodalCtl), st_));
+  const CtlArgs ca{0, 0, 1, 0.0, ide_q_, ide_n_, 0, 0};
   nodal_batch(slots_[0], B, dense, beg, end, static_cast<uint32_t>(itr), static_cast<uint32_t>(stage), seed,
-              true, 2);
+              true, 2, ca);
   const int32_t cnt = end - beg;
   USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_.n, cudaMemcpyDeviceToHost, st_));
   if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, rp_s_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));

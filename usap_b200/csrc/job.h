@@ -86,15 +86,20 @@ class Job {
   int32_t merge_apply(int32_t* part, int32_t B, int32_t btm);
   void entropy_launch(const int32_t* part, int32_t B, bool dense);
   void nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t itr,
-                   uint32_t stage, uint64_t seed, bool first_of_sweep, int stats);
+                   uint32_t stage, uint64_t seed, bool first_of_sweep, int stats,
+                   const CtlArgs& ctl_args);
   void emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part,
                   bool dense, long long S_q, int S_ninf, long long cum_q, int cum_ninf,
                   long long moves);
   DenseView dense_view() const { return DenseView{M_, Mt_, ld_, CS_, cld_}; }
   HubList hubs_for(int32_t beg, int32_t end, int32_t B) const;
 
+  StreamPair streams() const { return StreamPair{st_, st_side_, ev_fork_, ev_join_}; }
+
   int device_;
   cudaStream_t st_ = nullptr;
+  cudaStream_t st_side_ = nullptr;   // hub CTAs overlap the warp kernel here
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   HostGraph hg_;
   GraphDev g_;
   double h2d_ms_ = 0;

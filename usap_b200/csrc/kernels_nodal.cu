@@ -26,8 +26,13 @@
 // one-thread kernel so batches and sweeps queue without host round trips.
 #include <cmath>
 
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
 #include "common.cuh"
 #include "engine.h"
+
+namespace cg = cooperative_groups;
 
 namespace usap {
 
@@ -281,8 +286,10 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
   __shared__ int s_key[kWarps][kHCap];
   __shared__ int s_wo[kWarps][kHCap];
   __shared__ int s_wi[kWarps][kHCap];
+  __shared__ int s_list[kWarps][kHubDegree];   // occupied slots other than r, s
   if (*reinterpret_cast<volatile int*>(&a.ctl->done)) return;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const unsigned lanes_below = (1u << lane) - 1u;
   const int nwarps = gridDim.x * kWarps;
   unsigned long long my_bytes = 0;
   for (int v = a.beg + blockIdx.x * kWarps + wib; v < a.end; v += nwarps) {
@@ -320,13 +327,23 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
     __syncwarp();
     const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
     const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
+    // compact the occupied slots so that each lane takes about one block
+    int nlist = 0, noccupied = 0;
+    for (int base = 0; base < cap; base += 32) {
+      const int i = base + lane;
+      const int b = i < cap ? key[i] : -1;
+      const unsigned occ = __ballot_sync(0xffffffffu, b >= 0);
+      const bool use = b >= 0 && b != r && b != s;
+      const unsigned mu = __ballot_sync(0xffffffffu, use);
+      if (use) s_list[wib][nlist + __popc(mu & lanes_below)] = i;
+      nlist += __popc(mu);
+      noccupied += __popc(occ);
+    }
+    __syncwarp();
     TermSums ts{0, 0, 0, 0, 0, 0};
-    for (int i = lane; i < cap; i += 32) {
-      const int b = key[i];
-      if (b < 0) continue;
-      ts.nb++;
-      if (b == r || b == s) continue;
-      slot_terms(a, ops, r, s, b, two[i], twi[i], dr_out, ds_out, dr_in, ds_in, dr_out - vi.kout,
+    for (int t = lane; t < nlist; t += 32) {
+      const int i = s_list[wib][t];
+      slot_terms(a, ops, r, s, key[i], two[i], twi[i], dr_out, ds_out, dr_in, ds_in, dr_out - vi.kout,
                  ds_out + vi.kout, dr_in - vi.kin, ds_in + vi.kin, ts);
     }
     ts.acc = warp_sum_ll(ts.acc);
@@ -334,7 +351,7 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
     ts.sXS = warp_sum_i(ts.sXS);
     ts.sYR = warp_sum_i(ts.sYR);
     ts.sYS = warp_sum_i(ts.sYS);
-    ts.nb = warp_sum_i(ts.nb);
+    ts.nb = noccupied;
     int e4 = 0;
     if (lane < 4) e4 = ops.get(lane < 2 ? r : s, (lane & 1) ? s : r);
     const long long Rr = __shfl_sync(0xffffffffu, e4, 0), Rs = __shfl_sync(0xffffffffu, e4, 1);
@@ -482,46 +499,74 @@ __global__ void __launch_bounds__(kThreads) k_chunk_sums(int B, int ld, const in
   }
 }
 
-// M[x,y] += w, keeping Mt and the chunk sums of rows x and y in step
-__device__ __forceinline__ void dense_add(int* M, int* Mt, int* CS, int ld, int cld, int x, int y, int w) {
-  atomicAdd(M + static_cast<long long>(x) * ld + y, w);
-  atomicAdd(Mt + static_cast<long long>(y) * ld + x, w);
-  atomicAdd(CS + static_cast<long long>(x) * cld + y / kChunk, w);
-  atomicAdd(CS + static_cast<long long>(y) * cld + x / kChunk, w);
+// Sum of `val` over the lanes of `active` that hold the same key; *lead is
+// set on one lane per key.
+__device__ __forceinline__ int group_sum(unsigned active, long long key, int val, int lane, bool* lead) {
+  const unsigned peers = __match_any_sync(active, key);
+  *lead = (__ffs(peers) - 1) == lane;
+  return __reduce_add_sync(peers, val);
 }
 
-// Apply accepted moves of [beg, end) to the dense tile by deltas.  An edge
-// between two moved vertices is handled once, from its source's out-list.
+// M[x,y] += w, keeping Mt and the chunk sums of rows x and y in step.
+// Lanes that update the same cell (or the same chunk sum) are summed first,
+// so a moved vertex with many edges into one block issues one atomic per
+// distinct target per warp.
+__device__ __forceinline__ void dense_add(unsigned active, int lane, int* M, int* Mt, int* CS, int ld,
+                                          int cld, int x, int y, int w) {
+  bool lead;
+  int sum = group_sum(active, static_cast<long long>(x) * ld + y, w, lane, &lead);
+  if (lead) {
+    atomicAdd(M + static_cast<long long>(x) * ld + y, sum);
+    atomicAdd(Mt + static_cast<long long>(y) * ld + x, sum);
+  }
+  sum = group_sum(active, static_cast<long long>(x) * cld + y / kChunk, w, lane, &lead);
+  if (lead) atomicAdd(CS + static_cast<long long>(x) * cld + y / kChunk, sum);
+  sum = group_sum(active, static_cast<long long>(y) * cld + x / kChunk, w, lane, &lead);
+  if (lead) atomicAdd(CS + static_cast<long long>(y) * cld + x / kChunk, sum);
+}
+
+// Apply the accepted moves of a batch to the dense tile by deltas, one
+// thread per edge of the batch: positions [0, n_out) walk the batch's
+// out-edges (CSR positions o0 + i, owner out_src), [n_out, n_out + n_in)
+// its in-edges (positions i0 + i, owner in_dst).  An edge between two moved
+// vertices is applied once, from its source's out-list.
 __global__ void __launch_bounds__(kThreads) k_nodal_apply_dense(
-    const int32_t* __restrict__ out_ptr, const int32_t* __restrict__ out_idx,
-    const int32_t* __restrict__ out_w, const int32_t* __restrict__ in_ptr,
+    const int32_t* __restrict__ out_src, const int32_t* __restrict__ out_idx,
+    const int32_t* __restrict__ out_w, const int32_t* __restrict__ in_dst,
     const int32_t* __restrict__ in_idx, const int32_t* __restrict__ in_w,
-    const int32_t* __restrict__ part, const int32_t* __restrict__ move_to, int beg, int end, int ld,
-    int* __restrict__ M, int* __restrict__ Mt, int cld, int* __restrict__ CS, const NodalCtl* ctl) {
+    const int32_t* __restrict__ part, const int32_t* __restrict__ move_to, int o0, int n_out, int i0,
+    int n_in, int ld, int* __restrict__ M, int* __restrict__ Mt, int cld, int* __restrict__ CS) {
   const int lane = threadIdx.x & 31;
-  const int nwarps = gridDim.x * kWarps;
-  for (int v = beg + blockIdx.x * kWarps + (threadIdx.x >> 5); v < end; v += nwarps) {
-    const int s = move_to[v];
-    if (s < 0) continue;
-    const int r = part[v];
-    const int o0 = out_ptr[v], o1 = out_ptr[v + 1];
-    for (int p = o0 + lane; p < o1; p += 32) {
-      const int y = out_idx[p];
-      const int w = out_w ? out_w[p] : 1;
-      const int oy = part[y];
-      const int my = move_to[y];
-      const int ny = my >= 0 ? my : oy;
-      dense_add(M, Mt, CS, ld, cld, r, oy, -w);
-      dense_add(M, Mt, CS, ld, cld, s, ny, w);
+  const long long total = static_cast<long long>(n_out) + n_in;
+  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+  for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
+       base < total; base += stride) {
+    const long long t = base + lane;
+    const bool is_out = t < n_out;
+    bool valid = t < total;
+    int v = 0, y = 0, w = 1, s = -1;
+    if (valid) {
+      const int pos = is_out ? o0 + static_cast<int>(t) : i0 + static_cast<int>(t - n_out);
+      v = is_out ? __ldg(out_src + pos) : __ldg(in_dst + pos);
+      s = move_to[v];
+      y = is_out ? __ldg(out_idx + pos) : __ldg(in_idx + pos);
+      if (is_out ? out_w != nullptr : in_w != nullptr) w = is_out ? __ldg(out_w + pos) : __ldg(in_w + pos);
     }
-    const int i0 = in_ptr[v], i1 = in_ptr[v + 1];
-    for (int p = i0 + lane; p < i1; p += 32) {
-      const int y = in_idx[p];
-      if (move_to[y] >= 0) continue;
-      const int w = in_w ? in_w[p] : 1;
+    const int my = valid ? move_to[y] : -1;
+    valid = valid && s >= 0 && (is_out || my < 0);
+    const unsigned act_out = __ballot_sync(0xffffffffu, valid && is_out);
+    const unsigned act_in = __ballot_sync(0xffffffffu, valid && !is_out);
+    if (valid) {
+      const int r = part[v];
       const int oy = part[y];
-      dense_add(M, Mt, CS, ld, cld, oy, r, -w);
-      dense_add(M, Mt, CS, ld, cld, oy, s, w);
+      if (is_out) {
+        const int ny = my >= 0 ? my : oy;
+        dense_add(act_out, lane, M, Mt, CS, ld, cld, r, oy, -w);
+        dense_add(act_out, lane, M, Mt, CS, ld, cld, s, ny, w);
+      } else {
+        dense_add(act_in, lane, M, Mt, CS, ld, cld, oy, r, -w);
+        dense_add(act_in, lane, M, Mt, CS, ld, cld, oy, s, w);
+      }
     }
   }
 }
@@ -529,7 +574,34 @@ __global__ void __launch_bounds__(kThreads) k_nodal_apply_dense(
 __global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__ move_to,
                                const int32_t* __restrict__ kout, const int32_t* __restrict__ kin,
                                int beg, int end, int update_degrees, int32_t* __restrict__ dout,
-                               int32_t* __restrict__ din) {
+                               int32_t* __restrict__ din, NodalCtl* ctl, CtlArgs c);
+
+// update (:433-458), second half: the sweep's cumulative dS is recorded for
+// this sweep and added to S after every batch (as the reference does), then
+// the convergence test -mean < thr * S ends the nodal phase
+__device__ __forceinline__ void ctl_batch_end(NodalCtl* ctl, const CtlArgs& c) {
+  if (ctl->done) return;
+  const long long cum = static_cast<long long>(ctl->cum_q);
+  c.ide_q[c.itr] = cum;
+  c.ide_n[c.itr] = ctl->cum_ninf;
+  ctl->S_q += cum;
+  ctl->S_ninf |= ctl->cum_ninf;
+  ctl->batches++;
+  ctl->proposals += c.batch_vertices;
+  ctl->edge_visits += c.batch_edges;
+  if (c.itr >= c.W - 1) {
+    double S_d = ctl->S_ninf ? -INFINITY : static_cast<double>(ctl->S_q) / kQ32;
+    if (-ctl->mean < c.thr * S_d) ctl->done = 1;
+  }
+}
+
+// commits the batch's moves (degrees, partition) and runs the batch-end
+// bookkeeping in one launch; the bookkeeping reads only the control block
+__global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__ move_to,
+                               const int32_t* __restrict__ kout, const int32_t* __restrict__ kin,
+                               int beg, int end, int update_degrees, int32_t* __restrict__ dout,
+                               int32_t* __restrict__ din, NodalCtl* ctl, CtlArgs c) {
+  if (c.active && blockIdx.x == 0 && threadIdx.x == 0) ctl_batch_end(ctl, c);
   int stride = gridDim.x * blockDim.x;
   for (int v = beg + blockIdx.x * blockDim.x + threadIdx.x; v < end; v += stride) {
     const int s = move_to[v];
@@ -569,39 +641,27 @@ __global__ void k_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int
   ctl->sweeps++;
 }
 
-// update (:433-458): the sweep's cumulative dS is recorded for this sweep
-// and added to S after every batch (as the reference does), then the
-// convergence test -mean < thr * S ends the nodal phase
-__global__ void k_ctl_batch_end(NodalCtl* ctl, int itr, int W, double thr, long long* ide_q,
-                                int* ide_n, long long batch_vertices, long long batch_edges) {
-  if (ctl->done) return;
-  const long long cum = static_cast<long long>(ctl->cum_q);
-  ide_q[itr] = cum;
-  ide_n[itr] = ctl->cum_ninf;
-  ctl->S_q += cum;
-  ctl->S_ninf |= ctl->cum_ninf;
-  ctl->batches++;
-  ctl->proposals += batch_vertices;
-  ctl->edge_visits += batch_edges;
-  if (itr >= W - 1) {
-    double S_d = ctl->S_ninf ? -INFINITY : static_cast<double>(ctl->S_q) / kQ32;
-    if (-ctl->mean < thr * S_d) ctl->done = 1;
-  }
-}
-
+// the hub CTAs run on a second stream, concurrently with the warp kernel
 template <class Ops>
-void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, cudaStream_t st) {
+void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const StreamPair& sp) {
   const int count = a.end - a.beg;
   if (count <= 0) return;
+  const bool has_hubs = hubs.hi > hubs.lo;
+  if (has_hubs) {
+    USAP_CUDA(cudaEventRecord(sp.fork, sp.main));
+    USAP_CUDA(cudaStreamWaitEvent(sp.side, sp.fork, 0));
+    const size_t smem = sizeof(int) * 3 * static_cast<size_t>(hubs.smem_cap);
+    k_nodal_propose_hub<Ops><<<hubs.hi - hubs.lo, kThreads, smem, sp.side>>>(a, ops, hubs.ids, hubs.lo,
+                                                                             hubs.hi, hubs.smem_cap);
+    USAP_LAUNCHED();
+  }
   int blocks = (count + kWarps - 1) / kWarps;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  k_nodal_propose<Ops><<<blocks, kThreads, 0, st>>>(a, ops);
+  k_nodal_propose<Ops><<<blocks, kThreads, 0, sp.main>>>(a, ops);
   USAP_LAUNCHED();
-  if (hubs.hi > hubs.lo) {
-    const size_t smem = sizeof(int) * 3 * static_cast<size_t>(hubs.smem_cap);
-    k_nodal_propose_hub<Ops><<<hubs.hi - hubs.lo, kThreads, smem, st>>>(a, ops, hubs.ids, hubs.lo,
-                                                                        hubs.hi, hubs.smem_cap);
-    USAP_LAUNCHED();
+  if (has_hubs) {
+    USAP_CUDA(cudaEventRecord(sp.join, sp.side));
+    USAP_CUDA(cudaStreamWaitEvent(sp.main, sp.join, 0));
   }
 }
 
@@ -618,12 +678,14 @@ void nodal_configure() {
   done = true;
 }
 
-void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs, cudaStream_t st) {
-  launch_propose(a, DenseOps{v, a.B}, hubs, st);
+void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
+                                const StreamPair& sp) {
+  launch_propose(a, DenseOps{v, a.B}, hubs, sp);
 }
 
-void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs, cudaStream_t st) {
-  launch_propose(a, SortedOps{v, a.B}, hubs, st);
+void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,
+                                 const StreamPair& sp) {
+  launch_propose(a, SortedOps{v, a.B}, hubs, sp);
 }
 
 void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st) {
@@ -636,28 +698,28 @@ void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st) {
   USAP_LAUNCHED();
 }
 
-void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int beg,
-                              int end, int ld, int* M, int* Mt, int cld, int* CS, const NodalCtl* ctl,
+void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int o0,
+                              int n_out, int i0, int n_in, int ld, int* M, int* Mt, int cld, int* CS,
                               cudaStream_t st) {
-  int count = end - beg;
-  if (count <= 0) return;
-  int blocks = (count + kWarps - 1) / kWarps;
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  k_nodal_apply_dense<<<blocks, kThreads, 0, st>>>(g.out_ptr, g.out_idx, g.out_w, g.in_ptr, g.in_idx,
-                                                  g.in_w, part, move_to, beg, end, ld, M, Mt, cld, CS,
-                                                  ctl);
+  const long long total = static_cast<long long>(n_out) + n_in;
+  if (total <= 0) return;
+  long long blocks = (total + kThreads - 1) / kThreads;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_nodal_apply_dense<<<static_cast<int>(blocks), kThreads, 0, st>>>(
+      g.out_src, g.out_idx, g.out_w, g.in_dst, g.in_idx, g.in_w, part, move_to, o0, n_out, i0, n_in, ld, M,
+      Mt, cld, CS);
   USAP_LAUNCHED();
 }
 
 void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
-                         int update_degrees, int32_t* dout, int32_t* din, const NodalCtl* ctl,
-                         cudaStream_t st) {
+                         int update_degrees, int32_t* dout, int32_t* din, NodalCtl* ctl,
+                         const CtlArgs& c, cudaStream_t st) {
   int count = end - beg;
-  if (count <= 0) return;
   int blocks = (count + 255) / 256;
   if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks < 1) blocks = 1;
   k_nodal_commit<<<blocks, 256, 0, st>>>(part, move_to, g.kout, g.kin, beg, end, update_degrees, dout,
-                                         din);
+                                         din, ctl, c);
   USAP_LAUNCHED();
 }
 
@@ -667,10 +729,5 @@ void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int W, co
   USAP_LAUNCHED();
 }
 
-void launch_ctl_batch_end(NodalCtl* ctl, int itr, int W, double thr, long long* ide_q, int* ide_n,
-                          long long batch_vertices, long long batch_edges, cudaStream_t st) {
-  k_ctl_batch_end<<<1, 1, 0, st>>>(ctl, itr, W, thr, ide_q, ide_n, batch_vertices, batch_edges);
-  USAP_LAUNCHED();
-}
 
 }  // namespace usap

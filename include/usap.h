@@ -74,7 +74,8 @@ typedef struct usap_params {
   int32_t dense_max;   /* dense int32 tile for B <= dense_max (default 4096), sorted views above */
   int32_t device;      /* CUDA device for usap_partition (ignored by contexts) */
   int32_t stats;       /* 1: per-kernel CUDA-event timings and algorithmic byte counts */
-  int32_t reserved[6];
+  int32_t trace_kinds; /* trace events to emit: bit k-1 for kind k; 0 = all kinds */
+  int32_t reserved[5];
 } usap_params;
 
 typedef struct usap_result {

@@ -595,6 +595,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   int32_t bs = n / p.num_batch_nodal_update;
   if (bs < 1) bs = 1;
   const int stats = p.stats ? 1 : 0;
+  trace_mask_ = p.trace_kinds ? p.trace_kinds : 7;
   ev_used_ = 0;
   const LaunchCount lc0 = launch_count();
   long long d2h = 0;
@@ -637,7 +638,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     // batched nodal sweeps
     const bool dense = B <= dense_max;
     prepare_nodal_blocks(part, B, dense);
-    if (trace_) emit_trace(1, stage, 0, 0, B, part, dense, 0, 0, 0, 0, 0);
+    if (trace_on(1)) emit_trace(1, stage, 0, 0, B, part, dense, 0, 0, 0, 0, 0);
     USAP_CUDA(cudaMemsetAsync(ctl_, 0, sizeof(NodalCtl), st_));
     USAP_CUDA(cudaMemsetAsync(ide_q_, 0, sizeof(long long) * std::max(maxitr, 1), st_));
     USAP_CUDA(cudaMemsetAsync(ide_n_, 0, sizeof(int) * std::max(maxitr, 1), st_));
@@ -656,7 +657,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
                                 (static_cast<long long>(hg_.in_ptr[end]) - hg_.in_ptr[beg]);
         const CtlArgs ca{1, itr, W, thr, ide_q_, ide_n_, end - beg, edges};
         nodal_batch(part, B, dense, beg, end, itr, stage, seed, beg == 0, stats, ca);
-        if (trace_) {
+        if (trace_on(2)) {
           USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
           USAP_CUDA(cudaStreamSynchronize(st_));
           NodalCtl c = *h_ctl_;
@@ -697,7 +698,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     d2h += sizeof(NodalCtl);
     auto tn1 = std::chrono::steady_clock::now();
     ms_nodal += std::chrono::duration<double, std::milli>(tn1 - tm1).count();
-    if (trace_) emit_trace(3, stage, 0, 0, B, part, dense, S_fin, 0, 0, 0, 0);
+    if (trace_on(3)) emit_trace(3, stage, 0, 0, B, part, dense, S_fin, 0, 0, 0, 0);
     res->stages++;
     stage++;
 

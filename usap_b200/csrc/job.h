@@ -137,6 +137,8 @@ class Job {
   usap_trace_fn trace_ = nullptr;
   void* trace_user_ = nullptr;
   long long trace_prev_moves_ = 0;
+  int trace_mask_ = 7;
+  bool trace_on(int kind) const { return trace_ && (trace_mask_ >> (kind - 1) & 1); }
 };
 
 }  // namespace usap

@@ -280,9 +280,10 @@ __device__ __forceinline__ void record_stay(const NodalArgs& a, int v) {
   }
 }
 
-// one warp per vertex of degree <= kHubDegree
+// one warp per vertex of degree <= kHubDegree; 5 CTAs per SM so that a
+// batch of the bench workload (N/10 = 5000 vertices) runs in one wave
 template <class Ops>
-__global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops) {
+__global__ void __launch_bounds__(kThreads, 5) k_nodal_propose(NodalArgs a, Ops ops) {
   __shared__ int s_key[kWarps][kHCap];
   __shared__ int s_wo[kWarps][kHCap];
   __shared__ int s_wi[kWarps][kHCap];
@@ -296,16 +297,9 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
     const VertexInfo vi = vertex_info(a, v);
     const int deg = vi.dego + vi.degi;
     if (deg > kHubDegree) continue;   // handled by k_nodal_propose_hub
-    int scanned = 0;
     const int r = vi.r;
-    const int s = propose_target(a, ops, v, vi, lane, &scanned);
-    if (s == r) {
-      if (lane == 0) {
-        record_stay(a, v);
-        if (a.stats) my_bytes += 8 + 8ull * deg + 8ull * scanned;
-      }
-      continue;
-    }
+    // aggregate the neighbour blocks first: these loads do not depend on
+    // the target and overlap the sampling chain below
     int lg = 5;
     while ((1 << lg) < 2 * deg) lg++;
     const int cap = 1 << lg;   // <= kHCap since deg <= kHubDegree
@@ -324,7 +318,17 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose(NodalArgs a, Ops ops
       const int ww = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
       table_insert(key, two, twi, cap, lg, __ldg(a.part + nb), ww, is_out);
     }
+    int scanned = 0;
+    const int s = propose_target(a, ops, v, vi, lane, &scanned);
     __syncwarp();
+    if (s == r) {
+      if (lane == 0) {
+        record_stay(a, v);
+        if (a.stats) my_bytes += 8 + 8ull * deg + 8ull * scanned;
+      }
+      __syncwarp();
+      continue;
+    }
     const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
     const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
     // compact the occupied slots so that each lane takes about one block

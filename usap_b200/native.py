@@ -42,7 +42,7 @@ class Params(C.Structure):
                 ("delta_entropy_moving_avg_window", C.c_int32), ("verbose", C.c_int32),
                 ("dfs_depth", C.c_int32), ("t_block_num", C.c_int32), ("seed", C.c_uint64),
                 ("init_mode", C.c_int32), ("dense_max", C.c_int32), ("device", C.c_int32),
-                ("stats", C.c_int32), ("reserved", C.c_int32 * 6)]
+                ("stats", C.c_int32), ("trace_kinds", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class Result(C.Structure):

@@ -157,6 +157,41 @@ def reference_solve(G, threads: int, timeout: float = 600.0):
     return j["ms"] / 1000.0, j["B"], part
 
 
+def batched_vs_plain(local_rank: int, chains: int = 4):
+    """The batched workload: 64 graphs (N log-uniform in [1000, 20000]) x
+    `chains` Philox chains, solved (a) all at once by usap_batch_partition
+    and (b) one job at a time on the single-graph path, with the graph made
+    resident once per graph.  Wall time includes loading the graphs in both
+    cases.  Returns graphs/s (jobs/s) for both and the matched NMI."""
+    import numpy as np
+    from usap_b200 import api, generator as gen, native as nat
+    graphs = [gen.generate(c) for c in gen.config_c3(seed=0)]
+    seeds = [[1000 * k + c for c in range(chains)] for k in range(len(graphs))]
+    params = nat.default_params(num_batch_nodal_update=10, device=local_rank)
+    jobs, st = api.batch_partition(graphs, seeds, params, device=local_rank)   # warm-up
+    t0 = time.perf_counter()
+    jobs, st = api.batch_partition(graphs, seeds, params, device=local_rank)
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    plain = {}
+    for gi, G in enumerate(graphs):
+        ctx = api.Context(local_rank)
+        ctx.load(G.src, G.dst, None, G.n)
+        for sd in seeds[gi]:
+            plain[(gi, sd)], _ = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=sd))
+        ctx.close()
+    t_plain = time.perf_counter() - t0
+    same = all(np.array_equal(j["assign"], plain[(j["graph"], j["seed"])]) for j in jobs)
+    nmi = [api.evaluate(graphs[j["graph"]].truth, j["assign"])["nmi"] for j in jobs]
+    n_jobs = len(jobs)
+    return {"workload": "64 dcsbm graphs, N log-uniform [1000, 20000], B*=round(N^0.35), "
+                        "within U[0.5,0.8], alpha {1,10}, 4 chains each",
+            "jobs": n_jobs, "graphs_per_s": n_jobs / t_batch, "plain_graphs_per_s": n_jobs / t_plain,
+            "speedup": t_plain / t_batch, "seconds": t_batch, "plain_seconds": t_plain,
+            "workers": st["workers"], "identical_to_plain": bool(same),
+            "mean_nmi": float(np.mean(nmi)), "plain_mean_nmi": float(np.mean(nmi)) if same else None}
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -296,6 +331,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         except Exception as e:   # reported, not fatal
             cpu = {"value": None, "unit": "s", "cores": threads, "kind": "reference",
                    "sample": f"unavailable: {e}"}
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        try:
+            batched = batched_vs_plain(local_rank)
+        except Exception as e:   # reported, not fatal
+            batched = {"error": str(e)}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -315,6 +356,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "cub_calls": int(sum(r["cub_calls"] for r in results)),
         "roofline": roofline,
         "cpu_baseline": cpu,
+        "batched": batched,
         "clocks": clk,
         "mcmc_edge_visits_per_s": visits_per_s,
         "B": res["B"], "S": res["S"], "nmi": nmi, "sweeps": res["sweeps"], "stages": res["stages"],
@@ -332,6 +374,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched-vs-plain measurement of the 64-graph workload")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed solve of the workload (for ncu launch lists), no output")
     args = ap.parse_args()

@@ -150,6 +150,31 @@ usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out
                                usap_result* out);
 usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user);
 
+/* --- batched form: many independent jobs on one GPU ---------------------- */
+/* One job solves graphs[graph] with its own Philox seed (several jobs on the
+ * same graph are independent chains).  Graphs are loaded once and shared.
+ * Jobs run concurrently, each on its own stream driven by one of `workers`
+ * host threads (0 = automatic); their kernels overlap on the GPU.  Every
+ * job's result equals the result of solving it alone with the same seed. */
+typedef struct usap_batch_job {
+  int32_t graph;        /* index into graphs[] */
+  uint64_t seed;        /* Philox seed of this chain */
+  int32_t* out_assign;  /* caller buffer of that graph's n entries, or NULL */
+  usap_result result;   /* filled by the call */
+  usap_status status;   /* per-job status */
+} usap_batch_job;
+
+typedef struct usap_batch_stats {
+  double ms_total;      /* wall time of the whole call */
+  double ms_load;       /* loading the graphs */
+  int32_t workers;
+  int64_t kernel_launches;
+} usap_batch_stats;
+
+usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, const usap_params* p,
+                                 usap_batch_job* jobs, int32_t njobs, int32_t workers,
+                                 int32_t device, usap_batch_stats* stats);
+
 /* --- phase-level replay operations (host buffers in and out) ------------- */
 /* _scc (graph_parallel.hpp:514-603) */
 usap_status usap_op_scc(usap_ctx* ctx, int32_t dfs_depth, int32_t* part, int32_t* B);

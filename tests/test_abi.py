@@ -95,3 +95,15 @@ def test_no_device_is_reported(monkeypatch):
     rc = nat.lib().usap_ctx_create(0, C.byref(h))
     assert rc in (-5, -2)
     assert nat.lib().usap_last_error()
+
+
+def test_batch_rejects_bad_job_index():
+    import ctypes as C
+    src = np.array([0, 1], np.int32)
+    dst = np.array([1, 0], np.int32)
+    g, keep = nat.make_graph(src, dst)
+    garr = (nat.Graph * 1)(g)
+    jobs = (nat.BatchJob * 1)()
+    jobs[0].graph = 3
+    rc = nat.lib().usap_batch_partition(garr, 1, None, jobs, 1, 0, 0, C.byref(nat.BatchStats()))
+    assert rc == -1

@@ -252,3 +252,21 @@ def test_c2_scale_properties(api):
     s = api.evaluate(G.truth, part)
     assert s["nmi"] > 0.3
     ctx.close()
+
+
+def test_batch_equals_solo(api):
+    """Every job of a concurrent batch (several graphs x chains, several
+    workers) returns exactly the partition of solving it alone."""
+    from usap_b200 import native as nat
+    graphs = [gen.generate(c) for c in gen.config_c3(seed=4, graphs=6)]
+    graphs = [g for g in graphs if g.n <= 6000][:4] or graphs[:2]
+    seeds = [[11, 12, 13] for _ in graphs]
+    params = nat.default_params(num_batch_nodal_update=10)
+    jobs, stats = api.batch_partition(graphs, seeds, params, workers=5)
+    assert stats["workers"] >= 1 and len(jobs) == 3 * len(graphs)
+    for j in jobs:
+        G = graphs[j["graph"]]
+        solo, res = api.partition(G.src, G.dst, None, G.n,
+                                  params=nat.default_params(num_batch_nodal_update=10, seed=j["seed"]))
+        assert np.array_equal(solo, j["assign"]), (j["graph"], j["seed"])
+        assert res["S_q"] == j["result"]["S_q"]

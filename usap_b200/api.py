@@ -142,6 +142,40 @@ def partition(src, dst, weight=None, n: int = 0, one_based: bool = False,
     return out, nat.result_dict(res)
 
 
+def batch_partition(graphs, seeds_per_graph, params: Optional[nat.Params] = None,
+                    workers: int = 0, device: int = 0):
+    """Solve many (graph, seed) jobs at once on one GPU (usap_batch_partition).
+
+    ``graphs`` is a list of objects with ``src``, ``dst``, ``weight`` and ``n``
+    (e.g. generator.Graph); ``seeds_per_graph`` a list of seed lists (one
+    chain per seed).  Returns (jobs, stats): jobs is a list of dicts with
+    ``graph``, ``seed``, ``assign`` and ``result`` in submission order."""
+    structs, keep = [], []
+    for g in graphs:
+        gs, k = nat.make_graph(g.src, g.dst, g.weight, g.n)
+        structs.append(gs)
+        keep.append(k)
+    garr = (nat.Graph * len(structs))(*structs)
+    outs, meta = [], []
+    for gi, seeds in enumerate(seeds_per_graph):
+        for sd in seeds:
+            outs.append(np.empty(graphs[gi].n, np.int32))
+            meta.append((gi, int(sd)))
+    jarr = (nat.BatchJob * len(meta))()
+    for j, (gi, sd) in enumerate(meta):
+        jarr[j].graph = gi
+        jarr[j].seed = sd
+        jarr[j].out_assign = nat.p32(outs[j])
+    st = nat.BatchStats()
+    p = params if params is not None else nat.default_params()
+    rc = nat.lib().usap_batch_partition(garr, len(structs), C.byref(p), jarr, len(meta),
+                                        int(workers), int(device), C.byref(st))
+    nat.check(rc)
+    jobs = [{"graph": gi, "seed": sd, "assign": outs[j], "result": nat.result_dict(jarr[j].result)}
+            for j, (gi, sd) in enumerate(meta)]
+    return jobs, {f: getattr(st, f) for f, _ in nat.BatchStats._fields_}
+
+
 def evaluate(truth, given) -> dict:
     """bf::evaluate's scores (plus NMI) as a dict instead of printed lines."""
     t = np.ascontiguousarray(truth, np.int32)

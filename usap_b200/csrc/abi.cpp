@@ -1,10 +1,17 @@
 // extern "C" entry points (include/usap.h).  Errors never escape as C++
 // exceptions: each call returns a status and records a message for the
 // calling thread.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <numeric>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/usap.h"
 #include "job.h"
@@ -139,6 +146,95 @@ usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user) {
   return guarded([&] {
     check_ctx(ctx);
     ctx->job->set_trace(fn, user);
+  });
+}
+
+usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, const usap_params* p,
+                                 usap_batch_job* jobs, int32_t njobs, int32_t workers,
+                                 int32_t device, usap_batch_stats* stats) {
+  return guarded([&] {
+    if (!graphs || ngraphs <= 0 || !jobs || njobs < 0) throw usap::Error(USAP_ERR_INVALID, "bad batch");
+    for (int32_t j = 0; j < njobs; j++)
+      if (jobs[j].graph < 0 || jobs[j].graph >= ngraphs)
+        throw usap::Error(USAP_ERR_INVALID, "job names a graph outside the batch");
+    usap_params def;
+    usap_params_default(&def);
+    const usap_params base = p ? *p : def;
+    auto t0 = std::chrono::steady_clock::now();
+    int hw = static_cast<int>(std::thread::hardware_concurrency());
+    if (hw <= 0) hw = 8;
+    int W = workers > 0 ? workers : std::min(32, 2 * hw);
+    W = std::max(1, std::min(W, std::max(njobs, ngraphs)));
+    // load every graph once, in parallel
+    std::vector<std::shared_ptr<usap::GraphResident>> res(ngraphs);
+    std::vector<std::string> load_err(ngraphs);
+    {
+      std::atomic<int32_t> next{0};
+      std::vector<std::thread> th;
+      for (int w = 0; w < std::min(W, static_cast<int>(ngraphs)); w++)
+        th.emplace_back([&] {
+          for (int32_t i = next++; i < ngraphs; i = next++) {
+            try {
+              res[i] = usap::load_graph(device, graphs[i]);
+            } catch (const std::exception& e) {
+              load_err[i] = e.what();
+            }
+          }
+        });
+      for (auto& t : th) t.join();
+    }
+    for (int32_t i = 0; i < ngraphs; i++)
+      if (!res[i]) throw usap::Error(USAP_ERR_INVALID, "graph " + std::to_string(i) + ": " + load_err[i]);
+    auto t1 = std::chrono::steady_clock::now();
+    // largest graphs first (shortest makespan for a greedy pool)
+    std::vector<int32_t> order(njobs);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+      return res[jobs[a].graph]->hg.e > res[jobs[b].graph]->hg.e;
+    });
+    std::atomic<int32_t> next{0};
+    std::atomic<long long> launches{0};
+    std::vector<std::thread> th;
+    for (int w = 0; w < std::min(W, std::max<int32_t>(njobs, 1)); w++)
+      th.emplace_back([&] {
+        const auto lc0 = usap::launch_count();
+        std::unique_ptr<usap::Job> job;
+        try {
+          job = std::make_unique<usap::Job>(device);
+        } catch (const std::exception&) {
+          job.reset();
+        }
+        for (int32_t k = next++; k < njobs; k = next++) {
+          usap_batch_job& bj = jobs[order[k]];
+          if (!job) {
+            bj.status = USAP_ERR_CUDA;
+            continue;
+          }
+          try {
+            job->attach(res[bj.graph]);
+            usap_params prm = base;
+            prm.seed = bj.seed;
+            job->partition(prm, bj.out_assign, &bj.result);
+            bj.status = USAP_OK;
+          } catch (const usap::Error& e) {
+            bj.status = e.code();
+          } catch (const std::exception&) {
+            bj.status = USAP_ERR_INTERNAL;
+          }
+        }
+        job.reset();
+        launches += usap::launch_count().kernels - lc0.kernels;
+      });
+    for (auto& t : th) t.join();
+    res.clear();
+    if (stats) {
+      stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+      stats->ms_load = std::chrono::duration<double, std::milli>(t1 - t0).count();
+      stats->workers = W;
+      stats->kernel_launches = launches.load();
+    }
+    for (int32_t j = 0; j < njobs; j++)
+      if (jobs[j].status != USAP_OK) throw usap::Error(jobs[j].status, "a batch job failed");
   });
 }
 

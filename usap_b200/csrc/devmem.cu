@@ -1,0 +1,62 @@
+// Device memory and host tables shared by all jobs of the process.
+//
+// Device buffers come from the device's stream-ordered memory pool with its
+// release threshold raised, so memory freed by one job stays reserved and
+// the next job's allocations (a one-shot usap_partition call creates and
+// destroys a job) are served from the pool instead of the driver.
+// The FP64 log table log(k) is computed once per process on the host (glibc
+// log, the values both the GPU path and the oracle read) and grown on demand.
+#include <cmath>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "engine.h"
+
+namespace usap {
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::once_flag g_pool_once[kMaxDevices];
+std::mutex g_log_mu;
+std::shared_ptr<const std::vector<double>> g_log;
+}  // namespace
+
+void pool_configure(int device) {
+  if (device < 0 || device >= kMaxDevices) return;
+  std::call_once(g_pool_once[device], [device] {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return;
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  });
+}
+
+void* dev_alloc(size_t bytes, cudaStream_t st) {
+  void* p = nullptr;
+  USAP_CUDA(cudaMallocAsync(&p, bytes ? bytes : 16, st));
+  return p;
+}
+
+void dev_free(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
+std::shared_ptr<const std::vector<double>> log_table(int64_t max_k) {
+  std::lock_guard<std::mutex> lk(g_log_mu);
+  if (!g_log || static_cast<int64_t>(g_log->size()) <= max_k) {
+    auto t = std::make_shared<std::vector<double>>();
+    size_t old = g_log ? g_log->size() : 0;
+    t->resize(static_cast<size_t>(max_k) + 1);
+    if (old) std::copy(g_log->begin(), g_log->end(), t->begin());
+    if (old == 0) {
+      (*t)[0] = -INFINITY;
+      old = 1;
+    }
+    for (size_t k = old; k < t->size(); k++) (*t)[k] = std::log(static_cast<double>(k));
+    g_log = t;
+  }
+  return g_log;
+}
+
+}  // namespace usap

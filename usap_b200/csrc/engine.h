@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -60,6 +61,12 @@ LaunchCount& launch_count();
 // memory (3 ints per slot), larger ones use the vertex's global region.
 constexpr int kHubDegree = 128;
 constexpr int kHubSmemSlots = 16384;
+
+// process-wide device memory pool and host tables (devmem.cu)
+void pool_configure(int device);
+void* dev_alloc(size_t bytes, cudaStream_t st);
+void dev_free(void* p, cudaStream_t st);
+std::shared_ptr<const std::vector<double>> log_table(int64_t max_k);
 
 // Dense block matrix view: M[x*ld + y], transposed copy Mt[y*ld + x], and
 // per-row chunk sums CS[u*cld + c] of M[u,i]+M[i,u] over blocks
@@ -195,7 +202,7 @@ void launch_merge_union(int B, const int32_t* order, const int32_t* best_s, int 
 void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int32_t* present,
                           int32_t* newlabel, void* cub_tmp, size_t cub_bytes, cudaStream_t st);
 
-void nodal_configure();
+void nodal_configure(int device);
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
                                 const StreamPair& sp);
 void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,
@@ -215,8 +222,8 @@ void launch_merge_sort_keys(int B, const long long* best_q, unsigned long long* 
 // Sort-based construction of the sparse views (CUB radix sort).
 class SortedBuilder {
  public:
-  void reserve(int64_t e, int bmax);
-  void release();
+  void reserve(int64_t e, int bmax, cudaStream_t st);
+  void release(cudaStream_t st);
   // builds row view (+ optional CSC) and symmetric rows for partition `part`
   void build(const GraphDev& g, const int32_t* part, int B, bool with_csc, bool with_sym,
              cudaStream_t st);

@@ -15,6 +15,17 @@
 
 namespace usap {
 
+void scc_prepare(HostGraph& g) {
+  const int32_t n = g.n;
+  g.tptr.assign(n + 1, 0);
+  g.tidx.resize(g.e);
+  for (int64_t i = 0; i < g.e; i++) g.tptr[g.out_idx[i] + 1]++;
+  for (int32_t v = 0; v < n; v++) g.tptr[v + 1] += g.tptr[v];
+  std::vector<int32_t> fill(g.tptr.begin(), g.tptr.end() - 1);
+  for (int32_t i = 0; i < n; i++)
+    for (int32_t p = g.out_ptr[i]; p < g.out_ptr[i + 1]; p++) g.tidx[fill[g.out_idx[p]]++] = i;
+}
+
 int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part) {
   const int32_t n = g.n;
   std::vector<uint8_t> color(n, 0);
@@ -42,15 +53,8 @@ int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part) {
       }
     }
   }
-  // transpose with each list ordered by source vertex id
-  std::vector<int32_t> tptr(n + 1, 0), tidx(g.e);
-  for (int64_t i = 0; i < g.e; i++) tptr[g.out_idx[i] + 1]++;
-  for (int32_t v = 0; v < n; v++) tptr[v + 1] += tptr[v];
-  {
-    std::vector<int32_t> fill(tptr.begin(), tptr.end() - 1);
-    for (int32_t i = 0; i < n; i++)
-      for (int32_t p = g.out_ptr[i]; p < g.out_ptr[i + 1]; p++) tidx[fill[g.out_idx[p]]++] = i;
-  }
+  const std::vector<int32_t>& tptr = g.tptr;
+  const std::vector<int32_t>& tidx = g.tidx;
   std::vector<uint8_t> visited(n, 0);
   for (int32_t v = 0; v < n; v++) part[v] = -1;
   int32_t b = 0;

@@ -16,6 +16,19 @@
 
 namespace usap {
 
+// device buffers of a job come from the retained stream-ordered pool
+template <class T>
+void dalloc_on(T** p, size_t count, cudaStream_t st) {
+  *p = static_cast<T*>(dev_alloc(sizeof(T) * (count > 0 ? count : 1), st));
+}
+template <class T>
+void dfree_on(T*& p, cudaStream_t st) {
+  dev_free(p, st);
+  p = nullptr;
+}
+#define dalloc(pp, count) dalloc_on((pp), static_cast<size_t>(count), st_)
+#define dfree(p) dfree_on((p), st_)
+
 LaunchCount& launch_count() {
   static thread_local LaunchCount c;
   return c;
@@ -30,16 +43,6 @@ void cuda_check(cudaError_t e, const char* what, const char* file, int line) {
 
 namespace {
 
-template <class T>
-void dalloc(T** p, size_t count) {
-  USAP_CUDA(cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * (count ? count : 1)));
-}
-
-template <class T>
-void dfree(T*& p) {
-  if (p) cudaFree(p);
-  p = nullptr;
-}
 
 inline uint64_t mix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ull;
@@ -112,11 +115,12 @@ Job::Job(int device) : device_(device) {
   USAP_CUDA(cudaGetDeviceProperties(&prop, device));
   if (prop.major < 10)
     throw Error(USAP_ERR_NO_DEVICE, std::string("device is not sm_100 class: ") + prop.name);
+  pool_configure(device);
   USAP_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
   USAP_CUDA(cudaStreamCreateWithFlags(&st_side_, cudaStreamNonBlocking));
   USAP_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
   USAP_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
-  nodal_configure();
+  nodal_configure(device);
   USAP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ctl_), sizeof(NodalCtl)));
   dalloc(&ctl_, 1);
 }
@@ -126,6 +130,7 @@ Job::~Job() {
   free_state();
   free_graph();
   dfree(ctl_);
+  if (st_) cudaStreamSynchronize(st_);
   if (h_ctl_) cudaFreeHost(h_ctl_);
   for (auto e : ev_pool_) cudaEventDestroy(e);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
@@ -135,14 +140,9 @@ Job::~Job() {
 }
 
 void Job::free_graph() {
-  dfree(g_.src); dfree(g_.dst); dfree(g_.w);
-  dfree(g_.out_ptr); dfree(g_.out_idx); dfree(g_.out_w);
-  dfree(g_.in_ptr); dfree(g_.in_idx); dfree(g_.in_w);
-  dfree(g_.out_src); dfree(g_.in_dst);
-  dfree(g_.kout); dfree(g_.kin); dfree(g_.logk);
-  dfree(g_.hi_off); dfree(g_.hkey); dfree(g_.hwo); dfree(g_.hwi);
-  dfree(hubs_dev_);
-  hub_ids_.clear();
+  dfree(hkey_); dfree(hwo_); dfree(hwi_);
+  gr_.reset();
+  hg_ = nullptr;
   g_ = GraphDev{};
 }
 
@@ -150,12 +150,11 @@ void Job::free_state() {
   for (auto& s : slots_) dfree(s);
   dfree(move_to_); dfree(dout_); dfree(din_);
   dfree(M_); dfree(Mt_); dfree(CS_);
-  sb_.release();
+  sb_.release(st_);
   dfree(prop_s_); dfree(prop_q_); dfree(best_s_); dfree(best_q_);
   dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
   dfree(union_work_); dfree(root_); dfree(present_); dfree(newlabel_); dfree(merged_dev_);
-  if (cub_tmp_) cudaFree(cub_tmp_);
-  cub_tmp_ = nullptr;
+  dfree(cub_tmp_);
   cub_bytes_ = 0;
   dfree(ide_q_); dfree(ide_n_);
   dfree(rp_s_); dfree(rp_n_); dfree(rp_q_);
@@ -163,8 +162,8 @@ void Job::free_state() {
 }
 
 // --- graph load -----------------------------------------------------------------
-void Job::load(const usap_graph& in) {
-  USAP_CUDA(cudaSetDevice(device_));
+std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
+  USAP_CUDA(cudaSetDevice(device));
   if (in.e <= 0 || !in.src || !in.dst) throw Error(USAP_ERR_INVALID, "graph needs at least one edge");
   if (in.e >= (1ll << 30)) throw Error(USAP_ERR_LIMIT, "more than 2^30 edges");
   HostGraph h;
@@ -234,6 +233,7 @@ void Job::load(const usap_graph& in) {
       }
     }
   }
+  scc_prepare(h);
   // per-vertex global hash regions for degrees beyond the shared-memory table
   std::vector<int64_t> hi_off(n, -1);
   std::vector<int32_t> hubs;
@@ -249,12 +249,10 @@ void Job::load(const usap_graph& in) {
       }
     }
   }
-  std::vector<double> logk(wtot + 1);
-  logk[0] = -INFINITY;
-  for (int64_t k = 1; k <= wtot; k++) logk[k] = std::log(static_cast<double>(k));
+  const std::shared_ptr<const std::vector<double>> logk_all = log_table(wtot);
 
-  free_state();
-  free_graph();
+  auto gr = std::make_shared<GraphResident>(device);
+  cudaStream_t st_ = gr->st;
   cudaEvent_t e0, e1;
   USAP_CUDA(cudaEventCreate(&e0));
   USAP_CUDA(cudaEventCreate(&e1));
@@ -293,41 +291,89 @@ void Job::load(const usap_graph& in) {
     up(&g.out_src, osrc);
     up(&g.in_dst, idst);
   }
-  dalloc(&g.logk, logk.size());
-  USAP_CUDA(cudaMemcpyAsync(g.logk, logk.data(), sizeof(double) * logk.size(), cudaMemcpyHostToDevice, st_));
+  dalloc(&g.logk, wtot + 1);
+  USAP_CUDA(cudaMemcpyAsync(g.logk, logk_all->data(), sizeof(double) * (wtot + 1), cudaMemcpyHostToDevice, st_));
   dalloc(&g.hi_off, n);
   USAP_CUDA(cudaMemcpyAsync(g.hi_off, hi_off.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st_));
-  up_bytes += static_cast<long long>(sizeof(double) * logk.size() + sizeof(int64_t) * n +
+  up_bytes += static_cast<long long>(sizeof(double) * (wtot + 1) + sizeof(int64_t) * n +
                                      sizeof(int32_t) * hubs.size());
   g.hi_slots = hi_slots;
-  dalloc(&g.hkey, hi_slots);
-  dalloc(&g.hwo, hi_slots);
-  dalloc(&g.hwi, hi_slots);
-  dalloc(&hubs_dev_, hubs.size());
+  dalloc(&gr->hubs_dev, hubs.size());
   if (!hubs.empty())
-    USAP_CUDA(cudaMemcpyAsync(hubs_dev_, hubs.data(), sizeof(int32_t) * hubs.size(), cudaMemcpyHostToDevice, st_));
+    USAP_CUDA(cudaMemcpyAsync(gr->hubs_dev, hubs.data(), sizeof(int32_t) * hubs.size(), cudaMemcpyHostToDevice, st_));
   USAP_CUDA(cudaEventRecord(e1, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
   float ms = 0;
   USAP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  h2d_ms_ = ms;
-  h2d_bytes_ = up_bytes;
+  gr->h2d_ms = ms;
+  gr->h2d_bytes = up_bytes;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  g_ = g;
-  hg_ = std::move(h);
-  hub_ids_ = std::move(hubs);
+  gr->g = g;
+  gr->hg = std::move(h);
+  gr->hub_ids = std::move(hubs);
+  return gr;
 }
+
+GraphResident::GraphResident(int dev) : device(dev) {
+  pool_configure(dev);
+  USAP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+}
+
+GraphResident::~GraphResident() {
+  cudaSetDevice(device);
+  cudaStream_t st_ = st;
+  dfree(g.src); dfree(g.dst); dfree(g.w);
+  dfree(g.out_ptr); dfree(g.out_idx); dfree(g.out_w);
+  dfree(g.in_ptr); dfree(g.in_idx); dfree(g.in_w);
+  dfree(g.out_src); dfree(g.in_dst);
+  dfree(g.kout); dfree(g.kin); dfree(g.logk);
+  dfree(g.hi_off);
+  dfree(hubs_dev);
+  if (st) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+}
+
+void Job::load(const usap_graph& in) {
+  USAP_CUDA(cudaSetDevice(device_));
+  attach(load_graph(device_, in));
+}
+
+void Job::attach(std::shared_ptr<GraphResident> gr) {
+  USAP_CUDA(cudaSetDevice(device_));
+  if (gr_ != gr) {
+    // the hub scratch and per-vertex state depend on the graph
+    USAP_CUDA(cudaStreamSynchronize(st_));
+    free_state();
+    dfree(hkey_); dfree(hwo_); dfree(hwi_);
+  }
+  gr_ = std::move(gr);
+  hg_ = &gr_->hg;
+  g_ = gr_->g;
+  if (!hkey_) {
+    dalloc(&hkey_, g_.hi_slots);
+    dalloc(&hwo_, g_.hi_slots);
+    dalloc(&hwi_, g_.hi_slots);
+  }
+  g_.hkey = hkey_;
+  g_.hwo = hwo_;
+  g_.hwi = hwi_;
+}
+
+
 
 HubList Job::hubs_for(int32_t beg, int32_t end, int32_t B) const {
   HubList hl;
-  hl.ids = hubs_dev_;
-  hl.lo = static_cast<int>(std::lower_bound(hub_ids_.begin(), hub_ids_.end(), beg) - hub_ids_.begin());
-  hl.hi = static_cast<int>(std::lower_bound(hub_ids_.begin(), hub_ids_.end(), end) - hub_ids_.begin());
+  const std::vector<int32_t>& hub_ids = gr_->hub_ids;
+  hl.ids = gr_->hubs_dev;
+  hl.lo = static_cast<int>(std::lower_bound(hub_ids.begin(), hub_ids.end(), beg) - hub_ids.begin());
+  hl.hi = static_cast<int>(std::lower_bound(hub_ids.begin(), hub_ids.end(), end) - hub_ids.begin());
   int cap = 32;
   for (int i = hl.lo; i < hl.hi; i++) {
-    const int32_t v = hub_ids_[i];
-    int deg = (hg_.out_ptr[v + 1] - hg_.out_ptr[v]) + (hg_.in_ptr[v + 1] - hg_.in_ptr[v]);
+    const int32_t v = hub_ids[i];
+    int deg = (hg_->out_ptr[v + 1] - hg_->out_ptr[v]) + (hg_->in_ptr[v + 1] - hg_->in_ptr[v]);
     int c = 1 << hash_lg(std::min(deg, B));
     cap = std::max(cap, c);
   }
@@ -336,7 +382,7 @@ HubList Job::hubs_for(int32_t beg, int32_t end, int32_t B) const {
 }
 
 void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxitr) {
-  const int32_t n = hg_.n;
+  const int32_t n = hg_->n;
   bool fresh = slots_[0] == nullptr;
   if (fresh) {
     for (auto& s : slots_) dalloc(&s, n);
@@ -363,13 +409,13 @@ void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxit
     dalloc(&present_, B);
     dalloc(&newlabel_, B);
     dalloc(&merged_dev_, 1);
-    if (cub_tmp_) cudaFree(cub_tmp_);
+    dfree(cub_tmp_);
     size_t b1 = 0, b2 = 0;
     USAP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, skeys_, skeys_alt_, sidx_, sidx_alt_, B));
     USAP_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, b2, present_, newlabel_, B));
     cub_bytes_ = std::max(b1, b2);
-    USAP_CUDA(cudaMalloc(&cub_tmp_, cub_bytes_));
-    sb_.reserve(hg_.e, B);
+    cub_tmp_ = dev_alloc(cub_bytes_, st_);
+    sb_.reserve(hg_->e, B, st_);
     bcap_ = B;
     kcap_ = 0;
   }
@@ -437,7 +483,7 @@ int32_t Job::merge_apply(int32_t* part, int32_t B, int32_t btm) {
   USAP_CUB(cub::DeviceRadixSort::SortPairs(cub_tmp_, bytes, skeys_, skeys_alt_, sidx_, sidx_alt_, B, 0,
                                            64, st_));
   launch_merge_union(B, sidx_alt_, best_s_, btm, union_work_, root_, merged_dev_, st_);
-  launch_merge_relabel(hg_.n, B, part, root_, present_, newlabel_, cub_tmp_, cub_bytes_, st_);
+  launch_merge_relabel(hg_->n, B, part, root_, present_, newlabel_, cub_tmp_, cub_bytes_, st_);
   int32_t merged = 0;
   USAP_CUDA(cudaMemcpyAsync(&h_ctl_->pad0, merged_dev_, sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
@@ -510,8 +556,8 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
   else launch_nodal_propose_sorted(a, sb_.view(), hubs, streams());
   if (stats == 1) USAP_CUDA(cudaEventRecord(e1, st_));
   if (dense) {
-    const int o0 = hg_.out_ptr[beg], i0 = hg_.in_ptr[beg];
-    launch_nodal_apply_dense(g_, part, move_to_, o0, hg_.out_ptr[end] - o0, i0, hg_.in_ptr[end] - i0, ld_,
+    const int o0 = hg_->out_ptr[beg], i0 = hg_->in_ptr[beg];
+    launch_nodal_apply_dense(g_, part, move_to_, o0, hg_->out_ptr[end] - o0, i0, hg_->in_ptr[end] - i0, ld_,
                              M_, Mt_, cld_, CS_, st_);
   }
   launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, ctl_args, st_);
@@ -519,7 +565,7 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
 
 void Job::emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part, bool dense,
                      long long S_q, int S_ninf, long long cum_q, int cum_ninf, long long moves) {
-  const int32_t n = hg_.n;
+  const int32_t n = hg_->n;
   std::vector<int32_t> hp(n), hdo(B), hdi(B);
   USAP_CUDA(cudaMemcpyAsync(hp.data(), part, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaMemcpyAsync(hdo.data(), dout_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
@@ -588,7 +634,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   const int dense_max = p.dense_max > 0 ? p.dense_max : 4096;
   auto t_start = std::chrono::steady_clock::now();
   std::memset(res, 0, sizeof(*res));
-  const int32_t n = hg_.n;
+  const int32_t n = hg_->n;
   const int32_t K = p.num_agg_proposals_per_block;
   const int32_t W = p.delta_entropy_moving_avg_window;
   const int32_t maxitr = p.max_num_nodal_itr;
@@ -607,7 +653,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     for (int32_t v = 0; v < n; v++) part0[v] = v;
     B = n;
   } else {
-    B = scc_host(hg_, p.dfs_depth, part0.data());
+    B = scc_host(*hg_, p.dfs_depth, part0.data());
   }
   ensure_capacity(B, K, dense_max, std::max(maxitr, 1));
   int32_t work = 0;
@@ -644,7 +690,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     USAP_CUDA(cudaMemsetAsync(ide_n_, 0, sizeof(int) * std::max(maxitr, 1), st_));
     const bool isf = gs.large.finite && gs.med.finite && gs.small.finite;
     const double thr = isf ? p.delta_entropy_threshold2 : p.delta_entropy_threshold1;
-    const long long model_q = q32_host(model_S(n, hg_.e, B));
+    const long long model_q = q32_host(model_S(n, hg_->e, B));
     trace_prev_moves_ = 0;
     for (int32_t itr = 0; itr < maxitr; itr++) {
       if (!dense) sb_.build(g_, part, B, false, true, st_);
@@ -653,8 +699,8 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       size_t ev_mark = ev_used_;
       for (int32_t beg = 0; beg < n; beg += bs) {
         const int32_t end = beg + bs < n ? beg + bs : n;
-        const long long edges = (static_cast<long long>(hg_.out_ptr[end]) - hg_.out_ptr[beg]) +
-                                (static_cast<long long>(hg_.in_ptr[end]) - hg_.in_ptr[beg]);
+        const long long edges = (static_cast<long long>(hg_->out_ptr[end]) - hg_->out_ptr[beg]) +
+                                (static_cast<long long>(hg_->in_ptr[end]) - hg_->in_ptr[beg]);
         const CtlArgs ca{1, itr, W, thr, ide_q_, ide_n_, end - beg, edges};
         nodal_batch(part, B, dense, beg, end, itr, stage, seed, beg == 0, stats, ca);
         if (trace_on(2)) {
@@ -745,7 +791,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
 // --- phase-level operations -------------------------------------------------------
 int32_t Job::op_scc(int32_t depth, int32_t* part) {
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
-  return scc_host(hg_, depth, part);
+  return scc_host(*hg_, depth, part);
 }
 
 void Job::op_build(const int32_t* part, int32_t B, int32_t dense_max, int32_t* M, int32_t* dout,
@@ -753,7 +799,7 @@ void Job::op_build(const int32_t* part, int32_t B, int32_t dense_max, int32_t* M
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
   USAP_CUDA(cudaSetDevice(device_));
   ensure_capacity(B, 1, dense_max, 1);
-  const int32_t n = hg_.n;
+  const int32_t n = hg_->n;
   USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st_));
   const bool dense = B <= dense_max;
   prepare_nodal_blocks(slots_[0], B, dense);
@@ -786,13 +832,13 @@ int64_t Job::op_entropy(const int32_t* part, int32_t B, int32_t dense_max) {
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
   USAP_CUDA(cudaSetDevice(device_));
   ensure_capacity(B, 1, dense_max, 1);
-  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
   const bool dense = B <= dense_max;
   prepare_nodal_blocks(slots_[0], B, dense);
   entropy_launch(slots_[0], B, dense);
   USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
-  return q32_host(model_S(hg_.n, hg_.e, B)) - static_cast<long long>(h_ctl_->entropy_acc);
+  return q32_host(model_S(hg_->n, hg_->e, B)) - static_cast<long long>(h_ctl_->entropy_acc);
 }
 
 void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
@@ -801,7 +847,7 @@ void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stag
   if (K < 1) throw Error(USAP_ERR_INVALID, "K must be >= 1");
   USAP_CUDA(cudaSetDevice(device_));
   ensure_capacity(B, K, 1, 1);
-  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
   merge_phase(slots_[0], B, K, static_cast<uint32_t>(stage), seed);
   USAP_CUDA(cudaMemcpyAsync(best_s, best_s_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaMemcpyAsync(best_q, best_q_, sizeof(int64_t) * B, cudaMemcpyDeviceToHost, st_));
@@ -817,11 +863,11 @@ void Job::op_merge_apply(int32_t* part, int32_t B, const int32_t* best_s, const 
   for (int32_t i = 0; i < B; i++)
     if (best_s[i] < 0 || best_s[i] >= B) throw Error(USAP_ERR_INVALID, "best merge target out of range");
   ensure_capacity(B, 1, 1, 1);
-  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
   USAP_CUDA(cudaMemcpyAsync(best_s_, best_s, sizeof(int32_t) * B, cudaMemcpyHostToDevice, st_));
   USAP_CUDA(cudaMemcpyAsync(best_q_, best_q, sizeof(int64_t) * B, cudaMemcpyHostToDevice, st_));
   int32_t m = merge_apply(slots_[0], B, btm);
-  USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_.n, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_->n, cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
   *merged = m;
   *B_new = B - m;
@@ -831,10 +877,10 @@ void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t be
                          int32_t itr, int32_t stage, uint64_t seed, int32_t* prop_s, int64_t* prop_q,
                          int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves) {
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
-  if (beg < 0 || end > hg_.n || beg > end) throw Error(USAP_ERR_INVALID, "batch range out of bounds");
+  if (beg < 0 || end > hg_->n || beg > end) throw Error(USAP_ERR_INVALID, "batch range out of bounds");
   USAP_CUDA(cudaSetDevice(device_));
   ensure_capacity(B, 1, dense_max, 1);
-  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_.n, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
   const bool dense = B <= dense_max;
   prepare_nodal_blocks(slots_[0], B, dense);
   USAP_CUDA(cudaMemsetAsync(ctl_, 0, sizeof(NodalCtl), st_));
@@ -842,7 +888,7 @@ void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t be
   nodal_batch(slots_[0], B, dense, beg, end, static_cast<uint32_t>(itr), static_cast<uint32_t>(stage), seed,
               true, 2, ca);
   const int32_t cnt = end - beg;
-  USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_.n, cudaMemcpyDeviceToHost, st_));
+  USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_->n, cudaMemcpyDeviceToHost, st_));
   if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, rp_s_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));
   if (prop_q) USAP_CUDA(cudaMemcpyAsync(prop_q, rp_q_, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost, st_));
   if (prop_ninf) USAP_CUDA(cudaMemcpyAsync(prop_ninf, rp_n_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));

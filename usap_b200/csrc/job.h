@@ -17,9 +17,14 @@ struct HostGraph {
   bool unit = true;
   std::vector<int32_t> src, dst, w;
   std::vector<int32_t> out_ptr, out_idx, out_w, in_ptr, in_idx, in_w, kout, kin;
+  // in-lists ordered by source vertex id (the transpose _scc builds,
+  // graph_parallel.hpp:518-523), prepared once at load
+  std::vector<int32_t> tptr, tidx;
 };
 
-// _scc + _dfs_itr (graph_parallel.hpp:514-603), host side
+// _scc + _dfs_itr (graph_parallel.hpp:514-603), host side; scc_prepare
+// builds the transpose it walks (once per graph)
+void scc_prepare(HostGraph& g);
 int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part);
 
 // host evaluation (evaluate.hpp:18-266 scores + NMI + Hungarian accuracy)
@@ -44,6 +49,27 @@ int32_t reduce_blocks(int32_t B, float rate);   // (size_t)_P.B * rate, :340
 double model_S(int64_t n, int64_t e, int32_t B);   // :1314-1316
 long long q32_host(double t);
 
+// A graph loaded into HBM (CSR, edge list, log table, hub list); read-only
+// once loaded and shared by every job that solves it.  Its device arrays
+// are allocated and released on its own stream.
+struct GraphResident {
+  explicit GraphResident(int device);
+  ~GraphResident();
+  GraphResident(const GraphResident&) = delete;
+  GraphResident& operator=(const GraphResident&) = delete;
+  int device;
+  cudaStream_t st = nullptr;
+  HostGraph hg;
+  GraphDev g;                      // hkey/hwo/hwi belong to the jobs
+  std::vector<int32_t> hub_ids;    // vertices of degree > kHubDegree, ascending
+  int32_t* hubs_dev = nullptr;
+  double h2d_ms = 0;
+  long long h2d_bytes = 0;
+};
+
+// Graph_P constructor / load_graph_from_tsv (graph_parallel.hpp:251-317)
+std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in);
+
 class Job {
  public:
   explicit Job(int device);
@@ -52,8 +78,14 @@ class Job {
   Job& operator=(const Job&) = delete;
 
   void load(const usap_graph& g);
-  bool loaded() const { return hg_.n > 0; }
-  const HostGraph& host_graph() const { return hg_; }
+  // solve a graph that is already resident (shared with other jobs)
+  void attach(std::shared_ptr<GraphResident> gr);
+  bool loaded() const { return hg_ != nullptr; }
+  const HostGraph& host_graph() const {
+    static const HostGraph empty;
+    return hg_ ? *hg_ : empty;
+  }
+  const std::shared_ptr<GraphResident>& graph() const { return gr_; }
   void set_trace(usap_trace_fn fn, void* user) {
     trace_ = fn;
     trace_user_ = user;
@@ -73,8 +105,8 @@ class Job {
                       int32_t itr, int32_t stage, uint64_t seed, int32_t* prop_s, int64_t* prop_q,
                       int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves);
 
-  double last_h2d_ms() const { return h2d_ms_; }
-  long long last_h2d_bytes() const { return h2d_bytes_; }
+  double last_h2d_ms() const { return gr_ ? gr_->h2d_ms : 0.0; }
+  long long last_h2d_bytes() const { return gr_ ? gr_->h2d_bytes : 0; }
 
  private:
   void free_graph();
@@ -100,10 +132,10 @@ class Job {
   cudaStream_t st_ = nullptr;
   cudaStream_t st_side_ = nullptr;   // hub CTAs overlap the warp kernel here
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
-  HostGraph hg_;
-  GraphDev g_;
-  double h2d_ms_ = 0;
-  long long h2d_bytes_ = 0;   // bytes uploaded by load()
+  std::shared_ptr<GraphResident> gr_;
+  const HostGraph* hg_ = nullptr;
+  GraphDev g_;                       // the graph's arrays + this job's hub scratch
+  int32_t *hkey_ = nullptr, *hwo_ = nullptr, *hwi_ = nullptr;
   // state
   int32_t bcap_ = 0, kcap_ = 0, dcap_ = 0, icap_ = 0;
   int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -111,8 +143,6 @@ class Job {
   int32_t *dout_ = nullptr, *din_ = nullptr;
   int *M_ = nullptr, *Mt_ = nullptr, *CS_ = nullptr;
   int ld_ = 0, cld_ = 0;
-  std::vector<int32_t> hub_ids_;      // vertices of degree > kHubDegree, ascending
-  int32_t* hubs_dev_ = nullptr;
   SortedBuilder sb_;
   int32_t* prop_s_ = nullptr;
   long long* prop_q_ = nullptr;

@@ -212,29 +212,31 @@ void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, 
 }
 
 // --- SortedBuilder --------------------------------------------------------------
-void SortedBuilder::reserve(int64_t e, int bmax) {
-  release();
+void SortedBuilder::reserve(int64_t e, int bmax, cudaStream_t st) {
+  release(st);
   e_ = e;
   bmax_ = bmax;
-  int64_t e2 = 2 * e;
-  USAP_CUDA(cudaMalloc(&keys_, sizeof(unsigned long long) * e2));
-  USAP_CUDA(cudaMalloc(&keys_alt_, sizeof(unsigned long long) * e2));
-  USAP_CUDA(cudaMalloc(&ukeys_, sizeof(unsigned long long) * e2));
-  USAP_CUDA(cudaMalloc(&vals_, sizeof(int) * e2));
-  USAP_CUDA(cudaMalloc(&vals_alt_, sizeof(int) * e2));
-  USAP_CUDA(cudaMalloc(&uvals_, sizeof(int) * e2));
-  USAP_CUDA(cudaMalloc(&nruns_, sizeof(int) * 4));
-  USAP_CUDA(cudaMalloc(&nnz_, sizeof(int) * 4));
-  USAP_CUDA(cudaMalloc(&rowptr_, sizeof(int) * (bmax + 1)));
-  USAP_CUDA(cudaMalloc(&col_, sizeof(int) * e));
-  USAP_CUDA(cudaMalloc(&val_, sizeof(int) * e));
-  USAP_CUDA(cudaMalloc(&rowof_, sizeof(int) * e));
-  USAP_CUDA(cudaMalloc(&colptr_, sizeof(int) * (bmax + 1)));
-  USAP_CUDA(cudaMalloc(&crow_, sizeof(int) * e));
-  USAP_CUDA(cudaMalloc(&cval_, sizeof(int) * e));
-  USAP_CUDA(cudaMalloc(&symptr_, sizeof(int) * (bmax + 1)));
-  USAP_CUDA(cudaMalloc(&symcol_, sizeof(int) * e2));
-  USAP_CUDA(cudaMalloc(&symcum_, sizeof(int) * e2));
+  const int64_t e2 = 2 * e;
+  auto a64 = [&](int64_t n) { return static_cast<unsigned long long*>(dev_alloc(sizeof(unsigned long long) * n, st)); };
+  auto a32 = [&](int64_t n) { return static_cast<int*>(dev_alloc(sizeof(int) * n, st)); };
+  keys_ = a64(e2);
+  keys_alt_ = a64(e2);
+  ukeys_ = a64(e2);
+  vals_ = a32(e2);
+  vals_alt_ = a32(e2);
+  uvals_ = a32(e2);
+  nruns_ = a32(4);
+  nnz_ = a32(4);
+  rowptr_ = a32(bmax + 1);
+  col_ = a32(e);
+  val_ = a32(e);
+  rowof_ = a32(e);
+  colptr_ = a32(bmax + 1);
+  crow_ = a32(e);
+  cval_ = a32(e);
+  symptr_ = a32(bmax + 1);
+  symcol_ = a32(e2);
+  symcum_ = a32(e2);
   size_t b1 = 0, b2 = 0, b3 = 0;
   int n2 = static_cast<int>(e2);
   USAP_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, b1, keys_, keys_alt_, vals_, vals_alt_, n2));
@@ -243,14 +245,13 @@ void SortedBuilder::reserve(int64_t e, int bmax) {
   USAP_CUDA(cub::DeviceScan::InclusiveSum(nullptr, b3, uvals_, symcum_, n2));
   tmp_bytes_ = b1 > b2 ? b1 : b2;
   if (b3 > tmp_bytes_) tmp_bytes_ = b3;
-  USAP_CUDA(cudaMalloc(&tmp_, tmp_bytes_));
+  tmp_ = dev_alloc(tmp_bytes_, st);
 }
 
-void SortedBuilder::release() {
+void SortedBuilder::release(cudaStream_t st) {
   void* ptrs[] = {keys_, keys_alt_, ukeys_, vals_, vals_alt_, uvals_, nruns_, nnz_, rowptr_, col_, val_,
                   rowof_, colptr_, crow_, cval_, symptr_, symcol_, symcum_, tmp_};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (void* p : ptrs) dev_free(p, st);
   keys_ = keys_alt_ = ukeys_ = nullptr;
   vals_ = vals_alt_ = uvals_ = nruns_ = nnz_ = nullptr;
   rowptr_ = col_ = val_ = rowof_ = colptr_ = crow_ = cval_ = symptr_ = symcol_ = symcum_ = nullptr;

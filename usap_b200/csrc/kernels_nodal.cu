@@ -25,6 +25,7 @@
 // partition.  The convergence bookkeeping of the update task runs in a
 // one-thread kernel so batches and sweeps queue without host round trips.
 #include <cmath>
+#include <mutex>
 
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
@@ -42,6 +43,8 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHCap = 256;          // shared-memory hash slots per warp
 constexpr int kChunk = 128;         // blocks per chunk sum of a dense row
+constexpr int kHubThreads = 512;    // threads of a hub CTA
+constexpr int kHubWarps = kHubThreads / 32;
 
 struct DenseOps {
   DenseView v;
@@ -374,11 +377,11 @@ __global__ void __launch_bounds__(kThreads, 5) k_nodal_propose(NodalArgs a, Ops 
 // min(deg, B) distinct blocks and lives in dynamic shared memory
 // (`smem_cap` slots) or, beyond that, in the vertex's global region
 template <class Ops>
-__global__ void __launch_bounds__(kThreads) k_nodal_propose_hub(NodalArgs a, Ops ops, const int32_t* hubs,
-                                                               int hub_lo, int hub_hi, int smem_cap) {
+__global__ void __launch_bounds__(kHubThreads) k_nodal_propose_hub(NodalArgs a, Ops ops, const int32_t* hubs,
+                                                                  int hub_lo, int hub_hi, int smem_cap) {
   extern __shared__ int dyn[];
-  __shared__ long long s_acc[kWarps];
-  __shared__ int s_sum[5][kWarps];
+  __shared__ long long s_acc[kHubWarps];
+  __shared__ int s_sum[5][kHubWarps];
   __shared__ int s_target, s_scanned;
   if (*reinterpret_cast<volatile int*>(&a.ctl->done)) return;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -421,13 +424,13 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose_hub(NodalArgs a, Ops
       two = a.hwo + off;
       twi = a.hwi + off;
     }
-    for (int i = threadIdx.x; i < cap; i += kThreads) {
+    for (int i = threadIdx.x; i < cap; i += kHubThreads) {
       key[i] = -1;
       two[i] = 0;
       twi[i] = 0;
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < deg; j += kThreads) {
+    for (int j = threadIdx.x; j < deg; j += kHubThreads) {
       const bool is_out = j < vi.dego;
       const int nb = is_out ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
       const int ww = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose_hub(NodalArgs a, Ops
     const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
     const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
     TermSums ts{0, 0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < cap; i += kThreads) {
+    for (int i = threadIdx.x; i < cap; i += kHubThreads) {
       const int b = key[i];
       if (b < 0) continue;
       ts.nb++;
@@ -462,7 +465,7 @@ __global__ void __launch_bounds__(kThreads) k_nodal_propose_hub(NodalArgs a, Ops
     __syncthreads();
     if (threadIdx.x == 0) {
       TermSums tot{0, 0, 0, 0, 0, 0};
-      for (int w = 0; w < kWarps; w++) {
+      for (int w = 0; w < kHubWarps; w++) {
         tot.acc += s_acc[w];
         tot.sXR += s_sum[0][w];
         tot.sXS += s_sum[1][w];
@@ -655,8 +658,8 @@ void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const Stre
     USAP_CUDA(cudaEventRecord(sp.fork, sp.main));
     USAP_CUDA(cudaStreamWaitEvent(sp.side, sp.fork, 0));
     const size_t smem = sizeof(int) * 3 * static_cast<size_t>(hubs.smem_cap);
-    k_nodal_propose_hub<Ops><<<hubs.hi - hubs.lo, kThreads, smem, sp.side>>>(a, ops, hubs.ids, hubs.lo,
-                                                                             hubs.hi, hubs.smem_cap);
+    k_nodal_propose_hub<Ops><<<hubs.hi - hubs.lo, kHubThreads, smem, sp.side>>>(a, ops, hubs.ids, hubs.lo,
+                                                                                hubs.hi, hubs.smem_cap);
     USAP_LAUNCHED();
   }
   int blocks = (count + kWarps - 1) / kWarps;
@@ -671,15 +674,17 @@ void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const Stre
 
 }  // namespace
 
-void nodal_configure() {
-  static bool done = false;
-  if (done) return;
-  const int smem = static_cast<int>(sizeof(int) * 3 * kHubSmemSlots);
-  USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<DenseOps>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<SortedOps>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  done = true;
+// the hub kernel's dynamic shared memory limit, set once per device
+void nodal_configure(int device) {
+  static std::once_flag once[64];
+  if (device < 0 || device >= 64) return;
+  std::call_once(once[device], [] {
+    const int smem = static_cast<int>(sizeof(int) * 3 * kHubSmemSlots);
+    USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<DenseOps>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<SortedOps>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  });
 }
 
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,

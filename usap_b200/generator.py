@@ -215,3 +215,18 @@ def config_c1(within: float = 0.8, alpha: float = 10.0, seed: int = 0) -> SBMCon
 def config_c2(seed: int = 0) -> SBMConfig:
     """N=50000, 44 planted blocks, within-block 0.5, alpha 1 (~800k edges)."""
     return SBMConfig(n=50000, blocks=44, within=0.5, alpha=1.0, seed=seed)
+
+
+def config_c3(seed: int = 0, graphs: int = 64):
+    """Batched workload: ``graphs`` graphs with N log-uniform in [1000, 20000],
+    round(N^0.35) planted blocks, within-block fraction uniform in [0.5, 0.8]
+    and Dirichlet alpha in {1, 10}; one SBMConfig per graph."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(graphs):
+        n = int(round(np.exp(rng.uniform(np.log(1000), np.log(20000)))))
+        out.append(SBMConfig(n=n, blocks=max(1, int(round(n ** 0.35))),
+                             within=float(rng.uniform(0.5, 0.8)),
+                             alpha=float(rng.choice([1.0, 10.0])),
+                             seed=int(rng.integers(0, 2**31 - 1))))
+    return out

@@ -75,12 +75,22 @@ class TraceEvent(C.Structure):
 
 TRACE_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(TraceEvent))
 
+
+class BatchJob(C.Structure):
+    _fields_ = [("graph", C.c_int32), ("seed", C.c_uint64), ("out_assign", i32p),
+                ("result", Result), ("status", C.c_int32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("ms_load", C.c_double), ("workers", C.c_int32),
+                ("kernel_launches", C.c_int64)]
+
 # every exported symbol of include/usap.h
 EXPORTS = ("usap_version", "usap_last_error", "usap_params_default", "usap_partition",
            "usap_evaluate", "usap_ctx_create", "usap_ctx_destroy", "usap_ctx_load",
            "usap_ctx_num_nodes", "usap_ctx_partition", "usap_ctx_set_trace", "usap_op_scc",
            "usap_op_build", "usap_op_entropy", "usap_op_merge_phase", "usap_op_merge_apply",
-           "usap_op_nodal_batch")
+           "usap_op_nodal_batch", "usap_batch_partition")
 
 _lib = None
 
@@ -116,6 +126,9 @@ def lib() -> C.CDLL:
     L.usap_op_nodal_batch.argtypes = [C.c_void_p, i32p, C.c_int32, C.c_int32, C.c_int32,
                                       C.c_int32, C.c_int32, C.c_int32, C.c_uint64, i32p, i64p,
                                       i32p, i64p, i32p, i64p]
+    L.usap_batch_partition.argtypes = [C.POINTER(Graph), C.c_int32, C.POINTER(Params),
+                                       C.POINTER(BatchJob), C.c_int32, C.c_int32, C.c_int32,
+                                       C.POINTER(BatchStats)]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name.startswith("usap_") and name not in ("usap_version", "usap_last_error",

@@ -75,7 +75,8 @@ typedef struct usap_params {
   int32_t device;      /* CUDA device for usap_partition (ignored by contexts) */
   int32_t stats;       /* 1: per-kernel CUDA-event timings and algorithmic byte counts */
   int32_t trace_kinds; /* trace events to emit: bit k-1 for kind k; 0 = all kinds */
-  int32_t reserved[5];
+  int32_t sweep_graphs;/* 1: record each stage's nodal sweep as a CUDA graph and replay it */
+  int32_t reserved[4];
 } usap_params;
 
 typedef struct usap_result {
@@ -95,6 +96,7 @@ typedef struct usap_result {
   int64_t kernel_launches;    /* launches of this library's kernels during the call */
   int64_t cub_calls;          /* CUB sort/scan/reduce calls during the call */
   int64_t h2d_bytes, d2h_bytes;  /* host<->device traffic of the call */
+  int64_t sweep_graph_launches;  /* nodal sweeps replayed from a captured CUDA graph */
 } usap_result;
 
 typedef struct usap_scores {

@@ -92,10 +92,11 @@ struct StreamPair {
   cudaEvent_t fork, join;
 };
 
-// batch-end bookkeeping, run by the commit kernel (active = 1)
+// batch-end bookkeeping, run by the commit kernel (active = 1); the sweep
+// index comes from the control block
 struct CtlArgs {
   int active;
-  int itr, W;
+  int W;
   double thr;
   long long* ide_q;
   int* ide_n;
@@ -121,7 +122,7 @@ struct NodalCtl {
   int done;          // convergence reached: later batch kernels return at once
   int S_ninf;
   int cum_ninf;
-  int pad0;
+  int itr;           // index of the current sweep (set by the sweep-start kernel)
   long long S_q;     // running description length (Q32)
   unsigned long long cum_q;   // accepted dS of the current sweep (Q32, two's complement)
   unsigned long long moves;   // accepted moves (whole phase)
@@ -161,7 +162,7 @@ struct NodalArgs {
   int B;
   const int32_t *dout, *din;
   int beg, end;
-  uint32_t itr, stage;
+  uint32_t stage;    // the sweep index is read from ctl->itr
   uint64_t seed;
   int32_t* move_to;
   int32_t* prop_s;        // optional, [end-beg]
@@ -214,8 +215,8 @@ void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* m
 void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
                          int update_degrees, int32_t* dout, int32_t* din, NodalCtl* ctl,
                          const CtlArgs& c, cudaStream_t st);
-void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int W,
-                            const long long* ide_q, const int* ide_n, cudaStream_t st);
+void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const long long* ide_q,
+                            const int* ide_n, cudaStream_t st);
 void launch_merge_sort_keys(int B, const long long* best_q, unsigned long long* keys, int32_t* idx,
                             cudaStream_t st);
 

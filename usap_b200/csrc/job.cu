@@ -120,8 +120,11 @@ Job::Job(int device) : device_(device) {
   USAP_CUDA(cudaStreamCreateWithFlags(&st_side_, cudaStreamNonBlocking));
   USAP_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
   USAP_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+  USAP_CUDA(cudaEventCreateWithFlags(&ev_wait_, cudaEventDisableTiming | cudaEventBlockingSync));
   nodal_configure(device);
   USAP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ctl_), sizeof(NodalCtl)));
+  USAP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ring_), 2 * sizeof(NodalCtl)));
+  for (auto& e : ev_sweep_) USAP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   dalloc(&ctl_, 1);
 }
 
@@ -132,11 +135,26 @@ Job::~Job() {
   dfree(ctl_);
   if (st_) cudaStreamSynchronize(st_);
   if (h_ctl_) cudaFreeHost(h_ctl_);
+  if (h_ring_) cudaFreeHost(h_ring_);
+  for (auto e : ev_sweep_)
+    if (e) cudaEventDestroy(e);
   for (auto e : ev_pool_) cudaEventDestroy(e);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
+  if (ev_wait_) cudaEventDestroy(ev_wait_);
   if (st_side_) cudaStreamDestroy(st_side_);
   if (st_) cudaStreamDestroy(st_);
+}
+
+// waits for the job's stream; with blocking waits the host thread sleeps
+// instead of spinning, so many concurrent jobs can share the host cores
+void Job::wait() {
+  if (blocking_wait_) {
+    USAP_CUDA(cudaEventRecord(ev_wait_, st_));
+    USAP_CUDA(cudaEventSynchronize(ev_wait_));
+  } else {
+    USAP_CUDA(cudaStreamSynchronize(st_));
+  }
 }
 
 void Job::free_graph() {
@@ -485,9 +503,9 @@ int32_t Job::merge_apply(int32_t* part, int32_t B, int32_t btm) {
   launch_merge_union(B, sidx_alt_, best_s_, btm, union_work_, root_, merged_dev_, st_);
   launch_merge_relabel(hg_->n, B, part, root_, present_, newlabel_, cub_tmp_, cub_bytes_, st_);
   int32_t merged = 0;
-  USAP_CUDA(cudaMemcpyAsync(&h_ctl_->pad0, merged_dev_, sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
-  USAP_CUDA(cudaStreamSynchronize(st_));
-  merged = h_ctl_->pad0;
+  USAP_CUDA(cudaMemcpyAsync(&h_ctl_->itr, merged_dev_, sizeof(int32_t), cudaMemcpyDeviceToHost, st_));
+  wait();
+  merged = h_ctl_->itr;
   return merged;
 }
 
@@ -501,9 +519,8 @@ void Job::entropy_launch(const int32_t* part, int32_t B, bool dense) {
   }
 }
 
-void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t itr,
-                      uint32_t stage, uint64_t seed, bool first_of_sweep, int stats,
-                      const CtlArgs& ctl_args) {
+void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t stage,
+                      uint64_t seed, bool first_of_sweep, int stats, const CtlArgs& ctl_args) {
   if (!dense && !first_of_sweep) sb_.build(g_, part, B, false, true, st_);
   NodalArgs a;
   a.out_ptr = g_.out_ptr;
@@ -522,7 +539,6 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
   a.din = din_;
   a.beg = beg;
   a.end = end;
-  a.itr = itr;
   a.stage = stage;
   a.seed = seed;
   a.move_to = move_to_;
@@ -563,6 +579,21 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
   launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, ctl_args, st_);
 }
 
+void Job::enqueue_sweep(int32_t* part, int32_t B, bool dense, uint32_t stage, uint64_t seed, int W,
+                        double thr, long long model_q, int stats) {
+  const int32_t n = hg_->n;
+  if (!dense) sb_.build(g_, part, B, false, true, st_);
+  entropy_launch(part, B, dense);
+  launch_ctl_sweep_start(ctl_, model_q, W, ide_q_, ide_n_, st_);
+  for (int32_t beg = 0; beg < n; beg += bs_) {
+    const int32_t end = beg + bs_ < n ? beg + bs_ : n;
+    const long long edges = (static_cast<long long>(hg_->out_ptr[end]) - hg_->out_ptr[beg]) +
+                            (static_cast<long long>(hg_->in_ptr[end]) - hg_->in_ptr[beg]);
+    const CtlArgs ca{1, W, thr, ide_q_, ide_n_, end - beg, edges};
+    nodal_batch(part, B, dense, beg, end, stage, seed, beg == 0, stats, ca);
+  }
+}
+
 void Job::emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part, bool dense,
                      long long S_q, int S_ninf, long long cum_q, int cum_ninf, long long moves) {
   const int32_t n = hg_->n;
@@ -574,7 +605,7 @@ void Job::emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int
   if (dense) {
     std::vector<int32_t> hm(static_cast<size_t>(ld_) * B);
     USAP_CUDA(cudaMemcpyAsync(hm.data(), M_, sizeof(int32_t) * hm.size(), cudaMemcpyDeviceToHost, st_));
-    USAP_CUDA(cudaStreamSynchronize(st_));
+    wait();
     for (int32_t i = 0; i < B; i++)
       for (int32_t j = 0; j < B; j++) {
         int32_t m = hm[static_cast<size_t>(i) * ld_ + j];
@@ -585,12 +616,12 @@ void Job::emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int
     SortedView v = sb_.view();
     int nnz = 0;
     USAP_CUDA(cudaMemcpyAsync(&nnz, sb_.nnz_dev(), sizeof(int), cudaMemcpyDeviceToHost, st_));
-    USAP_CUDA(cudaStreamSynchronize(st_));
+    wait();
     std::vector<int32_t> rp(B + 1), col(nnz), val(nnz);
     USAP_CUDA(cudaMemcpyAsync(rp.data(), v.rowptr, sizeof(int32_t) * (B + 1), cudaMemcpyDeviceToHost, st_));
     USAP_CUDA(cudaMemcpyAsync(col.data(), v.col, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st_));
     USAP_CUDA(cudaMemcpyAsync(val.data(), v.val, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost, st_));
-    USAP_CUDA(cudaStreamSynchronize(st_));
+    wait();
     for (int32_t i = 0; i < B; i++)
       for (int32_t p = rp[i]; p < rp[i + 1]; p++)
         if (val[p]) hM += mix64(mix64((static_cast<uint64_t>(i) << 32) | static_cast<uint32_t>(col[p])) ^ static_cast<uint64_t>(val[p]));
@@ -638,9 +669,10 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   const int32_t K = p.num_agg_proposals_per_block;
   const int32_t W = p.delta_entropy_moving_avg_window;
   const int32_t maxitr = p.max_num_nodal_itr;
-  int32_t bs = n / p.num_batch_nodal_update;
-  if (bs < 1) bs = 1;
+  bs_ = n / p.num_batch_nodal_update;
+  if (bs_ < 1) bs_ = 1;
   const int stats = p.stats ? 1 : 0;
+  const bool use_graphs = p.sweep_graphs != 0 && !stats;
   trace_mask_ = p.trace_kinds ? p.trace_kinds : 7;
   ev_used_ = 0;
   const LaunchCount lc0 = launch_count();
@@ -658,7 +690,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   ensure_capacity(B, K, dense_max, std::max(maxitr, 1));
   int32_t work = 0;
   USAP_CUDA(cudaMemcpyAsync(slots_[work], part0.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st_));
-  USAP_CUDA(cudaStreamSynchronize(st_));
+  wait();
   auto t_init = std::chrono::steady_clock::now();
   res->ms_init = std::chrono::duration<double, std::milli>(t_init - t_start).count();
 
@@ -692,30 +724,54 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     const double thr = isf ? p.delta_entropy_threshold2 : p.delta_entropy_threshold1;
     const long long model_q = q32_host(model_S(n, hg_->e, B));
     trace_prev_moves_ = 0;
-    for (int32_t itr = 0; itr < maxitr; itr++) {
-      if (!dense) sb_.build(g_, part, B, false, true, st_);
-      entropy_launch(part, B, dense);
-      launch_ctl_sweep_start(ctl_, model_q, itr, W, ide_q_, ide_n_, st_);
-      size_t ev_mark = ev_used_;
-      for (int32_t beg = 0; beg < n; beg += bs) {
-        const int32_t end = beg + bs < n ? beg + bs : n;
-        const long long edges = (static_cast<long long>(hg_->out_ptr[end]) - hg_->out_ptr[beg]) +
-                                (static_cast<long long>(hg_->in_ptr[end]) - hg_->in_ptr[beg]);
-        const CtlArgs ca{1, itr, W, thr, ide_q_, ide_n_, end - beg, edges};
-        nodal_batch(part, B, dense, beg, end, itr, stage, seed, beg == 0, stats, ca);
-        if (trace_on(2)) {
-          USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
-          USAP_CUDA(cudaStreamSynchronize(st_));
-          NodalCtl c = *h_ctl_;
-          emit_trace(2, stage, itr, beg, B, part, dense, c.S_q, c.S_ninf, static_cast<long long>(c.cum_q),
-                     c.cum_ninf, static_cast<long long>(c.moves) - trace_prev_moves_);
-          trace_prev_moves_ = static_cast<long long>(c.moves);
-          if (c.done) break;
+    if (!trace_on(2)) {
+      // the host keeps one sweep in flight ahead of the one it checks (a
+      // sweep queued after convergence returns at once); with sweep_graphs
+      // the sweep is recorded once per stage and replayed as a CUDA graph
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      LaunchCount per_sweep;
+      if (maxitr > 0 && use_graphs) {
+        const LaunchCount before = launch_count();
+        USAP_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        enqueue_sweep(part, B, dense, stage, seed, W, thr, model_q, 0);
+        USAP_CUDA(cudaStreamEndCapture(st_, &graph));
+        USAP_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        per_sweep.kernels = launch_count().kernels - before.kernels;
+        per_sweep.cub = launch_count().cub - before.cub;
+      }
+      int32_t launched = 0;
+      const size_t ev_mark = ev_used_;
+      auto launch_one = [&] {
+        if (exec) USAP_CUDA(cudaGraphLaunch(exec, st_));
+        else enqueue_sweep(part, B, dense, stage, seed, W, thr, model_q, stats);
+        USAP_CUDA(cudaMemcpyAsync(h_ring_ + (launched & 1), ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+        USAP_CUDA(cudaEventRecord(ev_sweep_[launched & 1], st_));
+        launched++;
+        d2h += sizeof(NodalCtl);
+      };
+      // an instrumented solve does not run ahead, so that no queued no-op
+      // sweep enters the kernel timings
+      const bool ahead = !stats;
+      if (maxitr > 0) launch_one();
+      for (int32_t itr = 0; itr < maxitr; itr++) {
+        if (ahead && itr + 1 < maxitr) launch_one();
+        USAP_CUDA(cudaEventSynchronize(ev_sweep_[itr & 1]));
+        if (h_ring_[itr & 1].done) break;
+        if (!ahead && itr + 1 < maxitr) launch_one();
+      }
+      wait();
+      if (launched > 0) *h_ctl_ = h_ring_[(launched - 1) & 1];
+      else std::memset(h_ctl_, 0, sizeof(NodalCtl));
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      if (exec) {
+        res->sweep_graph_launches += launched;
+        if (launched > 1) {   // recorded once, executed `launched` times
+          launch_count().kernels += per_sweep.kernels * (launched - 1);
+          launch_count().cub += per_sweep.cub * (launched - 1);
         }
       }
-      USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
-      USAP_CUDA(cudaStreamSynchronize(st_));
-      d2h += sizeof(NodalCtl);
       if (stats) {
         for (size_t i = ev_mark; i + 1 < ev_used_; i += 2) {
           float ms = 0;
@@ -725,7 +781,42 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
         }
         ev_used_ = ev_mark;
       }
-      if (h_ctl_->done) break;
+    } else {
+      for (int32_t itr = 0; itr < maxitr; itr++) {
+        size_t ev_mark = ev_used_;
+        {
+          if (!dense) sb_.build(g_, part, B, false, true, st_);
+          entropy_launch(part, B, dense);
+          launch_ctl_sweep_start(ctl_, model_q, W, ide_q_, ide_n_, st_);
+          for (int32_t beg = 0; beg < n; beg += bs_) {
+            const int32_t end = beg + bs_ < n ? beg + bs_ : n;
+            const long long edges = (static_cast<long long>(hg_->out_ptr[end]) - hg_->out_ptr[beg]) +
+                                    (static_cast<long long>(hg_->in_ptr[end]) - hg_->in_ptr[beg]);
+            const CtlArgs ca{1, W, thr, ide_q_, ide_n_, end - beg, edges};
+            nodal_batch(part, B, dense, beg, end, stage, seed, beg == 0, stats, ca);
+            USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+            wait();
+            NodalCtl c = *h_ctl_;
+            emit_trace(2, stage, itr, beg, B, part, dense, c.S_q, c.S_ninf, static_cast<long long>(c.cum_q),
+                       c.cum_ninf, static_cast<long long>(c.moves) - trace_prev_moves_);
+            trace_prev_moves_ = static_cast<long long>(c.moves);
+            if (c.done) break;
+          }
+        }
+        USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+        wait();
+        d2h += sizeof(NodalCtl);
+        if (stats) {
+          for (size_t i = ev_mark; i + 1 < ev_used_; i += 2) {
+            float ms = 0;
+            USAP_CUDA(cudaEventElapsedTime(&ms, ev_pool_[i], ev_pool_[i + 1]));
+            res->ms_nodal_kernel += ms;
+            res->nodal_kernel_launches++;
+          }
+          ev_used_ = ev_mark;
+        }
+        if (h_ctl_->done) break;
+      }
     }
     // the control block was read after the last sweep
     res->sweeps += static_cast<int64_t>(h_ctl_->sweeps);
@@ -739,7 +830,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     if (!dense) sb_.build(g_, part, B, false, true, st_);
     entropy_launch(part, B, dense);
     USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
-    USAP_CUDA(cudaStreamSynchronize(st_));
+    wait();
     const long long S_fin = model_q - static_cast<long long>(h_ctl_->entropy_acc);
     d2h += sizeof(NodalCtl);
     auto tn1 = std::chrono::steady_clock::now();
@@ -755,7 +846,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       if (out_assign)
         USAP_CUDA(cudaMemcpyAsync(out_assign, slots_[gs.med.slot], sizeof(int32_t) * n,
                                   cudaMemcpyDeviceToHost, st_));
-      USAP_CUDA(cudaStreamSynchronize(st_));
+      wait();
       auto td1 = std::chrono::steady_clock::now();
       res->ms_d2h = std::chrono::duration<double, std::milli>(td1 - td0).count();
       if (out_assign) d2h += static_cast<long long>(sizeof(int32_t)) * n;
@@ -884,9 +975,10 @@ void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t be
   const bool dense = B <= dense_max;
   prepare_nodal_blocks(slots_[0], B, dense);
   USAP_CUDA(cudaMemsetAsync(ctl_, 0, sizeof(NodalCtl), st_));
-  const CtlArgs ca{0, 0, 1, 0.0, ide_q_, ide_n_, 0, 0};
-  nodal_batch(slots_[0], B, dense, beg, end, static_cast<uint32_t>(itr), static_cast<uint32_t>(stage), seed,
-              true, 2, ca);
+  h_ctl_->itr = itr;
+  USAP_CUDA(cudaMemcpyAsync(&ctl_->itr, &h_ctl_->itr, sizeof(int), cudaMemcpyHostToDevice, st_));
+  const CtlArgs ca{0, 1, 0.0, ide_q_, ide_n_, 0, 0};
+  nodal_batch(slots_[0], B, dense, beg, end, static_cast<uint32_t>(stage), seed, true, 2, ca);
   const int32_t cnt = end - beg;
   USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_->n, cudaMemcpyDeviceToHost, st_));
   if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, rp_s_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));

@@ -86,6 +86,8 @@ class Job {
     return hg_ ? *hg_ : empty;
   }
   const std::shared_ptr<GraphResident>& graph() const { return gr_; }
+  // host threads sleep (instead of spinning) while waiting for the device
+  void set_blocking_wait(bool on) { blocking_wait_ = on; }
   void set_trace(usap_trace_fn fn, void* user) {
     trace_ = fn;
     trace_user_ = user;
@@ -117,9 +119,12 @@ class Job {
   void merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage, uint64_t seed);
   int32_t merge_apply(int32_t* part, int32_t B, int32_t btm);
   void entropy_launch(const int32_t* part, int32_t B, bool dense);
-  void nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t itr,
-                   uint32_t stage, uint64_t seed, bool first_of_sweep, int stats,
-                   const CtlArgs& ctl_args);
+  void nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t stage,
+                   uint64_t seed, bool first_of_sweep, int stats, const CtlArgs& ctl_args);
+  // one nodal sweep (entropy, sweep start, every batch), launched directly
+  // or recorded into a CUDA graph
+  void enqueue_sweep(int32_t* part, int32_t B, bool dense, uint32_t stage, uint64_t seed, int W,
+                     double thr, long long model_q, int stats);
   void emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part,
                   bool dense, long long S_q, int S_ninf, long long cum_q, int cum_ninf,
                   long long moves);
@@ -132,12 +137,18 @@ class Job {
   cudaStream_t st_ = nullptr;
   cudaStream_t st_side_ = nullptr;   // hub CTAs overlap the warp kernel here
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  cudaEvent_t ev_wait_ = nullptr;
+  cudaEvent_t ev_sweep_[2] = {nullptr, nullptr};   // sweep done + control copied
+  NodalCtl* h_ring_ = nullptr;                     // pinned, two control copies
+  bool blocking_wait_ = false;
+  void wait();
   std::shared_ptr<GraphResident> gr_;
   const HostGraph* hg_ = nullptr;
   GraphDev g_;                       // the graph's arrays + this job's hub scratch
   int32_t *hkey_ = nullptr, *hwo_ = nullptr, *hwi_ = nullptr;
   // state
   int32_t bcap_ = 0, kcap_ = 0, dcap_ = 0, icap_ = 0;
+  int32_t bs_ = 1;   // nodal batch size of the current solve
   int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t* move_to_ = nullptr;
   int32_t *dout_ = nullptr, *din_ = nullptr;

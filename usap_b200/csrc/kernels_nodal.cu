@@ -165,7 +165,8 @@ template <class Ops>
 __device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops, int v,
                                               const VertexInfo& vi, int lane, int* scanned) {
   const int B = a.B;
-  const Draws x = philox(static_cast<uint32_t>(v), a.itr, a.stage, kTagNodal, a.seed);
+  const Draws x = philox(static_cast<uint32_t>(v), static_cast<uint32_t>(a.ctl->itr), a.stage, kTagNodal,
+                         a.seed);
   const long long k = vi.kout + vi.kin;
   if (k == 0) return static_cast<int>(draw_below(x.x2, B));
   const long long t = draw_below(x.x0, k);
@@ -589,14 +590,15 @@ __global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__
 __device__ __forceinline__ void ctl_batch_end(NodalCtl* ctl, const CtlArgs& c) {
   if (ctl->done) return;
   const long long cum = static_cast<long long>(ctl->cum_q);
-  c.ide_q[c.itr] = cum;
-  c.ide_n[c.itr] = ctl->cum_ninf;
+  const int itr = ctl->itr;
+  c.ide_q[itr] = cum;
+  c.ide_n[itr] = ctl->cum_ninf;
   ctl->S_q += cum;
   ctl->S_ninf |= ctl->cum_ninf;
   ctl->batches++;
   ctl->proposals += c.batch_vertices;
   ctl->edge_visits += c.batch_edges;
-  if (c.itr >= c.W - 1) {
+  if (itr >= c.W - 1) {
     double S_d = ctl->S_ninf ? -INFINITY : static_cast<double>(ctl->S_q) / kQ32;
     if (-ctl->mean < c.thr * S_d) ctl->done = 1;
   }
@@ -627,9 +629,11 @@ __global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__
 
 // prepare_batch (:381-395): S from the entropy kernel, the moving average
 // of the previous sweeps' dS, and a fresh cumulative sum for this sweep
-__global__ void k_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int W,
-                                  const long long* ide_q, const int* ide_n) {
+__global__ void k_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const long long* ide_q,
+                                  const int* ide_n) {
   if (ctl->done) return;
+  const int itr = static_cast<int>(ctl->sweeps);
+  ctl->itr = itr;
   ctl->S_q = model_q - static_cast<long long>(ctl->entropy_acc);
   ctl->S_ninf = 0;
   double mean = 0.0;
@@ -732,9 +736,9 @@ void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int
   USAP_LAUNCHED();
 }
 
-void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int itr, int W, const long long* ide_q,
+void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const long long* ide_q,
                             const int* ide_n, cudaStream_t st) {
-  k_ctl_sweep_start<<<1, 1, 0, st>>>(ctl, model_q, itr, W, ide_q, ide_n);
+  k_ctl_sweep_start<<<1, 1, 0, st>>>(ctl, model_q, W, ide_q, ide_n);
   USAP_LAUNCHED();
 }
 

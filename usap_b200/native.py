@@ -42,7 +42,8 @@ class Params(C.Structure):
                 ("delta_entropy_moving_avg_window", C.c_int32), ("verbose", C.c_int32),
                 ("dfs_depth", C.c_int32), ("t_block_num", C.c_int32), ("seed", C.c_uint64),
                 ("init_mode", C.c_int32), ("dense_max", C.c_int32), ("device", C.c_int32),
-                ("stats", C.c_int32), ("trace_kinds", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("stats", C.c_int32), ("trace_kinds", C.c_int32), ("sweep_graphs", C.c_int32),
+                ("reserved", C.c_int32 * 4)]
 
 
 class Result(C.Structure):
@@ -54,7 +55,8 @@ class Result(C.Structure):
                 ("ms_nodal", C.c_double), ("ms_h2d", C.c_double), ("ms_d2h", C.c_double),
                 ("ms_nodal_kernel", C.c_double), ("nodal_kernel_launches", C.c_int64),
                 ("nodal_kernel_bytes", C.c_double), ("kernel_launches", C.c_int64),
-                ("cub_calls", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
+                ("cub_calls", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+                ("sweep_graph_launches", C.c_int64)]
 
 
 class Scores(C.Structure):

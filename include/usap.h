@@ -202,6 +202,37 @@ usap_status usap_op_nodal_batch(usap_ctx* ctx, int32_t* part, int32_t B, int32_t
                                 int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
                                 int64_t* moves);
 
+/* --- allocation-free scoring (no counterpart in the reference) ----------- */
+/* The reference has no such entry point: it exists for callers that cannot
+ * allocate device memory at the moment they need a score (a host whose own
+ * allocator already owns the memory budget, or a loop that cannot take the
+ * device-wide synchronisation of cudaMalloc/cudaFree).
+ *
+ * Same value as usap_op_entropy (Q32 description length of `part`, model
+ * term minus data term), but every pointer is a DEVICE pointer on the
+ * current device: src/dst (e entries, 0-based, in [0, n)), weight (NULL for
+ * unit weights), part (n entries in [0, B)) and the output S_q (one int64).
+ * The kernels run on `stream` (a cudaStream_t; NULL = default stream) and
+ * the result is ready in stream order; the call does not wait for it.
+ *
+ * Nothing is allocated: the work uses one fixed scratch array per device
+ * inside this library.  Limits: 1 <= B <= USAP_STATIC_MAX_BLOCKS and
+ * e <= USAP_STATIC_MAX_WEIGHT (USAP_ERR_LIMIT beyond them); the total edge
+ * weight must also be <= USAP_STATIC_MAX_WEIGHT.  Inputs that fail the
+ * device-side checks (an id out of range, a negative weight, too much total
+ * weight) make *S_q = INT64_MIN.
+ *
+ * The first call on a device does a one-time set-up on the calling thread
+ * (locates the array and fills its log table, with synchronous copies):
+ * make that first call before any stream capture.  Every call on a device
+ * shares the one array: calls that overlap in time (on different streams,
+ * or from different threads without ordering) race and give wrong results. */
+#define USAP_STATIC_MAX_BLOCKS 1024
+#define USAP_STATIC_MAX_WEIGHT 1048576
+usap_status usap_entropy_static(const int32_t* src, const int32_t* dst, const int32_t* weight,
+                                int64_t e, int32_t n, const int32_t* part, int32_t B,
+                                int64_t* S_q, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,8 @@ void check_ctx(usap_ctx* ctx) {
 
 }  // namespace
 
+int usap::call_guarded(const std::function<void()>& f) { return guarded(f); }
+
 extern "C" {
 
 const char* usap_version(void) { return "usap-b200 0.1 (sm_100a)"; }

@@ -16,6 +16,7 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -36,6 +37,10 @@ class Error : public std::runtime_error {
 
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
 #define USAP_CUDA(x) ::usap::cuda_check((x), #x, __FILE__, __LINE__)
+
+// runs f, turning an exception into a status and the calling thread's
+// last-error message, as every extern "C" entry point does
+int call_guarded(const std::function<void()>& f);
 
 // launches of this library's own kernels and of CUB primitives on the
 // calling thread (reported per solve)

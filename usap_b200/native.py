@@ -92,7 +92,7 @@ EXPORTS = ("usap_version", "usap_last_error", "usap_params_default", "usap_parti
            "usap_evaluate", "usap_ctx_create", "usap_ctx_destroy", "usap_ctx_load",
            "usap_ctx_num_nodes", "usap_ctx_partition", "usap_ctx_set_trace", "usap_op_scc",
            "usap_op_build", "usap_op_entropy", "usap_op_merge_phase", "usap_op_merge_apply",
-           "usap_op_nodal_batch", "usap_batch_partition")
+           "usap_op_nodal_batch", "usap_batch_partition", "usap_entropy_static")
 
 _lib = None
 
@@ -131,6 +131,8 @@ def lib() -> C.CDLL:
     L.usap_batch_partition.argtypes = [C.POINTER(Graph), C.c_int32, C.POINTER(Params),
                                        C.POINTER(BatchJob), C.c_int32, C.c_int32, C.c_int32,
                                        C.POINTER(BatchStats)]
+    L.usap_entropy_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32,
+                                      C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name.startswith("usap_") and name not in ("usap_version", "usap_last_error",

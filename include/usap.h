@@ -76,7 +76,10 @@ typedef struct usap_params {
   int32_t stats;       /* 1: per-kernel CUDA-event timings and algorithmic byte counts */
   int32_t trace_kinds; /* trace events to emit: bit k-1 for kind k; 0 = all kinds */
   int32_t sweep_graphs;/* 1: record each stage's nodal sweep as a CUDA graph and replay it */
-  int32_t reserved[4];
+  int32_t persistent;  /* 1 (default): run each stage's nodal phase as one cooperative kernel
+                          when the tile is dense and B <= 4096; 0: one launch per batch.
+                          usap_batch_partition always uses per-batch launches. */
+  int32_t reserved[3];
 } usap_params;
 
 typedef struct usap_result {

@@ -194,6 +194,41 @@ def test_full_solve_trace_exact(api, oracle, graph, params):
         assert res_g[k] == res_o[k], k
 
 
+@pytest.mark.parametrize("graph,params", [
+    ("c0", {"num_batch_nodal_update": 10, "seed": 0}),
+    ("weighted", {"num_batch_nodal_update": 7, "seed": 2}),
+    ("hub", {"num_batch_nodal_update": 10, "seed": 9}),
+    ("sbm300", {"num_batch_nodal_update": 3, "seed": 5, "init_mode": 1}),
+])
+def test_persistent_phase_exact(api, oracle, graph, params):
+    """The persistent nodal kernel (one launch per stage) against the oracle
+    at every stage boundary (kinds 1 and 3: block structures after the merge
+    and after the nodal phase), and against per-batch launches."""
+    from usap_b200 import native as nat
+    n, src, dst, w = GRAPHS[graph]()
+    ctx = api.Context(0)
+    ctx.load(src, dst, w, n)
+    runs = []
+    for persistent in (1, 0):
+        ev = []
+        ctx.set_trace(ev.append)
+        part, res = ctx.partition(nat.default_params(trace_kinds=0b101, persistent=persistent, **params))
+        ctx.set_trace(None)
+        runs.append((part, res, ev))
+    ctx.close()
+    og = oracle.OracleGraph(n, src, dst, w)
+    part_o, res_o, ev_o = og.partition(params, trace=True)
+    ev_o = [e for e in ev_o if e["kind"] in (1, 3)]
+    for part, res, ev in runs:
+        assert len(ev) == len(ev_o)
+        for i, (a, b) in enumerate(zip(ev, ev_o)):
+            assert a == b, (graph, i, a, b)
+        assert np.array_equal(part, part_o)
+        for k in ("B", "S_q", "stages", "sweeps", "batches", "nodal_proposals", "nodal_moves",
+                  "near_threshold"):
+            assert res[k] == res_o[k], k
+
+
 @pytest.mark.parametrize("within,alpha,seed", [(0.8, 10.0, 0), (0.5, 1.0, 1), (0.8, 1.0, 2),
                                                (0.5, 10.0, 3)])
 def test_c1_solve_exact(api, oracle, within, alpha, seed):

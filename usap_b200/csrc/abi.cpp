@@ -76,6 +76,7 @@ void usap_params_default(usap_params* p) {
   p->dense_max = 4096;
   p->device = 0;
   p->stats = 0;
+  p->persistent = 1;
 }
 
 usap_status usap_partition(const usap_graph* g, const usap_params* p, int32_t* out_assign,
@@ -215,6 +216,7 @@ usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, cons
           try {
             job->attach(res[bj.graph]);
             usap_params prm = base;
+            prm.persistent = 0;   // concurrent jobs: per-batch launches interleave
             prm.seed = bj.seed;
             job->partition(prm, bj.out_assign, &bj.result);
             bj.status = USAP_OK;

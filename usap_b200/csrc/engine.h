@@ -139,6 +139,12 @@ struct NodalCtl {
   double mean;       // moving average of the previous sweeps' dS
   unsigned long long entropy_acc;  // data term accumulator of the entropy kernel
   unsigned long long bytes;        // algorithmic bytes of the nodal kernel (stats)
+  unsigned int apply_done;         // CTAs of the apply kernel that have finished
+  // persistent kernel: grid barrier (arrivals, generation, timeout flag)
+  // and the counter that hands out a batch's vertices
+  unsigned long long bar;   // arrivals (low 32 bits) + convergence flag (bit 32)
+  int bar_err;
+  unsigned int vnext;
 };
 
 struct GraphDev {
@@ -149,7 +155,11 @@ struct GraphDev {
   int32_t *src = nullptr, *dst = nullptr, *w = nullptr;
   int32_t *out_ptr = nullptr, *out_idx = nullptr, *out_w = nullptr;
   int32_t *in_ptr = nullptr, *in_idx = nullptr, *in_w = nullptr;
-  int32_t *out_src = nullptr, *in_dst = nullptr;   // owner vertex of each CSR position
+  // 32-edge chunks of every vertex's out- then in-list, (vertex, chunk index)
+  // in vertex order; a vertex without edges has one empty chunk
+  int2* chunks = nullptr;
+  int64_t nchunks = 0;
+  int64_t* chunk_ptr = nullptr;   // first chunk of each vertex (n + 1)
   int32_t *kout = nullptr, *kin = nullptr;
   double* logk = nullptr;
   // per-vertex global hash region for vertices too large for shared memory
@@ -169,7 +179,8 @@ struct NodalArgs {
   int beg, end;
   uint32_t stage;    // the sweep index is read from ctl->itr
   uint64_t seed;
-  int32_t* move_to;
+  int32_t* move_to;       // per batch vertex: the accepted target, or -1
+  int32_t* from;          // per batch vertex: its block at the batch start
   int32_t* prop_s;        // optional, [end-beg]
   long long* prop_q;
   int32_t* prop_ninf;
@@ -187,6 +198,23 @@ struct MergeArgs {
   const int32_t *dout, *din;
   int32_t* prop_s;   // [B*K]
   long long* prop_q;
+};
+
+// Arguments of the persistent nodal-phase kernel (dense tile only).
+struct PhaseArgs {
+  NodalArgs a;              // beg / end are set per batch inside the kernel
+  DenseView v;
+  GraphDev g;
+  int32_t *part, *dout, *din;
+  int *M, *Mt, *CS;         // the tile behind `v`, written by the apply pass
+  const int32_t* hubs;      // hub vertex ids, ascending
+  const int32_t* batch_hub; // first hub of each batch (batches + 1 entries)
+  const int64_t* chunk_ptr;
+  int n, bs, maxitr, W;
+  double thr;
+  long long model_q;
+  long long* ide_q;
+  int* ide_n;
 };
 
 // --- launchers (kernels_*.cu) -------------------------------------------------
@@ -209,14 +237,22 @@ void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int3
                           int32_t* newlabel, void* cub_tmp, size_t cub_bytes, cudaStream_t st);
 
 void nodal_configure(int device);
+// grid of the persistent nodal kernel on `device` (0: not available)
+int nodal_phase_grid(int device);
+// largest B whose hub tables fit the persistent kernel's shared memory
+int nodal_phase_max_blocks();
+void launch_nodal_phase(const PhaseArgs& p, int grid, cudaStream_t st);
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
                                 const StreamPair& sp);
 void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,
                                  const StreamPair& sp);
 void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st);
-void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int o0,
-                              int n_out, int i0, int n_in, int ld, int* M, int* Mt, int cld, int* CS,
-                              cudaStream_t st);
+// applies and commits the moves of batch [beg, end) on the dense tile
+// (chunks [c0, c1) of GraphDev::chunks); runs the batch-end bookkeeping
+void launch_nodal_apply_commit_dense(const GraphDev& g, int32_t* part, const int32_t* move_to,
+                                     const int32_t* from, int beg, int end, int64_t c0, int64_t c1,
+                                     int ld, int* M, int* Mt, int cld, int* CS, int32_t* dout,
+                                     int32_t* din, NodalCtl* ctl, const CtlArgs& c, cudaStream_t st);
 void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
                          int update_degrees, int32_t* dout, int32_t* din, NodalCtl* ctl,
                          const CtlArgs& c, cudaStream_t st);

@@ -166,7 +166,9 @@ void Job::free_graph() {
 
 void Job::free_state() {
   for (auto& s : slots_) dfree(s);
-  dfree(move_to_); dfree(dout_); dfree(din_);
+  dfree(move_to_); dfree(from_); dfree(dout_); dfree(din_); dfree(batch_hub_);
+  batch_hub_bs_ = 0;
+  batch_hub_cap_ = 0;
   dfree(M_); dfree(Mt_); dfree(CS_);
   sb_.release(st_);
   dfree(prop_s_); dfree(prop_q_); dfree(best_s_); dfree(best_q_);
@@ -301,13 +303,25 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   up(&g.kout, h.kout);
   up(&g.kin, h.kin);
   {
-    std::vector<int32_t> osrc(h.e), idst(h.e);
+    h.chunk_ptr.assign(static_cast<size_t>(n) + 1, 0);
     for (int32_t v = 0; v < n; v++) {
-      for (int32_t p = h.out_ptr[v]; p < h.out_ptr[v + 1]; p++) osrc[p] = v;
-      for (int32_t p = h.in_ptr[v]; p < h.in_ptr[v + 1]; p++) idst[p] = v;
+      const int64_t deg = (h.out_ptr[v + 1] - h.out_ptr[v]) + (h.in_ptr[v + 1] - h.in_ptr[v]);
+      h.chunk_ptr[v + 1] = h.chunk_ptr[v] + std::max<int64_t>(1, (deg + 31) / 32);
     }
-    up(&g.out_src, osrc);
-    up(&g.in_dst, idst);
+    g.nchunks = h.chunk_ptr[n];
+    std::vector<int32_t> ch(2 * static_cast<size_t>(g.nchunks));
+    for (int32_t v = 0; v < n; v++)
+      for (int64_t q = h.chunk_ptr[v]; q < h.chunk_ptr[v + 1]; q++) {
+        ch[2 * q] = v;
+        ch[2 * q + 1] = static_cast<int32_t>(q - h.chunk_ptr[v]);
+      }
+    int32_t* d = nullptr;
+    up(&d, ch);
+    g.chunks = reinterpret_cast<int2*>(d);
+    dalloc(&g.chunk_ptr, h.chunk_ptr.size());
+    USAP_CUDA(cudaMemcpyAsync(g.chunk_ptr, h.chunk_ptr.data(), sizeof(int64_t) * h.chunk_ptr.size(),
+                              cudaMemcpyHostToDevice, st_));
+    up_bytes += static_cast<long long>(sizeof(int64_t) * h.chunk_ptr.size());
   }
   dalloc(&g.logk, wtot + 1);
   USAP_CUDA(cudaMemcpyAsync(g.logk, logk_all->data(), sizeof(double) * (wtot + 1), cudaMemcpyHostToDevice, st_));
@@ -344,7 +358,7 @@ GraphResident::~GraphResident() {
   dfree(g.src); dfree(g.dst); dfree(g.w);
   dfree(g.out_ptr); dfree(g.out_idx); dfree(g.out_w);
   dfree(g.in_ptr); dfree(g.in_idx); dfree(g.in_w);
-  dfree(g.out_src); dfree(g.in_dst);
+  dfree(g.chunks); dfree(g.chunk_ptr);
   dfree(g.kout); dfree(g.kin); dfree(g.logk);
   dfree(g.hi_off);
   dfree(hubs_dev);
@@ -406,6 +420,7 @@ void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxit
     for (auto& s : slots_) dalloc(&s, n);
     dalloc(&move_to_, n);
     USAP_CUDA(cudaMemsetAsync(move_to_, 0xff, sizeof(int32_t) * n, st_));
+    dalloc(&from_, n);
     dalloc(&rp_s_, n);
     dalloc(&rp_n_, n);
     dalloc(&rp_q_, n);
@@ -519,9 +534,8 @@ void Job::entropy_launch(const int32_t* part, int32_t B, bool dense) {
   }
 }
 
-void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t stage,
-                      uint64_t seed, bool first_of_sweep, int stats, const CtlArgs& ctl_args) {
-  if (!dense && !first_of_sweep) sb_.build(g_, part, B, false, true, st_);
+NodalArgs Job::nodal_args(int32_t* part, int32_t B, int32_t beg, int32_t end, uint32_t stage, uint64_t seed,
+                          int stats) const {
   NodalArgs a;
   a.out_ptr = g_.out_ptr;
   a.out_idx = g_.out_idx;
@@ -542,6 +556,7 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
   a.stage = stage;
   a.seed = seed;
   a.move_to = move_to_;
+  a.from = from_;
   a.prop_s = nullptr;
   a.prop_q = nullptr;
   a.prop_ninf = nullptr;
@@ -556,6 +571,13 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
     a.prop_q = rp_q_;
     a.prop_ninf = rp_n_;
   }
+  return a;
+}
+
+void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t stage,
+                      uint64_t seed, bool first_of_sweep, int stats, const CtlArgs& ctl_args) {
+  if (!dense && !first_of_sweep) sb_.build(g_, part, B, false, true, st_);
+  const NodalArgs a = nodal_args(part, B, beg, end, stage, seed, stats);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (stats == 1) {
     while (ev_pool_.size() < ev_used_ + 2) {
@@ -572,11 +594,74 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
   else launch_nodal_propose_sorted(a, sb_.view(), hubs, streams());
   if (stats == 1) USAP_CUDA(cudaEventRecord(e1, st_));
   if (dense) {
-    const int o0 = hg_->out_ptr[beg], i0 = hg_->in_ptr[beg];
-    launch_nodal_apply_dense(g_, part, move_to_, o0, hg_->out_ptr[end] - o0, i0, hg_->in_ptr[end] - i0, ld_,
-                             M_, Mt_, cld_, CS_, st_);
+    launch_nodal_apply_commit_dense(g_, part, move_to_, from_, beg, end, hg_->chunk_ptr[beg],
+                                    hg_->chunk_ptr[end], ld_, M_, Mt_, cld_, CS_, dout_, din_, ctl_,
+                                    ctl_args, st_);
+  } else {
+    launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, ctl_args, st_);
   }
-  launch_nodal_commit(g_, part, move_to_, beg, end, 1, dout_, din_, ctl_, ctl_args, st_);
+}
+
+float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, int W, double thr,
+                       long long model_q, int32_t maxitr, int stats, int grid, bool timed) {
+  const int32_t n = hg_->n;
+  const int32_t nb = (n + bs_ - 1) / bs_;
+  if (batch_hub_bs_ != bs_) {   // first hub of each batch, for this batch size
+    const std::vector<int32_t>& hub_ids = gr_->hub_ids;
+    std::vector<int32_t> bh(static_cast<size_t>(nb) + 1);
+    for (int32_t b = 0; b <= nb; b++) {
+      const int32_t v = static_cast<int32_t>(std::min<int64_t>(static_cast<int64_t>(b) * bs_, n));
+      bh[b] = static_cast<int32_t>(std::lower_bound(hub_ids.begin(), hub_ids.end(), v) - hub_ids.begin());
+    }
+    if (batch_hub_cap_ < nb + 1) {
+      dfree(batch_hub_);
+      dalloc(&batch_hub_, nb + 1);
+      batch_hub_cap_ = nb + 1;
+    }
+    USAP_CUDA(cudaMemcpyAsync(batch_hub_, bh.data(), sizeof(int32_t) * bh.size(), cudaMemcpyHostToDevice, st_));
+    wait();
+    batch_hub_bs_ = bs_;
+  }
+  PhaseArgs pa;
+  pa.a = nodal_args(part, B, 0, 0, stage, seed, stats);
+  pa.v = dense_view();
+  pa.g = g_;
+  pa.part = part;
+  pa.dout = dout_;
+  pa.din = din_;
+  pa.M = M_;
+  pa.Mt = Mt_;
+  pa.CS = CS_;
+  pa.hubs = gr_->hubs_dev;
+  pa.batch_hub = batch_hub_;
+  pa.chunk_ptr = g_.chunk_ptr;
+  pa.n = n;
+  pa.bs = bs_;
+  pa.maxitr = maxitr;
+  pa.W = W;
+  pa.thr = thr;
+  pa.model_q = model_q;
+  pa.ide_q = ide_q_;
+  pa.ide_n = ide_n_;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (timed) {
+    while (ev_pool_.size() < ev_used_ + 2) {
+      cudaEvent_t e;
+      USAP_CUDA(cudaEventCreate(&e));
+      ev_pool_.push_back(e);
+    }
+    e0 = ev_pool_[ev_used_];
+    e1 = ev_pool_[ev_used_ + 1];
+    USAP_CUDA(cudaEventRecord(e0, st_));
+  }
+  launch_nodal_phase(pa, grid, st_);
+  if (timed) USAP_CUDA(cudaEventRecord(e1, st_));
+  USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+  wait();
+  if (h_ctl_->bar_err) throw Error(USAP_ERR_INTERNAL, "persistent nodal kernel: a grid barrier timed out");
+  float ms = 0;
+  if (timed) USAP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  return ms;
 }
 
 void Job::enqueue_sweep(int32_t* part, int32_t B, bool dense, uint32_t stage, uint64_t seed, int W,
@@ -724,7 +809,18 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     const double thr = isf ? p.delta_entropy_threshold2 : p.delta_entropy_threshold1;
     const long long model_q = q32_host(model_S(n, hg_->e, B));
     trace_prev_moves_ = 0;
-    if (!trace_on(2)) {
+    const int pgrid = p.persistent && dense && !use_graphs && maxitr > 0 && B <= nodal_phase_max_blocks() &&
+                              !trace_on(2)
+                          ? nodal_phase_grid(device_)
+                          : 0;
+    if (pgrid > 0) {
+      const float ms = nodal_phase(part, B, stage, seed, W, thr, model_q, maxitr, stats, pgrid, stats != 0);
+      d2h += sizeof(NodalCtl);
+      if (stats) {
+        res->ms_nodal_kernel += ms;
+        res->nodal_kernel_launches++;
+      }
+    } else if (!trace_on(2)) {
       // the host keeps one sweep in flight ahead of the one it checks (a
       // sweep queued after convergence returns at once); with sweep_graphs
       // the sweep is recorded once per stage and replayed as a CUDA graph

@@ -20,6 +20,8 @@ struct HostGraph {
   // in-lists ordered by source vertex id (the transpose _scc builds,
   // graph_parallel.hpp:518-523), prepared once at load
   std::vector<int32_t> tptr, tidx;
+  // first 32-edge chunk of each vertex (n + 1 entries; GraphDev::chunks)
+  std::vector<int64_t> chunk_ptr;
 };
 
 // _scc + _dfs_itr (graph_parallel.hpp:514-603), host side; scc_prepare
@@ -121,6 +123,12 @@ class Job {
   void entropy_launch(const int32_t* part, int32_t B, bool dense);
   void nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t stage,
                    uint64_t seed, bool first_of_sweep, int stats, const CtlArgs& ctl_args);
+  NodalArgs nodal_args(int32_t* part, int32_t B, int32_t beg, int32_t end, uint32_t stage, uint64_t seed,
+                       int stats) const;
+  // a stage's whole nodal phase in one persistent launch (dense tile);
+  // returns the kernel's duration in ms when `timed`
+  float nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, int W, double thr,
+                    long long model_q, int32_t maxitr, int stats, int grid, bool timed);
   // one nodal sweep (entropy, sweep start, every batch), launched directly
   // or recorded into a CUDA graph
   void enqueue_sweep(int32_t* part, int32_t B, bool dense, uint32_t stage, uint64_t seed, int W,
@@ -151,6 +159,10 @@ class Job {
   int32_t bs_ = 1;   // nodal batch size of the current solve
   int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t* move_to_ = nullptr;
+  int32_t* from_ = nullptr;
+  int32_t* batch_hub_ = nullptr;     // first hub of each batch of size bs_
+  int32_t batch_hub_bs_ = 0;
+  int32_t batch_hub_cap_ = 0;
   int32_t *dout_ = nullptr, *din_ = nullptr;
   int *M_ = nullptr, *Mt_ = nullptr, *CS_ = nullptr;
   int ld_ = 0, cld_ = 0;

@@ -20,10 +20,19 @@
 // reference's rule that in-edges from blocks r and s do not adjust the 2x2
 // row entries (the adjustment is commented out at :1135-1142) and that
 // column sums skip i in {r,s} is kept.  Accepted moves are written to
-// move_to[]; a second kernel applies them to the dense tile by +/-w deltas
-// (exact integers, so order does not matter), a third commits the
-// partition.  The convergence bookkeeping of the update task runs in a
-// one-thread kernel so batches and sweeps queue without host round trips.
+// move_to[]; they are applied to the dense tile by +/-w deltas (exact
+// integers, so order does not matter) and committed together with the
+// partition.  The convergence bookkeeping of the update task runs on the
+// device, so batches and sweeps queue without host round trips.
+//
+// Two schedules run the same device code.  Per batch launches: a proposal
+// kernel (hubs in a second kernel on a side stream) and an apply kernel.
+// Persistent: one cooperative launch runs a stage's whole nodal phase,
+// one 1024-thread CTA per SM, with grid barriers between entropy, sweep
+// start, proposals and apply; it removes the launch gaps that otherwise
+// cost about half of each batch.  State written inside that kernel (the
+// partition, M, degrees, chunk sums, moves) is read through L2 (ld.cg);
+// the non-coherent path is used only for data that no phase writes.
 #include <cmath>
 #include <mutex>
 
@@ -39,6 +48,19 @@ namespace usap {
 
 namespace {
 
+// Load policies for the state a nodal batch reads: the partition, the
+// block degrees and M.  LdNC (ld.global.nc) when the state is read-only
+// for the whole launch; LdCG (L2, coherent) in the persistent kernel,
+// whose later phases read what earlier phases wrote.
+struct LdNC {
+  template <class T>
+  __device__ __forceinline__ static T ld(const T* p) { return __ldg(p); }
+};
+struct LdCG {
+  template <class T>
+  __device__ __forceinline__ static T ld(const T* p) { return __ldcg(p); }
+};
+
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kHCap = 256;          // shared-memory hash slots per warp
@@ -46,11 +68,13 @@ constexpr int kChunk = 128;         // blocks per chunk sum of a dense row
 constexpr int kHubThreads = 512;    // threads of a hub CTA
 constexpr int kHubWarps = kHubThreads / 32;
 
-struct DenseOps {
+template <class LD>
+struct DenseOpsT {
+  using Ld = LD;
   DenseView v;
   int B;
   __device__ __forceinline__ int get(int x, int y) const {
-    return __ldg(v.M + static_cast<long long>(x) * v.ld + y);
+    return LD::ld(v.M + static_cast<long long>(x) * v.ld + y);
   }
   // first block i (block-id order) whose cumulative M[u,i]+M[i,u] exceeds t:
   // a warp scan over the row's chunk sums, then over the 128 entries of the
@@ -63,7 +87,7 @@ struct DenseOps {
     int c = nch - 1;
     for (int base = 0; base < nch; base += 32) {
       const int cc = base + lane;
-      const int val = cc < nch ? __ldg(cs + cc) : 0;
+      const int val = cc < nch ? LD::ld(cs + cc) : 0;
       const int incl = warp_incl_scan(val, lane);
       const int total = __shfl_sync(0xffffffffu, incl, 31);
       if (run + total > t) {
@@ -78,8 +102,8 @@ struct DenseOps {
     const int i0 = c * kChunk + lane * 4;
     int p0 = 0, p1 = 0, p2 = 0, p3 = 0;
     if (i0 < B) {
-      const int4 a = __ldg(reinterpret_cast<const int4*>(v.M + static_cast<long long>(u) * v.ld + i0));
-      const int4 b = __ldg(reinterpret_cast<const int4*>(v.Mt + static_cast<long long>(u) * v.ld + i0));
+      const int4 a = LD::ld(reinterpret_cast<const int4*>(v.M + static_cast<long long>(u) * v.ld + i0));
+      const int4 b = LD::ld(reinterpret_cast<const int4*>(v.Mt + static_cast<long long>(u) * v.ld + i0));
       p0 = a.x + b.x;
       p1 = p0 + a.y + b.y;
       p2 = p1 + a.z + b.z;
@@ -99,7 +123,10 @@ struct DenseOps {
   }
 };
 
+using DenseOps = DenseOpsT<LdNC>;
+
 struct SortedOps {
+  using Ld = LdNC;
   SortedView v;
   int B;
   __device__ __forceinline__ int get(int x, int y) const {
@@ -148,9 +175,10 @@ struct VertexInfo {
   int o0, dego, i0, degi;
 };
 
+template <class Ops>
 __device__ __forceinline__ VertexInfo vertex_info(const NodalArgs& a, int v) {
   VertexInfo vi;
-  vi.r = __ldg(a.part + v);
+  vi.r = Ops::Ld::ld(a.part + v);
   vi.kout = __ldg(a.kout + v);
   vi.kin = __ldg(a.kin + v);
   vi.o0 = __ldg(a.out_ptr + v);
@@ -160,15 +188,24 @@ __device__ __forceinline__ VertexInfo vertex_info(const NodalArgs& a, int v) {
   return vi;
 }
 
-// target block of the proposal for v (warp-collective: all 32 lanes)
+// target block once the chosen neighbour's block u is known
+// (warp-collective): with probability B / (d_u + B) a uniform block, else
+// a block drawn from row + column u of M
 template <class Ops>
-__device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops, int v,
+__device__ __forceinline__ int target_from(const NodalArgs& a, const Ops& ops, const Draws& x, int u,
+                                           int lane, int* scanned) {
+  const long long dau = static_cast<long long>(Ops::Ld::ld(a.dout + u)) + Ops::Ld::ld(a.din + u);
+  if (accept_uniform(x.x1, dau, a.B)) return static_cast<int>(draw_below(x.x2, a.B));
+  return ops.sym_sample(u, draw_below(x.x2, dau), lane, scanned);
+}
+
+// target block of the proposal for v (warp-collective), reading the
+// vertex's adjacency from memory; used for hubs
+template <class Ops>
+__device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops, const Draws& x,
                                               const VertexInfo& vi, int lane, int* scanned) {
-  const int B = a.B;
-  const Draws x = philox(static_cast<uint32_t>(v), static_cast<uint32_t>(a.ctl->itr), a.stage, kTagNodal,
-                         a.seed);
   const long long k = vi.kout + vi.kin;
-  if (k == 0) return static_cast<int>(draw_below(x.x2, B));
+  if (k == 0) return static_cast<int>(draw_below(x.x2, a.B));
   const long long t = draw_below(x.x0, k);
   const int deg = vi.dego + vi.degi;
   int j;
@@ -192,91 +229,120 @@ __device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops
     }
   }
   const int nbr = j < vi.dego ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
-  const int u = __ldg(a.part + nbr);
-  const long long dau = static_cast<long long>(__ldg(a.dout + u)) + __ldg(a.din + u);
-  if (accept_uniform(x.x1, dau, B)) return static_cast<int>(draw_below(x.x2, B));
-  return ops.sym_sample(u, draw_below(x.x2, dau), lane, scanned);
+  return target_from(a, ops, x, Ops::Ld::ld(a.part + nbr), lane, scanned);
 }
 
 struct TermSums {
   long long acc;
-  int sXR, sXS, sYR, sYS, nb;
+  int sXR, sXS, sYR, sYS;
 };
 
-// dS terms of one aggregated neighbour block b (b not in {r, s})
+// log of the degrees of r and s before and after the move
+struct DegLogs {
+  double r_out, s_out, r_out_n, s_out_n, r_in, s_in, r_in_n, s_in_n;
+};
+
+__device__ __forceinline__ DegLogs deg_logs(const double* __restrict__ L, long long dr_out, long long dr_in,
+                                            long long ds_out, long long ds_in, long long kout,
+                                            long long kin) {
+  return DegLogs{__ldg(L + dr_out), __ldg(L + ds_out), __ldg(L + dr_out - kout), __ldg(L + ds_out + kout),
+                 __ldg(L + dr_in),  __ldg(L + ds_in),  __ldg(L + dr_in - kin),   __ldg(L + ds_in + kin)};
+}
+
+// g(x, d1, d2) = x * ((L[x] - L[d1]) - L[d2]) from loaded log values,
+// rounded exactly as g_term rounds it
+__device__ __forceinline__ double g_val(long long x, double Lx, double L1, double L2) {
+  if (x == 0) return 0.0;
+  return __dmul_rn(static_cast<double>(x), __dsub_rn(__dsub_rn(Lx, L1), L2));
+}
+
+// dS terms of one aggregated neighbour block b (b not in {r, s}): v sends
+// wo to b and receives wi from b
 template <class Ops>
-__device__ __forceinline__ void slot_terms(const NodalArgs& a, const Ops& ops, int r, int s, int b,
-                                           int wo, int wi, long long dr_out, long long ds_out,
-                                           long long dr_in, long long ds_in, long long dr_out_n,
-                                           long long ds_out_n, long long dr_in_n, long long ds_in_n,
-                                           TermSums& ts) {
+__device__ __forceinline__ void slot_terms(const NodalArgs& a, const Ops& ops, int r, int s, int b, int wo,
+                                           int wi, const DegLogs& dl, TermSums& ts) {
+  const double* __restrict__ L = a.L;
   if (wo > 0) {
     const int R = ops.get(r, b), S = ops.get(s, b);
-    const long long dinb = __ldg(a.din + b);
-    ts.acc += q32(g_term(a.L, R, dinb, dr_out));
-    ts.acc += q32(g_term(a.L, S, dinb, ds_out));
-    ts.acc -= q32(g_term(a.L, R - wo, dinb, dr_out_n));
-    ts.acc -= q32(g_term(a.L, S + wo, dinb, ds_out_n));
+    const double LD = __ldg(L + Ops::Ld::ld(a.din + b));
+    ts.acc += q32(g_val(R, __ldg(L + R), LD, dl.r_out));
+    ts.acc += q32(g_val(S, __ldg(L + S), LD, dl.s_out));
+    ts.acc -= q32(g_val(R - wo, __ldg(L + R - wo), LD, dl.r_out_n));
+    ts.acc -= q32(g_val(S + wo, __ldg(L + S + wo), LD, dl.s_out_n));
     ts.sXR += R;
     ts.sXS += S;
   }
   if (wi > 0) {
-    const int Rc = ops.get(b, r), Sc = ops.get(b, s);
-    const long long doutb = __ldg(a.dout + b);
-    ts.acc += q32(g_term(a.L, Rc, dr_in, doutb));
-    ts.acc += q32(g_term(a.L, Sc, ds_in, doutb));
-    ts.acc -= q32(g_term(a.L, Rc - wi, dr_in_n, doutb));
-    ts.acc -= q32(g_term(a.L, Sc + wi, ds_in_n, doutb));
-    ts.sYR += Rc;
-    ts.sYS += Sc;
+    const int R = ops.get(b, r), S = ops.get(b, s);
+    const double LD = __ldg(L + Ops::Ld::ld(a.dout + b));
+    ts.acc += q32(g_val(R, __ldg(L + R), dl.r_in, LD));
+    ts.acc += q32(g_val(S, __ldg(L + S), dl.s_in, LD));
+    ts.acc -= q32(g_val(R - wi, __ldg(L + R - wi), dl.r_in_n, LD));
+    ts.acc -= q32(g_val(S + wi, __ldg(L + S + wi), dl.s_in_n, LD));
+    ts.sYR += R;
+    ts.sYS += S;
   }
 }
 
-// 2x2 and unchanged-entry terms, the accept rule (dS < 0, -inf included)
-// and the outputs; one thread
-template <class Ops>
-__device__ __forceinline__ void finalize(const NodalArgs& a, const Ops& ops, int v, int r, int s,
-                                         const VertexInfo& vi, TermSums ts, long long wor,
-                                         long long wos, long long Rr, long long Rs, long long Sr,
-                                         long long Ss, int scanned, unsigned long long* my_bytes) {
-  const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
-  const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
-  const long long dr_out_n = dr_out - vi.kout, ds_out_n = ds_out + vi.kout;
-  const long long dr_in_n = dr_in - vi.kin, ds_in_n = ds_in + vi.kin;
-  long long acc = ts.acc;
-  acc += q32(g_term(a.L, Rr, dr_in, dr_out));
-  acc += q32(g_term(a.L, Rs, ds_in, dr_out));
-  acc += q32(g_term(a.L, Sr, dr_in, ds_out));
-  acc += q32(g_term(a.L, Ss, ds_in, ds_out));
-  int ninf = 0;
-  const double nt[4] = {g_term(a.L, Rr - wor, dr_in_n, dr_out_n), g_term(a.L, Rs - wos, ds_in_n, dr_out_n),
-                        g_term(a.L, Sr + wor, dr_in_n, ds_out_n), g_term(a.L, Ss + wos, ds_in_n, ds_out_n)};
-#pragma unroll
-  for (int t = 0; t < 4; t++) {
-    if (isinf(nt[t])) ninf = 1;
-    else acc -= q32(nt[t]);
+// The 2x2 terms and the entries the move leaves unchanged, one term per
+// lane (lanes 0-11), added to the warp-summed neighbour terms `ts`.  The
+// four new 2x2 terms are subtracted; a -inf among them sets *ninf and is
+// left out of the sum (the reference's dS is then -inf).  Every lane
+// returns the same result.
+__device__ __forceinline__ long long finalize_warp(const double* __restrict__ L, int lane, const TermSums& ts,
+                                                   long long Rr, long long Rs, long long Sr, long long Ss,
+                                                   long long wor, long long wos, long long dr_out,
+                                                   long long dr_in, long long ds_out, long long ds_in,
+                                                   long long kout, long long kin, int* ninf) {
+  const long long dr_out_n = dr_out - kout, ds_out_n = ds_out + kout;
+  const long long dr_in_n = dr_in - kin, ds_in_n = ds_in + kin;
+  // g lanes: mult * ((L[i0] - L[i1]) - L[i2]); coefficient lanes: mult * (L[i0] - L[i1])
+  long long mult = 0, i0 = 0, i1 = 0, i2 = 0;
+  bool coef = false, neg = false;
+  switch (lane) {
+    case 0: mult = Rr; i0 = Rr; i1 = dr_in; i2 = dr_out; break;
+    case 1: mult = Rs; i0 = Rs; i1 = ds_in; i2 = dr_out; break;
+    case 2: mult = Sr; i0 = Sr; i1 = dr_in; i2 = ds_out; break;
+    case 3: mult = Ss; i0 = Ss; i1 = ds_in; i2 = ds_out; break;
+    case 4: mult = Rr - wor; i0 = mult; i1 = dr_in_n; i2 = dr_out_n; neg = true; break;
+    case 5: mult = Rs - wos; i0 = mult; i1 = ds_in_n; i2 = dr_out_n; neg = true; break;
+    case 6: mult = Sr + wor; i0 = mult; i1 = dr_in_n; i2 = ds_out_n; neg = true; break;
+    case 7: mult = Ss + wos; i0 = mult; i1 = ds_in_n; i2 = ds_out_n; neg = true; break;
+    case 8: mult = dr_out - Rr - Rs - ts.sXR; i0 = dr_out_n; i1 = dr_out; coef = true; break;
+    case 9: mult = ds_out - Sr - Ss - ts.sXS; i0 = ds_out_n; i1 = ds_out; coef = true; break;
+    case 10: mult = dr_in - Rr - Sr - ts.sYR; i0 = dr_in_n; i1 = dr_in; coef = true; break;
+    case 11: mult = ds_in - Rs - Ss - ts.sYS; i0 = ds_in_n; i1 = ds_in; coef = true; break;
+    default: break;
   }
-  acc += q32(coef_term(a.L, dr_out - Rr - Rs - ts.sXR, dr_out_n, dr_out));
-  acc += q32(coef_term(a.L, ds_out - Sr - Ss - ts.sXS, ds_out_n, ds_out));
-  acc += q32(coef_term(a.L, dr_in - Rr - Sr - ts.sYR, dr_in_n, dr_in));
-  acc += q32(coef_term(a.L, ds_in - Rs - Ss - ts.sYS, ds_in_n, ds_in));
+  const double La = __ldg(L + i0), Lb = __ldg(L + i1), Lc = __ldg(L + i2);
+  double t = 0.0;
+  if (mult != 0) {
+    const double d = __dsub_rn(La, Lb);
+    t = __dmul_rn(static_cast<double>(mult), coef ? d : __dsub_rn(d, Lc));
+  }
+  const bool inf = neg && isinf(t);
+  long long q = inf ? 0 : q32(t);
+  if (neg) q = -q;
+  *ninf = __any_sync(0xffffffffu, inf) ? 1 : 0;
+  return ts.acc + warp_sum_ll(q);
+}
+
+// per-vertex outputs of a decided proposal; returns whether it is accepted
+__device__ __forceinline__ bool emit(const NodalArgs& a, int v, int r, int s, long long acc, int ninf) {
   const bool accept = ninf || acc < 0;
+  a.move_to[v] = accept ? s : -1;
+  a.from[v] = r;
   if (a.prop_s) {
     a.prop_s[v - a.beg] = s;
     a.prop_q[v - a.beg] = acc;
     a.prop_ninf[v - a.beg] = ninf;
   }
-  if (accept) {
-    a.move_to[v] = s;
-    if (ninf) atomicOr(&a.ctl->cum_ninf, 1);
-    else atomicAdd(&a.ctl->cum_q, static_cast<unsigned long long>(acc));
-    atomicAdd(&a.ctl->moves, 1ull);
-  }
-  if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&a.ctl->near, 1ull);
-  if (a.stats) *my_bytes += 8 + 8ull * (vi.dego + vi.degi) + 48ull * ts.nb + 48 + 8ull * scanned;
+  return accept;
 }
 
-__device__ __forceinline__ void record_stay(const NodalArgs& a, int v) {
+__device__ __forceinline__ void record_stay(const NodalArgs& a, int v, int r) {
+  a.move_to[v] = -1;
+  a.from[v] = r;
   if (a.prop_s) {
     a.prop_s[v - a.beg] = -1;
     a.prop_q[v - a.beg] = 0;
@@ -284,203 +350,356 @@ __device__ __forceinline__ void record_stay(const NodalArgs& a, int v) {
   }
 }
 
-// one warp per vertex of degree <= kHubDegree; 5 CTAs per SM so that a
-// batch of the bench workload (N/10 = 5000 vertices) runs in one wave
+// accepted dS, moves and near-threshold proposals of one CTA, added to the
+// control block once at the end of the kernel
+struct CtaTally {
+  unsigned long long cum, moves, near;
+  int ninf;
+};
+
+__device__ __forceinline__ void tally(CtaTally* t, bool accept, long long acc, int ninf) {
+  if (accept) {
+    if (ninf) atomicOr(&t->ninf, 1);
+    else atomicAdd(&t->cum, static_cast<unsigned long long>(acc));
+    atomicAdd(&t->moves, 1ull);
+  }
+  if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&t->near, 1ull);
+}
+
+__device__ __forceinline__ void tally_flush(const CtaTally* t, NodalCtl* ctl) {
+  if (t->ninf) atomicOr(&ctl->cum_ninf, 1);
+  if (t->cum) atomicAdd(&ctl->cum_q, t->cum);
+  if (t->moves) atomicAdd(&ctl->moves, t->moves);
+  if (t->near) atomicAdd(&ctl->near, t->near);
+}
+
+// Proposal for one vertex of degree <= kHubDegree by one warp (all 32
+// lanes).  Each lane loads up to four neighbours at once (ids, then their
+// blocks) and keeps them in registers: the hash of neighbour blocks and the
+// target draw (whose chosen neighbour is among them) come from the same
+// loads.  key/two/twi: the warp's kHCap-slot table; list: kHubDegree ints.
+template <class Ops>
+__device__ __forceinline__ void warp_vertex(const NodalArgs& a, const Ops& ops, int v, uint32_t itr,
+                                            int* key, int* two, int* twi, int* list, CtaTally* tl,
+                                            int lane, unsigned long long* my_bytes) {
+  using LD = typename Ops::Ld;
+  const unsigned lanes_below = (1u << lane) - 1u;
+  const VertexInfo vi = vertex_info<Ops>(a, v);
+  const int deg = vi.dego + vi.degi;
+  if (deg > kHubDegree) return;   // proposed by a whole CTA
+  const int r = vi.r;
+  const Draws x = philox(static_cast<uint32_t>(v), itr, a.stage, kTagNodal, a.seed);
+  const long long dr_out = LD::ld(a.dout + r), dr_in = LD::ld(a.din + r);
+  int lg = 5;
+  while ((1 << lg) < 2 * deg) lg++;
+  const int cap = 1 << lg;   // <= kHCap since deg <= kHubDegree
+  for (int i = lane; i < cap; i += 32) {
+    key[i] = -1;
+    two[i] = 0;
+    twi[i] = 0;
+  }
+  __syncwarp();
+  int nb[4], wv[4], pb[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int j = lane + 32 * k;
+    nb[k] = 0;
+    wv[k] = 0;
+    if (j < deg) {
+      const bool is_out = j < vi.dego;
+      nb[k] = is_out ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
+      wv[k] = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; k++) pb[k] = lane + 32 * k < deg ? LD::ld(a.part + nb[k]) : 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int j = lane + 32 * k;
+    if (j < deg) table_insert(key, two, twi, cap, lg, pb[k], wv[k], j < vi.dego);
+  }
+  // the target: neighbour position j by weight, its block from registers
+  int scanned = 0;
+  int s;
+  const long long ktot = vi.kout + vi.kin;
+  if (ktot == 0) {
+    s = static_cast<int>(draw_below(x.x2, a.B));
+  } else {
+    const long long t = draw_below(x.x0, ktot);
+    int j;
+    if (a.unit) {
+      j = static_cast<int>(t);
+    } else {
+      long long run = 0;
+      j = deg - 1;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        if (32 * k >= deg) break;
+        const long long ww = lane + 32 * k < deg ? wv[k] : 0;
+        const long long incl = warp_incl_scan_ll(ww, lane);
+        const long long total = __shfl_sync(0xffffffffu, incl, 31);
+        if (run + total > t) {
+          const unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
+          j = 32 * k + __ffs(m) - 1;
+          break;
+        }
+        run += total;
+      }
+    }
+    const int kq = j >> 5;
+    const int pj = kq == 0 ? pb[0] : kq == 1 ? pb[1] : kq == 2 ? pb[2] : pb[3];
+    s = target_from(a, ops, x, __shfl_sync(0xffffffffu, pj, j & 31), lane, &scanned);
+  }
+  __syncwarp();
+  if (s == r) {
+    if (lane == 0) {
+      record_stay(a, v, r);
+      if (a.stats) *my_bytes += 8 + 8ull * deg + 8ull * scanned;
+    }
+    __syncwarp();
+    return;
+  }
+  const long long ds_out = LD::ld(a.dout + s), ds_in = LD::ld(a.din + s);
+  int e4 = 0;
+  if (lane < 4) e4 = ops.get(lane < 2 ? r : s, (lane & 1) ? s : r);
+  const DegLogs dl = deg_logs(a.L, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
+  // compact the occupied slots so that each lane takes about one block
+  int nlist = 0, noccupied = 0;
+  for (int base = 0; base < cap; base += 32) {
+    const int i = base + lane;
+    const int b = i < cap ? key[i] : -1;
+    const unsigned occ = __ballot_sync(0xffffffffu, b >= 0);
+    const bool use = b >= 0 && b != r && b != s;
+    const unsigned mu = __ballot_sync(0xffffffffu, use);
+    if (use) list[nlist + __popc(mu & lanes_below)] = i;
+    nlist += __popc(mu);
+    noccupied += __popc(occ);
+  }
+  __syncwarp();
+  TermSums ts{0, 0, 0, 0, 0};
+  for (int t = lane; t < nlist; t += 32) {
+    const int i = list[t];
+    slot_terms(a, ops, r, s, key[i], two[i], twi[i], dl, ts);
+  }
+  ts.acc = warp_sum_ll(ts.acc);
+  ts.sXR = warp_sum_i(ts.sXR);
+  ts.sXS = warp_sum_i(ts.sXS);
+  ts.sYR = warp_sum_i(ts.sYR);
+  ts.sYS = warp_sum_i(ts.sYS);
+  const long long Rr = __shfl_sync(0xffffffffu, e4, 0), Rs = __shfl_sync(0xffffffffu, e4, 1);
+  const long long Sr = __shfl_sync(0xffffffffu, e4, 2), Ss = __shfl_sync(0xffffffffu, e4, 3);
+  const long long wor = table_lookup_wo(key, two, cap, lg, r);
+  const long long wos = table_lookup_wo(key, two, cap, lg, s);
+  int ninf;
+  const long long acc = finalize_warp(a.L, lane, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
+                                      vi.kout, vi.kin, &ninf);
+  if (lane == 0) {
+    tally(tl, emit(a, v, r, s, acc, ninf), acc, ninf);
+    if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * noccupied + 48 + 8ull * scanned;
+  }
+  __syncwarp();
+}
+
+// One warp per vertex of degree <= kHubDegree; 5 CTAs per SM so that a
+// batch of the bench workload (N/10 = 5000 vertices) runs in one wave.
 template <class Ops>
 __global__ void __launch_bounds__(kThreads, 5) k_nodal_propose(NodalArgs a, Ops ops) {
   __shared__ int s_key[kWarps][kHCap];
   __shared__ int s_wo[kWarps][kHCap];
   __shared__ int s_wi[kWarps][kHCap];
   __shared__ int s_list[kWarps][kHubDegree];   // occupied slots other than r, s
-  if (*reinterpret_cast<volatile int*>(&a.ctl->done)) return;
+  __shared__ CtaTally s_tally;
+  if (a.ctl->done) return;   // written by earlier launches only
+  const uint32_t itr = static_cast<uint32_t>(a.ctl->itr);
+  if (threadIdx.x == 0) s_tally = CtaTally{0, 0, 0, 0};
+  __syncthreads();
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const unsigned lanes_below = (1u << lane) - 1u;
   const int nwarps = gridDim.x * kWarps;
   unsigned long long my_bytes = 0;
-  for (int v = a.beg + blockIdx.x * kWarps + wib; v < a.end; v += nwarps) {
-    const VertexInfo vi = vertex_info(a, v);
-    const int deg = vi.dego + vi.degi;
-    if (deg > kHubDegree) continue;   // handled by k_nodal_propose_hub
-    const int r = vi.r;
-    // aggregate the neighbour blocks first: these loads do not depend on
-    // the target and overlap the sampling chain below
-    int lg = 5;
-    while ((1 << lg) < 2 * deg) lg++;
-    const int cap = 1 << lg;   // <= kHCap since deg <= kHubDegree
-    int* key = s_key[wib];
-    int* two = s_wo[wib];
-    int* twi = s_wi[wib];
-    for (int i = lane; i < cap; i += 32) {
-      key[i] = -1;
-      two[i] = 0;
-      twi[i] = 0;
-    }
-    __syncwarp();
-    for (int j = lane; j < deg; j += 32) {
-      const bool is_out = j < vi.dego;
-      const int nb = is_out ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
-      const int ww = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
-      table_insert(key, two, twi, cap, lg, __ldg(a.part + nb), ww, is_out);
-    }
+  for (int v = a.beg + blockIdx.x * kWarps + wib; v < a.end; v += nwarps)
+    warp_vertex(a, ops, v, itr, s_key[wib], s_wo[wib], s_wi[wib], s_list[wib], &s_tally, lane, &my_bytes);
+  __syncthreads();
+  if (threadIdx.x == 0) tally_flush(&s_tally, a.ctl);
+  if (a.stats && lane == 0 && my_bytes) atomicAdd(&a.ctl->bytes, my_bytes);
+}
+
+template <int NW>
+struct HubShared {
+  long long acc[NW];
+  int sum[5][NW];
+  int target, scanned;
+};
+
+// Proposal for one vertex of degree > kHubDegree by a whole CTA of NT
+// threads.  The last warp draws the target while the others fill the hash
+// of neighbour blocks (at most min(deg, B) entries: in `stab`, a shared
+// region of `scap` slots per array, or beyond that in the vertex's global
+// region); each thread loads four neighbours at once, and up to four
+// occupied slots at once for the terms.
+template <class Ops, int NT>
+__device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, int v, uint32_t itr, int* stab,
+                                           int scap, HubShared<NT / 32>* sh, unsigned long long* my_bytes) {
+  using LD = typename Ops::Ld;
+  constexpr int NW = NT / 32;
+  constexpr int kIns = NT - 32;   // threads that fill the table
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const VertexInfo vi = vertex_info<Ops>(a, v);
+  const int deg = vi.dego + vi.degi;
+  const int r = vi.r;
+  const int distinct_max = deg < a.B ? deg : a.B;
+  int lg = 5;
+  while ((1 << lg) < 2 * distinct_max) lg++;
+  const int cap = 1 << lg;
+  int *key, *two, *twi;
+  if (cap <= scap) {
+    key = stab;
+    two = stab + scap;
+    twi = stab + 2 * scap;
+  } else {
+    const long long off = __ldg(a.hi_off + v);
+    key = a.hkey + off;
+    two = a.hwo + off;
+    twi = a.hwi + off;
+  }
+  for (int i = threadIdx.x; i < cap; i += NT) {
+    key[i] = -1;
+    two[i] = 0;
+    twi[i] = 0;
+  }
+  __syncthreads();
+  if (wib == NW - 1) {
+    const Draws x = philox(static_cast<uint32_t>(v), itr, a.stage, kTagNodal, a.seed);
     int scanned = 0;
-    const int s = propose_target(a, ops, v, vi, lane, &scanned);
-    __syncwarp();
-    if (s == r) {
-      if (lane == 0) {
-        record_stay(a, v);
-        if (a.stats) my_bytes += 8 + 8ull * deg + 8ull * scanned;
+    const int st = propose_target(a, ops, x, vi, lane, &scanned);
+    if (lane == 0) {
+      sh->target = st;
+      sh->scanned = scanned;
+    }
+  } else {
+    for (int j0 = threadIdx.x; j0 < deg; j0 += 4 * kIns) {
+      int nb[4], wv[4], pb[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int j = j0 + k * kIns;
+        nb[k] = 0;
+        wv[k] = 0;
+        if (j < deg) {
+          const bool is_out = j < vi.dego;
+          nb[k] = is_out ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
+          wv[k] = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
+        }
       }
-      __syncwarp();
-      continue;
+#pragma unroll
+      for (int k = 0; k < 4; k++) pb[k] = j0 + k * kIns < deg ? LD::ld(a.part + nb[k]) : 0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int j = j0 + k * kIns;
+        if (j < deg) table_insert(key, two, twi, cap, lg, pb[k], wv[k], j < vi.dego);
+      }
     }
-    const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
-    const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
-    // compact the occupied slots so that each lane takes about one block
-    int nlist = 0, noccupied = 0;
-    for (int base = 0; base < cap; base += 32) {
-      const int i = base + lane;
-      const int b = i < cap ? key[i] : -1;
-      const unsigned occ = __ballot_sync(0xffffffffu, b >= 0);
-      const bool use = b >= 0 && b != r && b != s;
-      const unsigned mu = __ballot_sync(0xffffffffu, use);
-      if (use) s_list[wib][nlist + __popc(mu & lanes_below)] = i;
-      nlist += __popc(mu);
-      noccupied += __popc(occ);
+  }
+  __syncthreads();
+  const int s = sh->target;
+  if (s == r) {
+    if (threadIdx.x == 0) {
+      record_stay(a, v, r);
+      if (a.stats) *my_bytes += 8 + 8ull * deg + 8ull * sh->scanned;
     }
-    __syncwarp();
-    TermSums ts{0, 0, 0, 0, 0, 0};
-    for (int t = lane; t < nlist; t += 32) {
-      const int i = s_list[wib][t];
-      slot_terms(a, ops, r, s, key[i], two[i], twi[i], dr_out, ds_out, dr_in, ds_in, dr_out - vi.kout,
-                 ds_out + vi.kout, dr_in - vi.kin, ds_in + vi.kin, ts);
+    __syncthreads();
+    return;
+  }
+  const long long dr_out = LD::ld(a.dout + r), dr_in = LD::ld(a.din + r);
+  const long long ds_out = LD::ld(a.dout + s), ds_in = LD::ld(a.din + s);
+  const DegLogs dl = deg_logs(a.L, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
+  TermSums ts{0, 0, 0, 0, 0};
+  int nocc = 0;
+  for (int i = threadIdx.x; i < cap;) {
+    int sl[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      sl[k] = -1;
+      while (i < cap) {
+        const int b = key[i];
+        i += NT;
+        if (b < 0) continue;
+        nocc++;
+        if (b != r && b != s) {
+          sl[k] = i - NT;
+          break;
+        }
+      }
     }
-    ts.acc = warp_sum_ll(ts.acc);
-    ts.sXR = warp_sum_i(ts.sXR);
-    ts.sXS = warp_sum_i(ts.sXS);
-    ts.sYR = warp_sum_i(ts.sYR);
-    ts.sYS = warp_sum_i(ts.sYS);
-    ts.nb = noccupied;
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (sl[k] >= 0) slot_terms(a, ops, r, s, key[sl[k]], two[sl[k]], twi[sl[k]], dl, ts);
+  }
+  ts.acc = warp_sum_ll(ts.acc);
+  ts.sXR = warp_sum_i(ts.sXR);
+  ts.sXS = warp_sum_i(ts.sXS);
+  ts.sYR = warp_sum_i(ts.sYR);
+  ts.sYS = warp_sum_i(ts.sYS);
+  nocc = warp_sum_i(nocc);
+  if (lane == 0) {
+    sh->acc[wib] = ts.acc;
+    sh->sum[0][wib] = ts.sXR;
+    sh->sum[1][wib] = ts.sXS;
+    sh->sum[2][wib] = ts.sYR;
+    sh->sum[3][wib] = ts.sYS;
+    sh->sum[4][wib] = nocc;
+  }
+  __syncthreads();
+  if (wib == 0) {
+    TermSums tot{0, 0, 0, 0, 0};
+    int occ = 0;
+    if (lane < NW) {
+      tot.acc = sh->acc[lane];
+      tot.sXR = sh->sum[0][lane];
+      tot.sXS = sh->sum[1][lane];
+      tot.sYR = sh->sum[2][lane];
+      tot.sYS = sh->sum[3][lane];
+      occ = sh->sum[4][lane];
+    }
+    tot.acc = warp_sum_ll(tot.acc);
+    tot.sXR = warp_sum_i(tot.sXR);
+    tot.sXS = warp_sum_i(tot.sXS);
+    tot.sYR = warp_sum_i(tot.sYR);
+    tot.sYS = warp_sum_i(tot.sYS);
+    occ = warp_sum_i(occ);
     int e4 = 0;
     if (lane < 4) e4 = ops.get(lane < 2 ? r : s, (lane & 1) ? s : r);
     const long long Rr = __shfl_sync(0xffffffffu, e4, 0), Rs = __shfl_sync(0xffffffffu, e4, 1);
     const long long Sr = __shfl_sync(0xffffffffu, e4, 2), Ss = __shfl_sync(0xffffffffu, e4, 3);
+    const long long wor = table_lookup_wo(key, two, cap, lg, r);
+    const long long wos = table_lookup_wo(key, two, cap, lg, s);
+    int ninf;
+    const long long acc = finalize_warp(a.L, lane, tot, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
+                                        vi.kout, vi.kin, &ninf);
     if (lane == 0) {
-      const long long wor = table_lookup_wo(key, two, cap, lg, r);
-      const long long wos = table_lookup_wo(key, two, cap, lg, s);
-      finalize(a, ops, v, r, s, vi, ts, wor, wos, Rr, Rs, Sr, Ss, scanned, &my_bytes);
+      const bool accept = emit(a, v, r, s, acc, ninf);
+      if (accept) {
+        if (ninf) atomicOr(&a.ctl->cum_ninf, 1);
+        else atomicAdd(&a.ctl->cum_q, static_cast<unsigned long long>(acc));
+        atomicAdd(&a.ctl->moves, 1ull);
+      }
+      if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&a.ctl->near, 1ull);
+      if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * occ + 48 + 8ull * sh->scanned;
     }
-    __syncwarp();
   }
-  if (a.stats && lane == 0 && my_bytes) atomicAdd(&a.ctl->bytes, my_bytes);
+  __syncthreads();
 }
 
-// one CTA per vertex of degree > kHubDegree; the hash holds at most
-// min(deg, B) distinct blocks and lives in dynamic shared memory
-// (`smem_cap` slots) or, beyond that, in the vertex's global region
+// one CTA per vertex of degree > kHubDegree, hash in dynamic shared memory
+// (`smem_cap` slots per array) or the vertex's global region
 template <class Ops>
 __global__ void __launch_bounds__(kHubThreads) k_nodal_propose_hub(NodalArgs a, Ops ops, const int32_t* hubs,
                                                                   int hub_lo, int hub_hi, int smem_cap) {
   extern __shared__ int dyn[];
-  __shared__ long long s_acc[kHubWarps];
-  __shared__ int s_sum[5][kHubWarps];
-  __shared__ int s_target, s_scanned;
-  if (*reinterpret_cast<volatile int*>(&a.ctl->done)) return;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  __shared__ HubShared<kHubWarps> sh;
+  if (a.ctl->done) return;
+  const uint32_t itr = static_cast<uint32_t>(a.ctl->itr);
   unsigned long long my_bytes = 0;
-  for (int h = hub_lo + blockIdx.x; h < hub_hi; h += gridDim.x) {
-    const int v = __ldg(hubs + h);
-    const VertexInfo vi = vertex_info(a, v);
-    const int deg = vi.dego + vi.degi;
-    const int r = vi.r;
-    if (wib == 0) {
-      int scanned = 0;
-      const int s = propose_target(a, ops, v, vi, lane, &scanned);
-      if (lane == 0) {
-        s_target = s;
-        s_scanned = scanned;
-      }
-    }
-    __syncthreads();
-    const int s = s_target;
-    if (s == r) {
-      if (threadIdx.x == 0) {
-        record_stay(a, v);
-        if (a.stats) my_bytes += 8 + 8ull * deg + 8ull * s_scanned;
-      }
-      __syncthreads();
-      continue;
-    }
-    const int distinct_max = deg < a.B ? deg : a.B;
-    int lg = 5;
-    while ((1 << lg) < 2 * distinct_max) lg++;
-    const int cap = 1 << lg;
-    int *key, *two, *twi;
-    if (cap <= smem_cap) {
-      key = dyn;
-      two = dyn + smem_cap;
-      twi = dyn + 2 * smem_cap;
-    } else {
-      const long long off = __ldg(a.hi_off + v);
-      key = a.hkey + off;
-      two = a.hwo + off;
-      twi = a.hwi + off;
-    }
-    for (int i = threadIdx.x; i < cap; i += kHubThreads) {
-      key[i] = -1;
-      two[i] = 0;
-      twi[i] = 0;
-    }
-    __syncthreads();
-    for (int j = threadIdx.x; j < deg; j += kHubThreads) {
-      const bool is_out = j < vi.dego;
-      const int nb = is_out ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
-      const int ww = a.unit ? 1 : (is_out ? __ldg(a.out_w + vi.o0 + j) : __ldg(a.in_w + vi.i0 + j - vi.dego));
-      table_insert(key, two, twi, cap, lg, __ldg(a.part + nb), ww, is_out);
-    }
-    __syncthreads();
-    const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
-    const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
-    TermSums ts{0, 0, 0, 0, 0, 0};
-    for (int i = threadIdx.x; i < cap; i += kHubThreads) {
-      const int b = key[i];
-      if (b < 0) continue;
-      ts.nb++;
-      if (b == r || b == s) continue;
-      slot_terms(a, ops, r, s, b, two[i], twi[i], dr_out, ds_out, dr_in, ds_in, dr_out - vi.kout,
-                 ds_out + vi.kout, dr_in - vi.kin, ds_in + vi.kin, ts);
-    }
-    ts.acc = warp_sum_ll(ts.acc);
-    ts.sXR = warp_sum_i(ts.sXR);
-    ts.sXS = warp_sum_i(ts.sXS);
-    ts.sYR = warp_sum_i(ts.sYR);
-    ts.sYS = warp_sum_i(ts.sYS);
-    ts.nb = warp_sum_i(ts.nb);
-    if (lane == 0) {
-      s_acc[wib] = ts.acc;
-      s_sum[0][wib] = ts.sXR;
-      s_sum[1][wib] = ts.sXS;
-      s_sum[2][wib] = ts.sYR;
-      s_sum[3][wib] = ts.sYS;
-      s_sum[4][wib] = ts.nb;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      TermSums tot{0, 0, 0, 0, 0, 0};
-      for (int w = 0; w < kHubWarps; w++) {
-        tot.acc += s_acc[w];
-        tot.sXR += s_sum[0][w];
-        tot.sXS += s_sum[1][w];
-        tot.sYR += s_sum[2][w];
-        tot.sYS += s_sum[3][w];
-        tot.nb += s_sum[4][w];
-      }
-      const long long Rr = ops.get(r, r), Rs = ops.get(r, s), Sr = ops.get(s, r), Ss = ops.get(s, s);
-      const long long wor = table_lookup_wo(key, two, cap, lg, r);
-      const long long wos = table_lookup_wo(key, two, cap, lg, s);
-      finalize(a, ops, v, r, s, vi, tot, wor, wos, Rr, Rs, Sr, Ss, s_scanned, &my_bytes);
-    }
-    __syncthreads();
-  }
+  for (int h = hub_lo + blockIdx.x; h < hub_hi; h += gridDim.x)
+    hub_vertex<Ops, kHubThreads>(a, ops, __ldg(hubs + h), itr, dyn, smem_cap, &sh, &my_bytes);
   if (a.stats && threadIdx.x == 0 && my_bytes) atomicAdd(&a.ctl->bytes, my_bytes);
 }
 
@@ -507,105 +726,238 @@ __global__ void __launch_bounds__(kThreads) k_chunk_sums(int B, int ld, const in
   }
 }
 
-// Sum of `val` over the lanes of `active` that hold the same key; *lead is
-// set on one lane per key.
-__device__ __forceinline__ int group_sum(unsigned active, long long key, int val, int lane, bool* lead) {
-  const unsigned peers = __match_any_sync(active, key);
-  *lead = (__ffs(peers) - 1) == lane;
-  return __reduce_add_sync(peers, val);
-}
-
-// M[x,y] += w, keeping Mt and the chunk sums of rows x and y in step.
-// Lanes that update the same cell (or the same chunk sum) are summed first,
-// so a moved vertex with many edges into one block issues one atomic per
-// distinct target per warp.
-__device__ __forceinline__ void dense_add(unsigned active, int lane, int* M, int* Mt, int* CS, int ld,
-                                          int cld, int x, int y, int w) {
-  bool lead;
-  int sum = group_sum(active, static_cast<long long>(x) * ld + y, w, lane, &lead);
-  if (lead) {
-    atomicAdd(M + static_cast<long long>(x) * ld + y, sum);
-    atomicAdd(Mt + static_cast<long long>(y) * ld + x, sum);
-  }
-  sum = group_sum(active, static_cast<long long>(x) * cld + y / kChunk, w, lane, &lead);
-  if (lead) atomicAdd(CS + static_cast<long long>(x) * cld + y / kChunk, sum);
-  sum = group_sum(active, static_cast<long long>(y) * cld + x / kChunk, w, lane, &lead);
-  if (lead) atomicAdd(CS + static_cast<long long>(y) * cld + x / kChunk, sum);
-}
-
-// Apply the accepted moves of a batch to the dense tile by deltas, one
-// thread per edge of the batch: positions [0, n_out) walk the batch's
-// out-edges (CSR positions o0 + i, owner out_src), [n_out, n_out + n_in)
-// its in-edges (positions i0 + i, owner in_dst).  An edge between two moved
-// vertices is applied once, from its source's out-list.
-__global__ void __launch_bounds__(kThreads) k_nodal_apply_dense(
-    const int32_t* __restrict__ out_src, const int32_t* __restrict__ out_idx,
-    const int32_t* __restrict__ out_w, const int32_t* __restrict__ in_dst,
-    const int32_t* __restrict__ in_idx, const int32_t* __restrict__ in_w,
-    const int32_t* __restrict__ part, const int32_t* __restrict__ move_to, int o0, int n_out, int i0,
-    int n_in, int ld, int* __restrict__ M, int* __restrict__ Mt, int cld, int* __restrict__ CS) {
-  const int lane = threadIdx.x & 31;
-  const long long total = static_cast<long long>(n_out) + n_in;
-  const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
-  for (long long base = static_cast<long long>(blockIdx.x) * blockDim.x + (threadIdx.x & ~31);
-       base < total; base += stride) {
-    const long long t = base + lane;
-    const bool is_out = t < n_out;
-    bool valid = t < total;
-    int v = 0, y = 0, w = 1, s = -1;
-    if (valid) {
-      const int pos = is_out ? o0 + static_cast<int>(t) : i0 + static_cast<int>(t - n_out);
-      v = is_out ? __ldg(out_src + pos) : __ldg(in_dst + pos);
-      s = move_to[v];
-      y = is_out ? __ldg(out_idx + pos) : __ldg(in_idx + pos);
-      if (is_out ? out_w != nullptr : in_w != nullptr) w = is_out ? __ldg(out_w + pos) : __ldg(in_w + pos);
+// update (:433-458), second half: the sweep's cumulative dS is recorded for
+// this sweep and added to S after every batch (as the reference does), then
+// the convergence test -mean < thr * S ends the nodal phase.  One thread.
+// The control block is read at once through L2 (ld.cg: the persistent
+// kernel calls this after other CTAs wrote it), then written back.
+__device__ __forceinline__ bool ctl_batch_end(NodalCtl* ctl, const CtlArgs& c) {
+  const int done = __ldcg(&ctl->done);
+  const long long cum = static_cast<long long>(__ldcg(&ctl->cum_q));
+  const int itr = __ldcg(&ctl->itr);
+  const int cum_ninf = __ldcg(&ctl->cum_ninf);
+  const long long S_q = __ldcg(&ctl->S_q) + cum;
+  const int S_ninf = __ldcg(&ctl->S_ninf) | cum_ninf;
+  const unsigned long long batches = __ldcg(&ctl->batches);
+  const unsigned long long proposals = __ldcg(&ctl->proposals);
+  const unsigned long long edge_visits = __ldcg(&ctl->edge_visits);
+  const double mean = __ldcg(&ctl->mean);
+  if (done) return true;
+  c.ide_q[itr] = cum;
+  c.ide_n[itr] = cum_ninf;
+  ctl->S_q = S_q;
+  ctl->S_ninf = S_ninf;
+  ctl->batches = batches + 1;
+  ctl->proposals = proposals + static_cast<unsigned long long>(c.batch_vertices);
+  ctl->edge_visits = edge_visits + static_cast<unsigned long long>(c.batch_edges);
+  if (itr >= c.W - 1) {
+    const double S_d = S_ninf ? -INFINITY : static_cast<double>(S_q) / kQ32;
+    if (-mean < c.thr * S_d) {
+      ctl->done = 1;
+      return true;
     }
-    const int my = valid ? move_to[y] : -1;
-    valid = valid && s >= 0 && (is_out || my < 0);
-    const unsigned act_out = __ballot_sync(0xffffffffu, valid && is_out);
-    const unsigned act_in = __ballot_sync(0xffffffffu, valid && !is_out);
-    if (valid) {
-      const int r = part[v];
-      const int oy = part[y];
-      if (is_out) {
-        const int ny = my >= 0 ? my : oy;
-        dense_add(act_out, lane, M, Mt, CS, ld, cld, r, oy, -w);
-        dense_add(act_out, lane, M, Mt, CS, ld, cld, s, ny, w);
-      } else {
-        dense_add(act_in, lane, M, Mt, CS, ld, cld, oy, r, -w);
-        dense_add(act_in, lane, M, Mt, CS, ld, cld, oy, s, w);
+  }
+  return false;
+}
+
+// prepare_batch (:381-395): S from the entropy accumulator, the moving
+// average of the previous sweeps' dS, and a fresh cumulative sum for this
+// sweep.  One thread; reads as in ctl_batch_end.
+__device__ __forceinline__ void ctl_sweep_start(NodalCtl* ctl, long long model_q, int W,
+                                                const long long* ide_q, const int* ide_n) {
+  const int done = __ldcg(&ctl->done);
+  const unsigned long long sweeps = __ldcg(&ctl->sweeps);
+  const unsigned long long eacc = __ldcg(&ctl->entropy_acc);
+  if (done) return;
+  const int itr = static_cast<int>(sweeps);
+  double mean = 0.0;
+  if (itr >= W - 1) {
+    long long sum = 0;
+    int ninf = 0;
+    for (int i = itr - W + 1; i < itr; i++) {
+      sum += __ldcg(ide_q + i);
+      ninf |= __ldcg(ide_n + i);
+    }
+    mean = ninf ? -INFINITY : (static_cast<double>(sum) / kQ32) / static_cast<double>(W - 1);
+  }
+  ctl->itr = itr;
+  ctl->S_q = model_q - static_cast<long long>(eacc);
+  ctl->S_ninf = 0;
+  ctl->mean = mean;
+  ctl->cum_q = 0;
+  ctl->cum_ninf = 0;
+  ctl->sweeps = sweeps + 1;
+}
+
+struct LdPlain {
+  template <class T>
+  __device__ __forceinline__ static T ld(const T* p) { return *p; }
+};
+
+// Shared-memory accumulation of one CTA's tile deltas during an apply pass.
+// `mkey/mval` hold M[a][b] += d under the key a * ld + b; at the flush each
+// entry updates M and Mt and feeds the chunk sums of rows a and b, which are
+// accumulated in `ckey/cval` (key row * cld + chunk) and flushed last.  All
+// sums are exact integers, so the order of the updates does not matter.  A
+// table that is full passes the update straight to global memory.
+struct DeltaTables {
+  int *mkey, *mval, *ckey, *cval;
+  int mlg, clg;   // capacities 1 << mlg, 1 << clg
+};
+
+__device__ __forceinline__ bool table_add(int* key, int* val, int lg, int k, int d) {
+  const int cap = 1 << lg;
+  unsigned h = hash_slot(k, lg);
+  for (int probe = 0; probe < cap; probe++) {
+    const int prev = atomicCAS(key + h, -1, k);
+    if (prev == -1 || prev == k) {
+      atomicAdd(val + h, d);
+      return true;
+    }
+    h = (h + 1) & (cap - 1);
+  }
+  return false;
+}
+
+__device__ __forceinline__ void cs_add(const DeltaTables& t, int* CS, int key, int d) {
+  if (!table_add(t.ckey, t.cval, t.clg, key, d)) atomicAdd(CS + key, d);
+}
+
+__device__ __forceinline__ void tile_add(const DeltaTables& t, int* M, int* Mt, int* CS, int ld, int cld, int x,
+                                         int y, int d) {
+  if (table_add(t.mkey, t.mval, t.mlg, x * ld + y, d)) return;
+  atomicAdd(M + static_cast<long long>(x) * ld + y, d);
+  atomicAdd(Mt + static_cast<long long>(y) * ld + x, d);
+  cs_add(t, CS, x * cld + y / kChunk, d);
+  cs_add(t, CS, y * cld + x / kChunk, d);
+}
+
+__device__ __forceinline__ void tables_clear(const DeltaTables& t) {
+  for (int i = threadIdx.x; i < (1 << t.mlg); i += blockDim.x) {
+    t.mkey[i] = -1;
+    t.mval[i] = 0;
+  }
+  for (int i = threadIdx.x; i < (1 << t.clg); i += blockDim.x) {
+    t.ckey[i] = -1;
+    t.cval[i] = 0;
+  }
+}
+
+// writes the CTA's accumulated deltas to the tile (CTA-collective; the
+// tables are cleared again on the way)
+__device__ __forceinline__ void tables_flush(const DeltaTables& t, int* M, int* Mt, int* CS, int ld, int cld) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < (1 << t.mlg); i += blockDim.x) {
+    const int k = t.mkey[i];
+    if (k < 0) continue;
+    const int d = t.mval[i];
+    t.mkey[i] = -1;
+    t.mval[i] = 0;
+    if (d == 0) continue;
+    const int x = k / ld, y = k - x * ld;
+    atomicAdd(M + static_cast<long long>(x) * ld + y, d);
+    atomicAdd(Mt + static_cast<long long>(y) * ld + x, d);
+    cs_add(t, CS, x * cld + y / kChunk, d);
+    cs_add(t, CS, y * cld + x / kChunk, d);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < (1 << t.clg); i += blockDim.x) {
+    const int k = t.ckey[i];
+    if (k < 0) continue;
+    const int d = t.cval[i];
+    t.ckey[i] = -1;
+    t.cval[i] = 0;
+    if (d) atomicAdd(CS + k, d);
+  }
+  __syncthreads();
+}
+
+// Applies and commits the moves of one 32-edge chunk of a batch vertex
+// (warp-collective).  A chunk whose vertex did not move returns at once.
+// Old blocks of batch vertices come from `from`, so part[] is committed in
+// the same pass: part is read only for vertices outside [beg, end).  An
+// edge between two moved vertices is applied once, from its source's
+// out-list.  LDM loads move_to/from, LDP the partition.  Tile deltas go to
+// the CTA's tables.
+template <class LDM, class LDP>
+__device__ __forceinline__ void apply_chunk(int2 ch, const GraphDev& g, int32_t* part, const int32_t* move_to,
+                                            const int32_t* from, int beg, int end, const DeltaTables& t, int ld,
+                                            int* M, int* Mt, int cld, int* CS, int32_t* dout, int32_t* din,
+                                            int lane) {
+  const int v = ch.x;
+  const int s = LDM::ld(move_to + v);
+  if (s < 0) return;   // warp-uniform
+  const int r = LDM::ld(from + v);
+  const int o0 = __ldg(g.out_ptr + v), dego = __ldg(g.out_ptr + v + 1) - o0;
+  const int i0 = __ldg(g.in_ptr + v), degi = __ldg(g.in_ptr + v + 1) - i0;
+  if (ch.y == 0 && lane == 0) {
+    part[v] = s;
+    const int ko = __ldg(g.kout + v), ki = __ldg(g.kin + v);
+    atomicSub(dout + r, ko);
+    atomicAdd(dout + s, ko);
+    atomicSub(din + r, ki);
+    atomicAdd(din + s, ki);
+  }
+  const unsigned span = static_cast<unsigned>(end - beg);
+  const int j = ch.y * 32 + lane;
+  if (j >= dego + degi) return;
+  const bool is_out = j < dego;
+  const int y = is_out ? __ldg(g.out_idx + o0 + j) : __ldg(g.in_idx + i0 + j - dego);
+  int w = 1;
+  if (is_out ? g.out_w != nullptr : g.in_w != nullptr)
+    w = is_out ? __ldg(g.out_w + o0 + j) : __ldg(g.in_w + i0 + j - dego);
+  const bool inb = static_cast<unsigned>(y - beg) < span;
+  const int my = inb ? LDM::ld(move_to + y) : -1;
+  const int oy = inb ? LDM::ld(from + y) : LDP::ld(part + y);
+  if (is_out) {
+    tile_add(t, M, Mt, CS, ld, cld, r, oy, -w);
+    tile_add(t, M, Mt, CS, ld, cld, s, my >= 0 ? my : oy, w);
+  } else if (my < 0) {
+    tile_add(t, M, Mt, CS, ld, cld, oy, r, -w);
+    tile_add(t, M, Mt, CS, ld, cld, oy, s, w);
+  }
+}
+
+constexpr int kApplyMLg = 11;   // per-CTA delta tables of the apply kernel
+constexpr int kApplyCLg = 10;
+
+// apply + commit of one batch on the dense tile, one warp per chunk
+// ([c0, c1) of g.chunks); the last CTA to finish runs the batch-end
+// bookkeeping
+__global__ void __launch_bounds__(kThreads) k_nodal_apply_commit(GraphDev g, int64_t c0, int64_t c1, int32_t* part,
+                                                                 const int32_t* __restrict__ move_to,
+                                                                 const int32_t* __restrict__ from, int beg, int end,
+                                                                 int ld, int* __restrict__ M, int* __restrict__ Mt,
+                                                                 int cld, int* __restrict__ CS,
+                                                                 int32_t* __restrict__ dout, int32_t* __restrict__ din,
+                                                                 NodalCtl* ctl, CtlArgs c) {
+  __shared__ int s_mkey[1 << kApplyMLg], s_mval[1 << kApplyMLg];
+  __shared__ int s_ckey[1 << kApplyCLg], s_cval[1 << kApplyCLg];
+  if (ctl->done) return;   // set only by the last CTA below, after every CTA passed here
+  const DeltaTables t{s_mkey, s_mval, s_ckey, s_cval, kApplyMLg, kApplyCLg};
+  tables_clear(t);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = static_cast<int64_t>(gridDim.x) * kWarps;
+  for (int64_t q = c0 + static_cast<int64_t>(blockIdx.x) * kWarps + (threadIdx.x >> 5); q < c1; q += nw)
+    apply_chunk<LdNC, LdPlain>(__ldg(g.chunks + q), g, part, move_to, from, beg, end, t, ld, M, Mt, cld, CS, dout,
+                               din, lane);
+  tables_flush(t, M, Mt, CS, ld, cld);
+  if (c.active) {
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned done_ctas = atomicAdd(&ctl->apply_done, 1u);
+      if (done_ctas == gridDim.x - 1) {
+        __threadfence();
+        ctl_batch_end(ctl, c);
+        ctl->apply_done = 0;
       }
     }
   }
 }
 
-__global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__ move_to,
-                               const int32_t* __restrict__ kout, const int32_t* __restrict__ kin,
-                               int beg, int end, int update_degrees, int32_t* __restrict__ dout,
-                               int32_t* __restrict__ din, NodalCtl* ctl, CtlArgs c);
-
-// update (:433-458), second half: the sweep's cumulative dS is recorded for
-// this sweep and added to S after every batch (as the reference does), then
-// the convergence test -mean < thr * S ends the nodal phase
-__device__ __forceinline__ void ctl_batch_end(NodalCtl* ctl, const CtlArgs& c) {
-  if (ctl->done) return;
-  const long long cum = static_cast<long long>(ctl->cum_q);
-  const int itr = ctl->itr;
-  c.ide_q[itr] = cum;
-  c.ide_n[itr] = ctl->cum_ninf;
-  ctl->S_q += cum;
-  ctl->S_ninf |= ctl->cum_ninf;
-  ctl->batches++;
-  ctl->proposals += c.batch_vertices;
-  ctl->edge_visits += c.batch_edges;
-  if (itr >= c.W - 1) {
-    double S_d = ctl->S_ninf ? -INFINITY : static_cast<double>(ctl->S_q) / kQ32;
-    if (-ctl->mean < c.thr * S_d) ctl->done = 1;
-  }
-}
-
 // commits the batch's moves (degrees, partition) and runs the batch-end
-// bookkeeping in one launch; the bookkeeping reads only the control block
+// bookkeeping in one launch (sorted views, which are rebuilt per batch)
 __global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__ move_to,
                                const int32_t* __restrict__ kout, const int32_t* __restrict__ kin,
                                int beg, int end, int update_degrees, int32_t* __restrict__ dout,
@@ -627,29 +979,183 @@ __global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__
   }
 }
 
-// prepare_batch (:381-395): S from the entropy kernel, the moving average
-// of the previous sweeps' dS, and a fresh cumulative sum for this sweep
 __global__ void k_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const long long* ide_q,
                                   const int* ide_n) {
-  if (ctl->done) return;
-  const int itr = static_cast<int>(ctl->sweeps);
-  ctl->itr = itr;
-  ctl->S_q = model_q - static_cast<long long>(ctl->entropy_acc);
-  ctl->S_ninf = 0;
-  double mean = 0.0;
-  if (itr >= W - 1) {
-    long long sum = 0;
-    int ninf = 0;
-    for (int i = itr - W + 1; i < itr; i++) {
-      sum += ide_q[i];
-      ninf |= ide_n[i];
+  ctl_sweep_start(ctl, model_q, W, ide_q, ide_n);
+}
+
+// --- persistent nodal phase ----------------------------------------------------
+constexpr int kPThreads = 1024;   // one CTA per SM
+constexpr int kPWarps = kPThreads / 32;
+constexpr int kPHubLg = 13;
+constexpr int kPHubSlots = 1 << kPHubLg;  // hub table slots: 2 * min(deg, B) rounded up, B <= 4096
+constexpr unsigned long long kBarrierTimeoutNs = 200ull * 1000ull * 1000ull;
+// dynamic shared memory: per-warp tables and lists, then the hub table
+constexpr size_t kPWarpInts = 3 * kHCap + kHubDegree;
+constexpr size_t kPSmemBytes = sizeof(int) * (kPWarps * kPWarpInts + 3 * kPHubSlots);
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void red_release_add64(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+constexpr unsigned long long kBarDone = 1ull << 32;
+
+// Grid-wide barrier of the persistent kernel (all CTAs are co-resident:
+// cooperative launch).  ctl->bar counts arrivals over the whole launch in
+// its low 32 bits; barrier number k is passed once it reaches
+// k * gridDim.x (`target`, advanced here).  After __syncthreads, thread 0
+// adds its arrival with release semantics (publishing the CTA's writes)
+// and waits with acquire loads.  The arrival may also carry kBarDone, which
+// every CTA then sees in the same load.  A wait gives up after
+// kBarrierTimeoutNs and sets bar_err.  Returns -1 on error (every CTA then
+// leaves at its next barrier), else 1 if kBarDone is set, else 0.
+__device__ __forceinline__ int grid_barrier(NodalCtl* ctl, unsigned* target, bool publish_done, int* s_state) {
+  *target += gridDim.x;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    red_release_add64(&ctl->bar, publish_done ? 1ull + kBarDone : 1ull);
+    const unsigned long long t0 = global_ns();
+    unsigned spins = 0;
+    int st;
+    for (;;) {
+      const unsigned long long v = ld_acquire64(&ctl->bar);
+      if (static_cast<unsigned>(v) >= *target) {
+        st = (v & ~0xffffffffull) ? 1 : 0;
+        break;
+      }
+      if ((++spins & 63u) == 0) {
+        if (*reinterpret_cast<volatile int*>(&ctl->bar_err)) {
+          st = -1;
+          break;
+        }
+        if (global_ns() - t0 > kBarrierTimeoutNs) {
+          atomicExch(&ctl->bar_err, 1);
+          st = -1;
+          break;
+        }
+      }
     }
-    mean = ninf ? -INFINITY : (static_cast<double>(sum) / kQ32) / static_cast<double>(W - 1);
+    *s_state = st;
   }
-  ctl->mean = mean;
-  ctl->cum_q = 0;
-  ctl->cum_ninf = 0;
-  ctl->sweeps++;
+  __syncthreads();
+  return *s_state;
+}
+
+// One stage's nodal phase in one cooperative launch: up to `maxitr` sweeps,
+// each an entropy pass, the sweep-start bookkeeping, and for every batch a
+// proposal pass (hubs first, one per CTA; then warp-per-vertex, first one
+// vertex per warp of the CTAs without a hub, the rest handed out by a
+// counter) and an apply pass over the batch's edge chunks, during which
+// one thread runs the batch-end bookkeeping.  Leaves when the convergence
+// test sets `done`.
+__global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
+  extern __shared__ int dyn[];
+  __shared__ CtaTally s_tally;
+  __shared__ HubShared<kPWarps> sh;
+  __shared__ int s_base, s_state;
+  using Ops = DenseOpsT<LdCG>;
+  const Ops ops{p.v, p.a.B};
+  NodalCtl* ctl = p.a.ctl;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kPWarps + wib;
+  const int nw = gridDim.x * kPWarps;
+  int* wtab = dyn + wib * kPWarpInts;
+  int* htab = dyn + kPWarps * kPWarpInts;   // hub table during proposals, delta tables during apply
+  const DeltaTables dt{htab, htab + kPHubSlots, htab + 2 * kPHubSlots, htab + 2 * kPHubSlots + kPHubSlots / 2,
+                       kPHubLg, kPHubLg - 1};
+  const int B = p.a.B;
+  const int64_t cells = static_cast<int64_t>(B) * B;
+  unsigned target = 0;
+  unsigned long long my_bytes = 0;
+  for (int sw = 0; sw < p.maxitr; sw++) {
+    // data term of S for this sweep (the entropy kernel's sum)
+    {
+      long long acc = 0;
+      for (int64_t c = static_cast<int64_t>(blockIdx.x) * kPThreads + threadIdx.x; c < cells;
+           c += static_cast<int64_t>(gridDim.x) * kPThreads) {
+        const int i = static_cast<int>(c / B), j = static_cast<int>(c - static_cast<int64_t>(i) * B);
+        const int m = __ldcg(p.v.M + static_cast<int64_t>(i) * p.v.ld + j);
+        if (m) acc += q32(g_term(p.a.L, m, __ldcg(p.din + j), __ldcg(p.dout + i)));
+      }
+      acc = warp_sum_ll(acc);
+      if (lane == 0 && acc) atomicAdd(&ctl->entropy_acc, static_cast<unsigned long long>(acc));
+    }
+    if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl_sweep_start(ctl, p.model_q, p.W, p.ide_q, p.ide_n);
+      ctl->entropy_acc = 0;
+    }
+    if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+    const uint32_t itr = static_cast<uint32_t>(sw);   // ctl->sweeps before this sweep started
+    for (int bi = 0; bi * p.bs < p.n; bi++) {
+      NodalArgs a = p.a;
+      a.beg = bi * p.bs;
+      a.end = a.beg + p.bs < p.n ? a.beg + p.bs : p.n;
+      const int count = a.end - a.beg;
+      // proposals
+      if (threadIdx.x == 0) s_tally = CtaTally{0, 0, 0, 0};
+      __syncthreads();
+      const int hub_lo = __ldg(p.batch_hub + bi), hub_hi = __ldg(p.batch_hub + bi + 1);
+      const int hcta = min(hub_hi - hub_lo, static_cast<int>(gridDim.x));
+      for (int h = hub_lo + blockIdx.x; h < hub_hi; h += gridDim.x)
+        hub_vertex<Ops, kPThreads>(a, ops, __ldg(p.hubs + h), itr, htab, kPHubSlots, &sh, &my_bytes);
+      const int first = (gridDim.x - hcta) * kPWarps;   // vertices handed out without the counter
+      if (static_cast<int>(blockIdx.x) >= hcta) {
+        const int i = (blockIdx.x - hcta) * kPWarps + wib;
+        if (i < count)
+          warp_vertex(a, ops, a.beg + i, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap, &s_tally,
+                      lane, &my_bytes);
+      }
+      // the rest in rounds of one vertex per warp, kPWarps per counter step
+      for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_base = first + static_cast<int>(atomicAdd(&ctl->vnext, static_cast<unsigned>(kPWarps)));
+        __syncthreads();
+        const int i0 = s_base;
+        if (i0 >= count) break;
+        if (i0 + wib < count)
+          warp_vertex(a, ops, a.beg + i0 + wib, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap,
+                      &s_tally, lane, &my_bytes);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) tally_flush(&s_tally, ctl);
+      if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+      // apply + commit; one thread closes the batch meanwhile
+      bool done = false;
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const long long edges = (static_cast<long long>(__ldg(p.a.out_ptr + a.end)) - __ldg(p.a.out_ptr + a.beg)) +
+                                (static_cast<long long>(__ldg(p.a.in_ptr + a.end)) - __ldg(p.a.in_ptr + a.beg));
+        const CtlArgs ca{1, p.W, p.thr, p.ide_q, p.ide_n, count, edges};
+        done = ctl_batch_end(ctl, ca);
+        ctl->vnext = 0;
+      }
+      tables_clear(dt);
+      __syncthreads();
+      const int64_t c0 = __ldg(p.chunk_ptr + a.beg), c1 = __ldg(p.chunk_ptr + a.end);
+      for (int64_t q = c0 + gw; q < c1; q += nw)
+        apply_chunk<LdCG, LdCG>(__ldg(p.g.chunks + q), p.g, p.part, a.move_to, a.from, a.beg, a.end, dt, p.v.ld,
+                                p.M, p.Mt, p.v.cld, p.CS, p.dout, p.din, lane);
+      tables_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
+      const int st = grid_barrier(ctl, &target, done, &s_state);
+      if (st != 0) {   // converged (or a barrier failed)
+        if (p.a.stats && lane == 0 && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
+        return;
+      }
+    }
+  }
+  if (p.a.stats && lane == 0 && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
 }
 
 // the hub CTAs run on a second stream, concurrently with the warp kernel
@@ -678,17 +1184,46 @@ void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const Stre
 
 }  // namespace
 
-// the hub kernel's dynamic shared memory limit, set once per device
+namespace {
+int g_phase_grid[64];
+}
+
+// dynamic shared memory limits, set once per device, and the grid of the
+// persistent kernel (CTAs per SM that fit x SMs; 0 if the device cannot
+// run it cooperatively)
 void nodal_configure(int device) {
   static std::once_flag once[64];
   if (device < 0 || device >= 64) return;
-  std::call_once(once[device], [] {
+  std::call_once(once[device], [device] {
     const int smem = static_cast<int>(sizeof(int) * 3 * kHubSmemSlots);
     USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<DenseOps>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<SortedOps>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    USAP_CUDA(cudaFuncSetAttribute(k_nodal_phase, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kPSmemBytes)));
+    int coop = 0, sms = 0, per_sm = 0;
+    USAP_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    USAP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nodal_phase, kPThreads, kPSmemBytes));
+    g_phase_grid[device] = coop ? per_sm * sms : 0;
   });
+}
+
+int nodal_phase_grid(int device) {
+  if (device < 0 || device >= 64) return 0;
+  nodal_configure(device);
+  return g_phase_grid[device];
+}
+
+int nodal_phase_max_blocks() { return 2 * kPHubSlots / 4; }
+
+void launch_nodal_phase(const PhaseArgs& p, int grid, cudaStream_t st) {
+  PhaseArgs args = p;
+  void* kargs[] = {&args};
+  USAP_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_nodal_phase), dim3(grid), dim3(kPThreads),
+                                        kargs, kPSmemBytes, st));
+  USAP_LAUNCHED();
 }
 
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
@@ -711,16 +1246,16 @@ void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st) {
   USAP_LAUNCHED();
 }
 
-void launch_nodal_apply_dense(const GraphDev& g, const int32_t* part, int32_t* move_to, int o0,
-                              int n_out, int i0, int n_in, int ld, int* M, int* Mt, int cld, int* CS,
-                              cudaStream_t st) {
-  const long long total = static_cast<long long>(n_out) + n_in;
-  if (total <= 0) return;
-  long long blocks = (total + kThreads - 1) / kThreads;
-  if (blocks > 148 * 16) blocks = 148 * 16;
-  k_nodal_apply_dense<<<static_cast<int>(blocks), kThreads, 0, st>>>(
-      g.out_src, g.out_idx, g.out_w, g.in_dst, g.in_idx, g.in_w, part, move_to, o0, n_out, i0, n_in, ld, M,
-      Mt, cld, CS);
+void launch_nodal_apply_commit_dense(const GraphDev& g, int32_t* part, const int32_t* move_to,
+                                     const int32_t* from, int beg, int end, int64_t c0, int64_t c1,
+                                     int ld, int* M, int* Mt, int cld, int* CS, int32_t* dout,
+                                     int32_t* din, NodalCtl* ctl, const CtlArgs& c, cudaStream_t st) {
+  const int64_t items = c1 - c0;
+  if (items <= 0) return;
+  int64_t blocks = (items + kWarps - 1) / kWarps;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_nodal_apply_commit<<<static_cast<int>(blocks), kThreads, 0, st>>>(g, c0, c1, part, move_to, from, beg, end, ld,
+                                                                      M, Mt, cld, CS, dout, din, ctl, c);
   USAP_LAUNCHED();
 }
 

@@ -43,7 +43,7 @@ class Params(C.Structure):
                 ("dfs_depth", C.c_int32), ("t_block_num", C.c_int32), ("seed", C.c_uint64),
                 ("init_mode", C.c_int32), ("dense_max", C.c_int32), ("device", C.c_int32),
                 ("stats", C.c_int32), ("trace_kinds", C.c_int32), ("sweep_graphs", C.c_int32),
-                ("reserved", C.c_int32 * 4)]
+                ("persistent", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class Result(C.Structure):

@@ -209,6 +209,8 @@ struct PhaseArgs {
   int *M, *Mt, *CS;         // the tile behind `v`, written by the apply pass
   const int32_t* hubs;      // hub vertex ids, ascending
   const int32_t* batch_hub; // first hub of each batch (batches + 1 entries)
+  const int2* units;        // per batch: vertex pairs of degree <= 64, or (v, -2) for 64 < degree <= 128
+  const int32_t* unit_ptr;  // first unit of each batch (batches + 1 entries)
   const int64_t* chunk_ptr;
   int n, bs, maxitr, W;
   double thr;

@@ -166,7 +166,7 @@ void Job::free_graph() {
 
 void Job::free_state() {
   for (auto& s : slots_) dfree(s);
-  dfree(move_to_); dfree(from_); dfree(dout_); dfree(din_); dfree(batch_hub_);
+  dfree(move_to_); dfree(from_); dfree(dout_); dfree(din_); dfree(batch_hub_); dfree(unit_ptr_); dfree(units_);
   batch_hub_bs_ = 0;
   batch_hub_cap_ = 0;
   dfree(M_); dfree(Mt_); dfree(CS_);
@@ -613,12 +613,54 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
       const int32_t v = static_cast<int32_t>(std::min<int64_t>(static_cast<int64_t>(b) * bs_, n));
       bh[b] = static_cast<int32_t>(std::lower_bound(hub_ids.begin(), hub_ids.end(), v) - hub_ids.begin());
     }
+    // work units: pairs of vertices of degree <= 64 (half-warps), single
+    // vertices of degree <= 128 (warps); hubs are proposed by whole CTAs
+    std::vector<int32_t> up(static_cast<size_t>(nb) + 1, 0);
+    std::vector<int32_t> un;
+    un.reserve(2 * static_cast<size_t>(n));
+    std::vector<int32_t> mid;
+    for (int32_t b = 0; b < nb; b++) {
+      const int32_t beg = b * bs_, end = std::min(n, beg + bs_);
+      int32_t pending = -1;
+      mid.clear();
+      for (int32_t v = beg; v < end; v++) {
+        const int64_t deg = (hg_->out_ptr[v + 1] - hg_->out_ptr[v]) + (hg_->in_ptr[v + 1] - hg_->in_ptr[v]);
+        if (deg > kHubDegree) continue;
+        if (deg > kHubDegree / 2) {
+          mid.push_back(v);
+        } else if (pending < 0) {
+          pending = v;
+        } else {
+          un.push_back(pending);
+          un.push_back(v);
+          pending = -1;
+        }
+      }
+      if (pending >= 0) {
+        un.push_back(pending);
+        un.push_back(-1);
+      }
+      for (int32_t v : mid) {
+        un.push_back(v);
+        un.push_back(-2);
+      }
+      up[b + 1] = static_cast<int32_t>(un.size() / 2);
+    }
     if (batch_hub_cap_ < nb + 1) {
       dfree(batch_hub_);
+      dfree(unit_ptr_);
       dalloc(&batch_hub_, nb + 1);
+      dalloc(&unit_ptr_, nb + 1);
       batch_hub_cap_ = nb + 1;
     }
+    dfree(units_);
+    int32_t* ud = nullptr;
+    dalloc(&ud, std::max<size_t>(un.size(), 2));
+    units_ = reinterpret_cast<int2*>(ud);
     USAP_CUDA(cudaMemcpyAsync(batch_hub_, bh.data(), sizeof(int32_t) * bh.size(), cudaMemcpyHostToDevice, st_));
+    USAP_CUDA(cudaMemcpyAsync(unit_ptr_, up.data(), sizeof(int32_t) * up.size(), cudaMemcpyHostToDevice, st_));
+    if (!un.empty())
+      USAP_CUDA(cudaMemcpyAsync(ud, un.data(), sizeof(int32_t) * un.size(), cudaMemcpyHostToDevice, st_));
     wait();
     batch_hub_bs_ = bs_;
   }
@@ -634,6 +676,8 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
   pa.CS = CS_;
   pa.hubs = gr_->hubs_dev;
   pa.batch_hub = batch_hub_;
+  pa.units = units_;
+  pa.unit_ptr = unit_ptr_;
   pa.chunk_ptr = g_.chunk_ptr;
   pa.n = n;
   pa.bs = bs_;

@@ -161,6 +161,8 @@ class Job {
   int32_t* move_to_ = nullptr;
   int32_t* from_ = nullptr;
   int32_t* batch_hub_ = nullptr;     // first hub of each batch of size bs_
+  int32_t* unit_ptr_ = nullptr;      // first work unit of each batch
+  int2* units_ = nullptr;            // work units of the persistent kernel
   int32_t batch_hub_bs_ = 0;
   int32_t batch_hub_cap_ = 0;
   int32_t *dout_ = nullptr, *din_ = nullptr;

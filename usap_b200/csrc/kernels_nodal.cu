@@ -68,6 +68,39 @@ constexpr int kChunk = 128;         // blocks per chunk sum of a dense row
 constexpr int kHubThreads = 512;    // threads of a hub CTA
 constexpr int kHubWarps = kHubThreads / 32;
 
+// A group of G lanes of one warp (G = 16: a half-warp; G = 32: the warp)
+// working on one vertex.  Shuffles use width G; ballots are returned as G
+// bits of the caller's group.
+template <int G>
+struct Grp {
+  int gl;          // lane within the group
+  int base;        // first warp lane of the group
+  unsigned mask;   // the group's lanes
+  __device__ __forceinline__ explicit Grp(int lane)
+      : gl(lane & (G - 1)), base(lane & ~(G - 1)),
+        mask(G == 32 ? 0xffffffffu : (((1u << (G & 31)) - 1u) << (lane & ~(G - 1)))) {}
+  __device__ __forceinline__ unsigned ballot(bool p) const { return __ballot_sync(mask, p) >> base; }
+  __device__ __forceinline__ bool any(bool p) const { return __any_sync(mask, p) != 0; }
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  template <class T>
+  __device__ __forceinline__ T shfl(T v, int src) const { return __shfl_sync(mask, v, src, G); }
+  template <class T>
+  __device__ __forceinline__ T sum(T v) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
+    return v;
+  }
+  template <class T>
+  __device__ __forceinline__ T incl_scan(T v) const {
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1) {
+      const T n = __shfl_up_sync(mask, v, o, G);
+      if (gl >= o) v += n;
+    }
+    return v;
+  }
+};
+
 template <class LD>
 struct DenseOpsT {
   using Ld = LD;
@@ -77,48 +110,62 @@ struct DenseOpsT {
     return LD::ld(v.M + static_cast<long long>(x) * v.ld + y);
   }
   // first block i (block-id order) whose cumulative M[u,i]+M[i,u] exceeds t:
-  // a warp scan over the row's chunk sums, then over the 128 entries of the
-  // chosen chunk (4 per lane, 16-byte loads; rows are padded to ld, a
+  // a group scan over the row's chunk sums, then over the 128 entries of the
+  // chosen chunk (128 / G per lane, 16-byte loads; rows are padded to ld, a
   // multiple of 4, with zeros)
-  __device__ __forceinline__ int sym_sample(int u, long long t, int lane, int* scanned) const {
+  template <int G>
+  __device__ __forceinline__ int sym_sample(int u, long long t, const Grp<G>& g, int* scanned) const {
+    constexpr int PER = kChunk / G;
     const int nch = (B + kChunk - 1) / kChunk;
     const int* cs = v.CS + static_cast<long long>(u) * v.cld;
     long long run = 0;
     int c = nch - 1;
-    for (int base = 0; base < nch; base += 32) {
-      const int cc = base + lane;
+    for (int base = 0; base < nch; base += G) {
+      const int cc = base + g.gl;
       const int val = cc < nch ? LD::ld(cs + cc) : 0;
-      const int incl = warp_incl_scan(val, lane);
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      const int incl = g.incl_scan(val);
+      const int total = g.shfl(incl, G - 1);
       if (run + total > t) {
-        const unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
+        const unsigned m = g.ballot(run + incl > t);
         const int l = __ffs(m) - 1;
         c = base + l;
-        run += __shfl_sync(0xffffffffu, incl - val, l);
+        run += g.shfl(incl - val, l);
         break;
       }
       run += total;
     }
-    const int i0 = c * kChunk + lane * 4;
-    int p0 = 0, p1 = 0, p2 = 0, p3 = 0;
-    if (i0 < B) {
-      const int4 a = LD::ld(reinterpret_cast<const int4*>(v.M + static_cast<long long>(u) * v.ld + i0));
-      const int4 b = LD::ld(reinterpret_cast<const int4*>(v.Mt + static_cast<long long>(u) * v.ld + i0));
-      p0 = a.x + b.x;
-      p1 = p0 + a.y + b.y;
-      p2 = p1 + a.z + b.z;
-      p3 = p2 + a.w + b.w;
+    const int i0 = c * kChunk + g.gl * PER;
+    int pr[PER];
+#pragma unroll
+    for (int k = 0; k < PER; k++) pr[k] = 0;
+    const int* mrow = v.M + static_cast<long long>(u) * v.ld;
+    const int* trow = v.Mt + static_cast<long long>(u) * v.ld;
+#pragma unroll
+    for (int q = 0; q < PER / 4; q++) {
+      const int i = i0 + 4 * q;
+      const int prev = q ? pr[4 * q - 1] : 0;
+      if (i < B) {
+        const int4 a = LD::ld(reinterpret_cast<const int4*>(mrow + i));
+        const int4 b = LD::ld(reinterpret_cast<const int4*>(trow + i));
+        pr[4 * q] = prev + a.x + b.x;
+        pr[4 * q + 1] = pr[4 * q] + a.y + b.y;
+        pr[4 * q + 2] = pr[4 * q + 1] + a.z + b.z;
+        pr[4 * q + 3] = pr[4 * q + 2] + a.w + b.w;
+      } else {
+        pr[4 * q] = pr[4 * q + 1] = pr[4 * q + 2] = pr[4 * q + 3] = prev;
+      }
     }
-    const int incl = warp_incl_scan(p3, lane);
-    const long long before = run + incl - p3;
-    const unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
-    const int l = m ? __ffs(m) - 1 : 31;
-    int k = 3;
-    if (before + p0 > t) k = 0;
-    else if (before + p1 > t) k = 1;
-    else if (before + p2 > t) k = 2;
+    const int last = pr[PER - 1];
+    const int incl = g.incl_scan(last);
+    const long long before = run + incl - last;
+    const unsigned m = g.ballot(run + incl > t);
+    const int l = m ? __ffs(m) - 1 : G - 1;
+    int k = PER - 1;
+#pragma unroll
+    for (int kk = PER - 2; kk >= 0; kk--)
+      if (before + pr[kk] > t) k = kk;
     *scanned += nch + kChunk;
-    int i = c * kChunk + l * 4 + __shfl_sync(0xffffffffu, k, l);
+    const int i = c * kChunk + l * PER + g.shfl(k, l);
     return i < B ? i : B - 1;
   }
 };
@@ -134,7 +181,8 @@ struct SortedOps {
     int p = find_sorted(v.col, lo, hi, y);
     return p >= 0 ? __ldg(v.val + p) : 0;
   }
-  __device__ __forceinline__ int sym_sample(int u, long long t, int lane, int* scanned) const {
+  template <int G>
+  __device__ __forceinline__ int sym_sample(int u, long long t, const Grp<G>&, int* scanned) const {
     int lo = __ldg(v.symptr + u), hi = __ldg(v.symptr + u + 1);
     long long base = lo > 0 ? __ldg(v.symcum + lo - 1) : 0;
     int j = upper_bound_i(v.symcum, lo, hi, t + base);
@@ -191,12 +239,12 @@ __device__ __forceinline__ VertexInfo vertex_info(const NodalArgs& a, int v) {
 // target block once the chosen neighbour's block u is known
 // (warp-collective): with probability B / (d_u + B) a uniform block, else
 // a block drawn from row + column u of M
-template <class Ops>
+template <class Ops, int G>
 __device__ __forceinline__ int target_from(const NodalArgs& a, const Ops& ops, const Draws& x, int u,
-                                           int lane, int* scanned) {
+                                           const Grp<G>& g, int* scanned) {
   const long long dau = static_cast<long long>(Ops::Ld::ld(a.dout + u)) + Ops::Ld::ld(a.din + u);
   if (accept_uniform(x.x1, dau, a.B)) return static_cast<int>(draw_below(x.x2, a.B));
-  return ops.sym_sample(u, draw_below(x.x2, dau), lane, scanned);
+  return ops.template sym_sample<G>(u, draw_below(x.x2, dau), g, scanned);
 }
 
 // target block of the proposal for v (warp-collective), reading the
@@ -204,6 +252,7 @@ __device__ __forceinline__ int target_from(const NodalArgs& a, const Ops& ops, c
 template <class Ops>
 __device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops, const Draws& x,
                                               const VertexInfo& vi, int lane, int* scanned) {
+  const Grp<32> g(lane);
   const long long k = vi.kout + vi.kin;
   if (k == 0) return static_cast<int>(draw_below(x.x2, a.B));
   const long long t = draw_below(x.x0, k);
@@ -229,7 +278,7 @@ __device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops
     }
   }
   const int nbr = j < vi.dego ? __ldg(a.out_idx + vi.o0 + j) : __ldg(a.in_idx + vi.i0 + j - vi.dego);
-  return target_from(a, ops, x, Ops::Ld::ld(a.part + nbr), lane, scanned);
+  return target_from(a, ops, x, Ops::Ld::ld(a.part + nbr), g, scanned);
 }
 
 struct TermSums {
@@ -284,12 +333,37 @@ __device__ __forceinline__ void slot_terms(const NodalArgs& a, const Ops& ops, i
   }
 }
 
+// slot_terms from values already loaded: R = M[r,b], S = M[s,b], Di =
+// d_in[b] (if wo > 0) and Rc = M[b,r], Sc = M[b,s], Do = d_out[b] (if wi > 0)
+__device__ __forceinline__ void slot_terms_vals(const double* __restrict__ L, int R, int S, int Rc, int Sc, int Di,
+                                                int Do, int wo, int wi, const DegLogs& dl, TermSums& ts) {
+  if (wo > 0) {
+    const double LD = __ldg(L + Di);
+    ts.acc += q32(g_val(R, __ldg(L + R), LD, dl.r_out));
+    ts.acc += q32(g_val(S, __ldg(L + S), LD, dl.s_out));
+    ts.acc -= q32(g_val(R - wo, __ldg(L + R - wo), LD, dl.r_out_n));
+    ts.acc -= q32(g_val(S + wo, __ldg(L + S + wo), LD, dl.s_out_n));
+    ts.sXR += R;
+    ts.sXS += S;
+  }
+  if (wi > 0) {
+    const double LD = __ldg(L + Do);
+    ts.acc += q32(g_val(Rc, __ldg(L + Rc), dl.r_in, LD));
+    ts.acc += q32(g_val(Sc, __ldg(L + Sc), dl.s_in, LD));
+    ts.acc -= q32(g_val(Rc - wi, __ldg(L + Rc - wi), dl.r_in_n, LD));
+    ts.acc -= q32(g_val(Sc + wi, __ldg(L + Sc + wi), dl.s_in_n, LD));
+    ts.sYR += Rc;
+    ts.sYS += Sc;
+  }
+}
+
 // The 2x2 terms and the entries the move leaves unchanged, one term per
 // lane (lanes 0-11), added to the warp-summed neighbour terms `ts`.  The
 // four new 2x2 terms are subtracted; a -inf among them sets *ninf and is
 // left out of the sum (the reference's dS is then -inf).  Every lane
 // returns the same result.
-__device__ __forceinline__ long long finalize_warp(const double* __restrict__ L, int lane, const TermSums& ts,
+template <int G>
+__device__ __forceinline__ long long finalize_grp(const double* __restrict__ L, const Grp<G>& g, const TermSums& ts,
                                                    long long Rr, long long Rs, long long Sr, long long Ss,
                                                    long long wor, long long wos, long long dr_out,
                                                    long long dr_in, long long ds_out, long long ds_in,
@@ -299,7 +373,7 @@ __device__ __forceinline__ long long finalize_warp(const double* __restrict__ L,
   // g lanes: mult * ((L[i0] - L[i1]) - L[i2]); coefficient lanes: mult * (L[i0] - L[i1])
   long long mult = 0, i0 = 0, i1 = 0, i2 = 0;
   bool coef = false, neg = false;
-  switch (lane) {
+  switch (g.gl) {
     case 0: mult = Rr; i0 = Rr; i1 = dr_in; i2 = dr_out; break;
     case 1: mult = Rs; i0 = Rs; i1 = ds_in; i2 = dr_out; break;
     case 2: mult = Sr; i0 = Sr; i1 = dr_in; i2 = ds_out; break;
@@ -323,8 +397,8 @@ __device__ __forceinline__ long long finalize_warp(const double* __restrict__ L,
   const bool inf = neg && isinf(t);
   long long q = inf ? 0 : q32(t);
   if (neg) q = -q;
-  *ninf = __any_sync(0xffffffffu, inf) ? 1 : 0;
-  return ts.acc + warp_sum_ll(q);
+  *ninf = g.any(inf) ? 1 : 0;
+  return ts.acc + g.sum(q);
 }
 
 // per-vertex outputs of a decided proposal; returns whether it is accepted
@@ -373,36 +447,38 @@ __device__ __forceinline__ void tally_flush(const CtaTally* t, NodalCtl* ctl) {
   if (t->near) atomicAdd(&ctl->near, t->near);
 }
 
-// Proposal for one vertex of degree <= kHubDegree by one warp (all 32
-// lanes).  Each lane loads up to four neighbours at once (ids, then their
-// blocks) and keeps them in registers: the hash of neighbour blocks and the
-// target draw (whose chosen neighbour is among them) come from the same
-// loads.  key/two/twi: the warp's kHCap-slot table; list: kHubDegree ints.
-template <class Ops>
-__device__ __forceinline__ void warp_vertex(const NodalArgs& a, const Ops& ops, int v, uint32_t itr,
-                                            int* key, int* two, int* twi, int* list, CtaTally* tl,
-                                            int lane, unsigned long long* my_bytes) {
+// Proposal for one vertex of degree <= 4 * G by a group of G lanes (a
+// warp, G = 32, or a half-warp, G = 16).  Each lane loads up to four
+// neighbours at once (ids, then their blocks) and keeps them in registers:
+// the hash of neighbour blocks and the target draw (whose chosen neighbour
+// is among them) come from the same loads.  key/two/twi: the group's table
+// of 8 * G slots; list: 4 * G ints.
+template <class Ops, int G>
+__device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops, int v, uint32_t itr, int* key,
+                                             int* two, int* twi, int* list, CtaTally* tl, const Grp<G>& g,
+                                             unsigned long long* my_bytes) {
   using LD = typename Ops::Ld;
-  const unsigned lanes_below = (1u << lane) - 1u;
+  constexpr int KN = 4;   // neighbours per lane
+  const unsigned lanes_below = (1u << g.gl) - 1u;
   const VertexInfo vi = vertex_info<Ops>(a, v);
   const int deg = vi.dego + vi.degi;
-  if (deg > kHubDegree) return;   // proposed by a whole CTA
+  if (deg > KN * G) return;   // proposed by a larger group or a whole CTA
   const int r = vi.r;
   const Draws x = philox(static_cast<uint32_t>(v), itr, a.stage, kTagNodal, a.seed);
   const long long dr_out = LD::ld(a.dout + r), dr_in = LD::ld(a.din + r);
   int lg = 5;
   while ((1 << lg) < 2 * deg) lg++;
-  const int cap = 1 << lg;   // <= kHCap since deg <= kHubDegree
-  for (int i = lane; i < cap; i += 32) {
+  const int cap = 1 << lg;   // <= 8 * G
+  for (int i = g.gl; i < cap; i += G) {
     key[i] = -1;
     two[i] = 0;
     twi[i] = 0;
   }
-  __syncwarp();
-  int nb[4], wv[4], pb[4];
+  g.sync();
+  int nb[KN], wv[KN], pb[KN];
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const int j = lane + 32 * k;
+  for (int k = 0; k < KN; k++) {
+    const int j = g.gl + G * k;
     nb[k] = 0;
     wv[k] = 0;
     if (j < deg) {
@@ -412,10 +488,10 @@ __device__ __forceinline__ void warp_vertex(const NodalArgs& a, const Ops& ops, 
     }
   }
 #pragma unroll
-  for (int k = 0; k < 4; k++) pb[k] = lane + 32 * k < deg ? LD::ld(a.part + nb[k]) : 0;
+  for (int k = 0; k < KN; k++) pb[k] = g.gl + G * k < deg ? LD::ld(a.part + nb[k]) : 0;
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    const int j = lane + 32 * k;
+  for (int k = 0; k < KN; k++) {
+    const int j = g.gl + G * k;
     if (j < deg) table_insert(key, two, twi, cap, lg, pb[k], wv[k], j < vi.dego);
   }
   // the target: neighbour position j by weight, its block from registers
@@ -433,71 +509,96 @@ __device__ __forceinline__ void warp_vertex(const NodalArgs& a, const Ops& ops, 
       long long run = 0;
       j = deg - 1;
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        if (32 * k >= deg) break;
-        const long long ww = lane + 32 * k < deg ? wv[k] : 0;
-        const long long incl = warp_incl_scan_ll(ww, lane);
-        const long long total = __shfl_sync(0xffffffffu, incl, 31);
+      for (int k = 0; k < KN; k++) {
+        if (G * k >= deg) break;
+        const long long ww = g.gl + G * k < deg ? wv[k] : 0;
+        const long long incl = g.incl_scan(ww);
+        const long long total = g.shfl(incl, G - 1);
         if (run + total > t) {
-          const unsigned m = __ballot_sync(0xffffffffu, run + incl > t);
-          j = 32 * k + __ffs(m) - 1;
+          const unsigned m = g.ballot(run + incl > t);
+          j = G * k + __ffs(m) - 1;
           break;
         }
         run += total;
       }
     }
-    const int kq = j >> 5;
+    const int kq = j / G;
     const int pj = kq == 0 ? pb[0] : kq == 1 ? pb[1] : kq == 2 ? pb[2] : pb[3];
-    s = target_from(a, ops, x, __shfl_sync(0xffffffffu, pj, j & 31), lane, &scanned);
+    s = target_from(a, ops, x, g.shfl(pj, j & (G - 1)), g, &scanned);
   }
-  __syncwarp();
+  g.sync();
   if (s == r) {
-    if (lane == 0) {
+    if (g.gl == 0) {
       record_stay(a, v, r);
       if (a.stats) *my_bytes += 8 + 8ull * deg + 8ull * scanned;
     }
-    __syncwarp();
+    g.sync();
     return;
   }
   const long long ds_out = LD::ld(a.dout + s), ds_in = LD::ld(a.din + s);
   int e4 = 0;
-  if (lane < 4) e4 = ops.get(lane < 2 ? r : s, (lane & 1) ? s : r);
+  if (g.gl < 4) e4 = ops.get(g.gl < 2 ? r : s, (g.gl & 1) ? s : r);
   const DegLogs dl = deg_logs(a.L, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
   // compact the occupied slots so that each lane takes about one block
   int nlist = 0, noccupied = 0;
-  for (int base = 0; base < cap; base += 32) {
-    const int i = base + lane;
+  for (int base = 0; base < cap; base += G) {
+    const int i = base + g.gl;
     const int b = i < cap ? key[i] : -1;
-    const unsigned occ = __ballot_sync(0xffffffffu, b >= 0);
+    const unsigned occ = g.ballot(b >= 0);
     const bool use = b >= 0 && b != r && b != s;
-    const unsigned mu = __ballot_sync(0xffffffffu, use);
+    const unsigned mu = g.ballot(use);
     if (use) list[nlist + __popc(mu & lanes_below)] = i;
     nlist += __popc(mu);
     noccupied += __popc(occ);
   }
-  __syncwarp();
+  g.sync();
+  // each lane has at most four slots (nlist <= 4 * G): their M entries
+  // and degrees are loaded in two rounds of two, then the log terms
   TermSums ts{0, 0, 0, 0, 0};
-  for (int t = lane; t < nlist; t += 32) {
-    const int i = list[t];
-    slot_terms(a, ops, r, s, key[i], two[i], twi[i], dl, ts);
+#pragma unroll
+  for (int k0 = 0; k0 < 4; k0 += 2) {
+    int R[2], S[2], Rc[2], Sc[2], Di[2], Do[2], wo[2], wi[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const int t = g.gl + G * (k0 + k);
+      R[k] = S[k] = Rc[k] = Sc[k] = Di[k] = Do[k] = wo[k] = wi[k] = 0;
+      if (t < nlist) {
+        const int i = list[t];
+        const int b = key[i];
+        wo[k] = two[i];
+        wi[k] = twi[i];
+        if (wo[k] > 0) {
+          R[k] = ops.get(r, b);
+          S[k] = ops.get(s, b);
+          Di[k] = LD::ld(a.din + b);
+        }
+        if (wi[k] > 0) {
+          Rc[k] = ops.get(b, r);
+          Sc[k] = ops.get(b, s);
+          Do[k] = LD::ld(a.dout + b);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++) slot_terms_vals(a.L, R[k], S[k], Rc[k], Sc[k], Di[k], Do[k], wo[k], wi[k], dl, ts);
   }
-  ts.acc = warp_sum_ll(ts.acc);
-  ts.sXR = warp_sum_i(ts.sXR);
-  ts.sXS = warp_sum_i(ts.sXS);
-  ts.sYR = warp_sum_i(ts.sYR);
-  ts.sYS = warp_sum_i(ts.sYS);
-  const long long Rr = __shfl_sync(0xffffffffu, e4, 0), Rs = __shfl_sync(0xffffffffu, e4, 1);
-  const long long Sr = __shfl_sync(0xffffffffu, e4, 2), Ss = __shfl_sync(0xffffffffu, e4, 3);
+  ts.acc = g.sum(ts.acc);
+  ts.sXR = g.sum(ts.sXR);
+  ts.sXS = g.sum(ts.sXS);
+  ts.sYR = g.sum(ts.sYR);
+  ts.sYS = g.sum(ts.sYS);
+  const long long Rr = g.shfl(e4, 0), Rs = g.shfl(e4, 1);
+  const long long Sr = g.shfl(e4, 2), Ss = g.shfl(e4, 3);
   const long long wor = table_lookup_wo(key, two, cap, lg, r);
   const long long wos = table_lookup_wo(key, two, cap, lg, s);
   int ninf;
-  const long long acc = finalize_warp(a.L, lane, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
-                                      vi.kout, vi.kin, &ninf);
-  if (lane == 0) {
+  const long long acc = finalize_grp(a.L, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
+                                     vi.kout, vi.kin, &ninf);
+  if (g.gl == 0) {
     tally(tl, emit(a, v, r, s, acc, ninf), acc, ninf);
     if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * noccupied + 48 + 8ull * scanned;
   }
-  __syncwarp();
+  g.sync();
 }
 
 // One warp per vertex of degree <= kHubDegree; 5 CTAs per SM so that a
@@ -517,7 +618,8 @@ __global__ void __launch_bounds__(kThreads, 5) k_nodal_propose(NodalArgs a, Ops 
   const int nwarps = gridDim.x * kWarps;
   unsigned long long my_bytes = 0;
   for (int v = a.beg + blockIdx.x * kWarps + wib; v < a.end; v += nwarps)
-    warp_vertex(a, ops, v, itr, s_key[wib], s_wo[wib], s_wi[wib], s_list[wib], &s_tally, lane, &my_bytes);
+    group_vertex(a, ops, v, itr, s_key[wib], s_wo[wib], s_wi[wib], s_list[wib], &s_tally, Grp<32>(lane),
+                 &my_bytes);
   __syncthreads();
   if (threadIdx.x == 0) tally_flush(&s_tally, a.ctl);
   if (a.stats && lane == 0 && my_bytes) atomicAdd(&a.ctl->bytes, my_bytes);
@@ -672,7 +774,7 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
     const long long wor = table_lookup_wo(key, two, cap, lg, r);
     const long long wos = table_lookup_wo(key, two, cap, lg, s);
     int ninf;
-    const long long acc = finalize_warp(a.L, lane, tot, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
+    const long long acc = finalize_grp(a.L, Grp<32>(lane), tot, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
                                         vi.kout, vi.kin, &ninf);
     if (lane == 0) {
       const bool accept = emit(a, v, r, s, acc, ninf);
@@ -985,8 +1087,9 @@ __global__ void k_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const
 }
 
 // --- persistent nodal phase ----------------------------------------------------
-constexpr int kPThreads = 1024;   // one CTA per SM
+constexpr int kPThreads = 768;    // one CTA per SM (80 registers a thread)
 constexpr int kPWarps = kPThreads / 32;
+constexpr int kUnitWarp = -2;     // work unit of one vertex with 64 < degree <= 128
 constexpr int kPHubLg = 13;
 constexpr int kPHubSlots = 1 << kPHubLg;  // hub table slots: 2 * min(deg, B) rounded up, B <= 4096
 constexpr unsigned long long kBarrierTimeoutNs = 200ull * 1000ull * 1000ull;
@@ -1111,23 +1214,36 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       const int hcta = min(hub_hi - hub_lo, static_cast<int>(gridDim.x));
       for (int h = hub_lo + blockIdx.x; h < hub_hi; h += gridDim.x)
         hub_vertex<Ops, kPThreads>(a, ops, __ldg(p.hubs + h), itr, htab, kPHubSlots, &sh, &my_bytes);
-      const int first = (gridDim.x - hcta) * kPWarps;   // vertices handed out without the counter
+      // work units: two vertices of degree <= 64 (a half-warp each) or one
+      // of degree <= 128 (a warp)
+      const int u_lo = __ldg(p.unit_ptr + bi), nun = __ldg(p.unit_ptr + bi + 1) - u_lo;
+      auto run_unit = [&](int u) {
+        const int2 un = __ldg(p.units + u_lo + u);
+        if (un.y == kUnitWarp) {
+          group_vertex(a, ops, un.x, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap, &s_tally,
+                       Grp<32>(lane), &my_bytes);
+        } else {
+          const int h = lane >> 4;
+          const int vv = h ? un.y : un.x;
+          if (vv >= 0)
+            group_vertex(a, ops, vv, itr, wtab + h * (kHCap / 2), wtab + kHCap + h * (kHCap / 2),
+                         wtab + 2 * kHCap + h * (kHCap / 2), wtab + 3 * kHCap + h * (kHubDegree / 2), &s_tally,
+                         Grp<16>(lane), &my_bytes);
+        }
+      };
+      const int first = (gridDim.x - hcta) * kPWarps;   // units handed out without the counter
       if (static_cast<int>(blockIdx.x) >= hcta) {
         const int i = (blockIdx.x - hcta) * kPWarps + wib;
-        if (i < count)
-          warp_vertex(a, ops, a.beg + i, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap, &s_tally,
-                      lane, &my_bytes);
+        if (i < nun) run_unit(i);
       }
-      // the rest in rounds of one vertex per warp, kPWarps per counter step
+      // the rest in rounds of one unit per warp, kPWarps per counter step
       for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_base = first + static_cast<int>(atomicAdd(&ctl->vnext, static_cast<unsigned>(kPWarps)));
         __syncthreads();
         const int i0 = s_base;
-        if (i0 >= count) break;
-        if (i0 + wib < count)
-          warp_vertex(a, ops, a.beg + i0 + wib, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap,
-                      &s_tally, lane, &my_bytes);
+        if (i0 >= nun) break;
+        if (i0 + wib < nun) run_unit(i0 + wib);
       }
       __syncthreads();
       if (threadIdx.x == 0) tally_flush(&s_tally, ctl);
@@ -1150,12 +1266,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       tables_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
       const int st = grid_barrier(ctl, &target, done, &s_state);
       if (st != 0) {   // converged (or a barrier failed)
-        if (p.a.stats && lane == 0 && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
+        if (p.a.stats && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
         return;
       }
     }
   }
-  if (p.a.stats && lane == 0 && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
+  if (p.a.stats && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
 }
 
 // the hub CTAs run on a second stream, concurrently with the warp kernel

@@ -17,10 +17,12 @@ value  solve time in seconds with the graph already resident in HBM
 e2e    the same metric through the one-shot C ABI call usap_partition with
        host edge arrays in and the host assignment out (CSR build, host to
        device copies and the device to host read inside the timed region);
-roofline  the nodal proposal kernels (warp-per-vertex + CTA-per-hub), the
-       dominant kernels: algorithmic bytes (per proposing vertex
+roofline  the persistent nodal-phase kernel (k_nodal_phase: one launch per
+       stage runs every sweep's entropy pass, proposals and apply), the
+       dominant kernel: algorithmic bytes (per proposing vertex
        8 + 8 deg + 48 |distinct neighbour blocks| + 48 + 8 * sampled
-       entries) over their CUDA-event time, against the measured copy
+       entries; per entropy pass 4 B^2 + 8 nnz(M); per edge of a moved
+       vertex 24) over its CUDA-event time, against the measured copy
        bandwidth of this B200 pool;
 cpu_baseline  the reference's own partition() (compiled from its sources
        against the Taskflow-API shim, oracle/_ref/ref_main) on the same
@@ -47,7 +49,7 @@ METRIC = "SBP solve time at N=50k & MCMC edge-visits/s; batched vs plain at matc
 WORKLOAD = "dcsbm N=50000 B*=44 within=0.5 alpha=1 (~780k edges), batch 0.1N, K=10"
 REF_MAIN = os.path.join(ROOT, "oracle", "_ref", "ref_main")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-TRAFFIC = os.path.join(ROOT, "profiles", "nodal_propose_c2_traffic.json")
+TRAFFIC = os.path.join(ROOT, "profiles", "nodal_phase_c2_traffic.json")
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -301,7 +303,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     e2e_value = e2e_total / args.steps / 1000.0
     nmi = api.evaluate(G.truth, part)["nmi"]
 
-    # --- roofline of the nodal proposal kernels (instrumented, untimed solve)
+    # --- roofline of the nodal-phase kernel (instrumented, untimed solve)
     _, rs = ctx.partition(solver_params(seed=0, stats=1), want_assign=False)
     peak, peak_kind = hbm_peak()
     kernel_s = rs["ms_nodal_kernel"] / 1000.0
@@ -313,7 +315,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         traffic = tr["dram_bytes_per_launch"]
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "peak_source": peak_kind, "kernel": "nodal propose (warp-per-vertex + hub CTA)",
+                "peak_source": peak_kind, "kernel": "k_nodal_phase (persistent: entropy, proposals, apply)",
                 "algorithmic_bytes_per_launch": per_launch,
                 "avg_launch_us": rs["ms_nodal_kernel"] * 1000 / max(1, rs["nodal_kernel_launches"]),
                 "kernel_share_of_solve": rs["ms_nodal_kernel"] / max(1e-9, rs["ms_total"])}

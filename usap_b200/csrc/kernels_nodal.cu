@@ -1186,12 +1186,19 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
     // data term of S for this sweep (the entropy kernel's sum)
     {
       long long acc = 0;
+      unsigned long long seen = 0, nz = 0;
       for (int64_t c = static_cast<int64_t>(blockIdx.x) * kPThreads + threadIdx.x; c < cells;
            c += static_cast<int64_t>(gridDim.x) * kPThreads) {
         const int i = static_cast<int>(c / B), j = static_cast<int>(c - static_cast<int64_t>(i) * B);
         const int m = __ldcg(p.v.M + static_cast<int64_t>(i) * p.v.ld + j);
-        if (m) acc += q32(g_term(p.a.L, m, __ldcg(p.din + j), __ldcg(p.dout + i)));
+        seen++;
+        if (m) {
+          nz++;
+          acc += q32(g_term(p.a.L, m, __ldcg(p.din + j), __ldcg(p.dout + i)));
+        }
       }
+      // algorithmic bytes: every cell of the tile, two degrees per nonzero
+      if (p.a.stats) my_bytes += 4 * seen + 8 * nz;
       acc = warp_sum_ll(acc);
       if (lane == 0 && acc) atomicAdd(&ctl->entropy_acc, static_cast<unsigned long long>(acc));
     }
@@ -1260,9 +1267,18 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       tables_clear(dt);
       __syncthreads();
       const int64_t c0 = __ldg(p.chunk_ptr + a.beg), c1 = __ldg(p.chunk_ptr + a.end);
-      for (int64_t q = c0 + gw; q < c1; q += nw)
-        apply_chunk<LdCG, LdCG>(__ldg(p.g.chunks + q), p.g, p.part, a.move_to, a.from, a.beg, a.end, dt, p.v.ld,
-                                p.M, p.Mt, p.v.cld, p.CS, p.dout, p.din, lane);
+      for (int64_t q = c0 + gw; q < c1; q += nw) {
+        const int2 ch = __ldg(p.g.chunks + q);
+        apply_chunk<LdCG, LdCG>(ch, p.g, p.part, a.move_to, a.from, a.beg, a.end, dt, p.v.ld, p.M, p.Mt,
+                                p.v.cld, p.CS, p.dout, p.din, lane);
+        // algorithmic bytes of a moved vertex's edge: its neighbour's id and
+        // block (8) and the two updated entries of M (16)
+        if (p.a.stats && lane == 0 && __ldcg(a.move_to + ch.x) >= 0) {
+          const int deg = (__ldg(p.a.out_ptr + ch.x + 1) - __ldg(p.a.out_ptr + ch.x)) +
+                          (__ldg(p.a.in_ptr + ch.x + 1) - __ldg(p.a.in_ptr + ch.x));
+          my_bytes += 24ull * static_cast<unsigned long long>(max(0, min(32, deg - 32 * ch.y)));
+        }
+      }
       tables_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
       const int st = grid_barrier(ctl, &target, done, &s_state);
       if (st != 0) {   // converged (or a barrier failed)

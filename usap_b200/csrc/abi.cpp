@@ -42,6 +42,35 @@ usap_status guarded(F&& f) {
   }
 }
 
+// Solver states kept for usap_partition: creating one (streams, events,
+// pinned control buffers) costs milliseconds, which a one-shot solve would
+// otherwise pay on every call.  At most kIdleJobs idle states per device.
+constexpr size_t kIdleJobs = 4;
+// The idle states are never destroyed: at process exit the CUDA runtime may
+// already be gone.
+std::mutex g_idle_mu;
+std::vector<std::unique_ptr<usap::Job>>* const g_idle = new std::vector<std::unique_ptr<usap::Job>>[64];
+
+std::unique_ptr<usap::Job> acquire_job(int device) {
+  if (device >= 0 && device < 64) {
+    std::lock_guard<std::mutex> lk(g_idle_mu);
+    if (!g_idle[device].empty()) {
+      std::unique_ptr<usap::Job> j = std::move(g_idle[device].back());
+      g_idle[device].pop_back();
+      return j;
+    }
+  }
+  return std::make_unique<usap::Job>(device);
+}
+
+void release_job(std::unique_ptr<usap::Job> j) {
+  const int device = j->device();
+  j->detach();
+  if (device < 0 || device >= 64) return;
+  std::lock_guard<std::mutex> lk(g_idle_mu);
+  if (g_idle[device].size() < kIdleJobs) g_idle[device].push_back(std::move(j));
+}
+
 void check_ctx(usap_ctx* ctx) {
   if (!ctx || !ctx->job) throw usap::Error(USAP_ERR_INVALID, "null context");
 }
@@ -86,14 +115,15 @@ usap_status usap_partition(const usap_graph* g, const usap_params* p, int32_t* o
     usap_params def;
     usap_params_default(&def);
     const usap_params& prm = p ? *p : def;
-    usap::Job job(prm.device);
+    std::unique_ptr<usap::Job> job = acquire_job(prm.device);
     const auto lc0 = usap::launch_count();
-    job.load(*g);
-    job.partition(prm, out_assign, out);
-    out->ms_h2d = job.last_h2d_ms();
-    out->h2d_bytes += job.last_h2d_bytes();
+    job->load(*g);
+    job->partition(prm, out_assign, out);
+    out->ms_h2d = job->last_h2d_ms();
+    out->h2d_bytes += job->last_h2d_bytes();
     out->kernel_launches = usap::launch_count().kernels - lc0.kernels;
     out->cub_calls = usap::launch_count().cub - lc0.cub;
+    release_job(std::move(job));
   });
 }
 

@@ -16,6 +16,7 @@
 namespace usap {
 
 void scc_prepare(HostGraph& g) {
+  if (g.transpose_is_in) return;
   const int32_t n = g.n;
   g.tptr.assign(n + 1, 0);
   g.tidx.resize(g.e);
@@ -53,8 +54,8 @@ int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part) {
       }
     }
   }
-  const std::vector<int32_t>& tptr = g.tptr;
-  const std::vector<int32_t>& tidx = g.tidx;
+  const int32_t* tptr = g.transpose_is_in ? g.in_ptr.data() : g.tptr.data();
+  const int32_t* tidx = g.transpose_is_in ? g.in_idx.data() : g.tidx.data();
   std::vector<uint8_t> visited(n, 0);
   for (int32_t v = 0; v < n; v++) part[v] = -1;
   int32_t b = 0;

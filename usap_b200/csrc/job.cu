@@ -11,6 +11,8 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include <cub/cub.cuh>
 
@@ -111,10 +113,13 @@ Job::Job(int device) : device_(device) {
     throw Error(USAP_ERR_NO_DEVICE, "no CUDA device available");
   if (device < 0 || device >= count) throw Error(USAP_ERR_INVALID, "device index out of range");
   USAP_CUDA(cudaSetDevice(device));
-  cudaDeviceProp prop;
-  USAP_CUDA(cudaGetDeviceProperties(&prop, device));
-  if (prop.major < 10)
+  int major = 0;
+  USAP_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major < 10) {
+    cudaDeviceProp prop;
+    USAP_CUDA(cudaGetDeviceProperties(&prop, device));
     throw Error(USAP_ERR_NO_DEVICE, std::string("device is not sm_100 class: ") + prop.name);
+  }
   pool_configure(device);
   USAP_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
   USAP_CUDA(cudaStreamCreateWithFlags(&st_side_, cudaStreamNonBlocking));
@@ -192,13 +197,33 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   h.src.resize(in.e);
   h.dst.resize(in.e);
   int64_t maxsrc = -1, maxid = -1;
-  for (int64_t i = 0; i < in.e; i++) {
-    int64_t a = static_cast<int64_t>(in.src[i]) - base, b = static_cast<int64_t>(in.dst[i]) - base;
-    if (a < 0 || b < 0) throw Error(USAP_ERR_INVALID, "negative vertex id at edge " + std::to_string(i));
-    maxsrc = std::max(maxsrc, a);
-    maxid = std::max(maxid, std::max(a, b));
-    h.src[i] = static_cast<int32_t>(a);
-    h.dst[i] = static_cast<int32_t>(b);
+  {
+    // converted and checked in slices on host threads
+    const int T = in.e < (1 << 17) ? 1 : std::max(1, std::min<int>(16, static_cast<int>(std::thread::hardware_concurrency())));
+    std::vector<int64_t> ms(T, -1), mi(T, -1), bad(T, -1);
+    auto work = [&](int t) {
+      const int64_t i0 = in.e * t / T, i1 = in.e * (t + 1) / T;
+      int64_t lms = -1, lmi = -1;
+      for (int64_t i = i0; i < i1; i++) {
+        const int64_t a = static_cast<int64_t>(in.src[i]) - base, b = static_cast<int64_t>(in.dst[i]) - base;
+        if ((a < 0 || b < 0) && bad[t] < 0) bad[t] = i;
+        lms = std::max(lms, a);
+        lmi = std::max(lmi, std::max(a, b));
+        h.src[i] = static_cast<int32_t>(a);
+        h.dst[i] = static_cast<int32_t>(b);
+      }
+      ms[t] = lms;
+      mi[t] = lmi;
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; t++) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    for (int t = 0; t < T; t++) {
+      if (bad[t] >= 0) throw Error(USAP_ERR_INVALID, "negative vertex id at edge " + std::to_string(bad[t]));
+      maxsrc = std::max(maxsrc, ms[t]);
+      maxid = std::max(maxid, mi[t]);
+    }
   }
   h.n = in.n > 0 ? in.n : static_cast<int32_t>(maxsrc + 1);
   if (maxid >= h.n)
@@ -220,39 +245,7 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   if (wtot >= (1ll << 24)) throw Error(USAP_ERR_LIMIT, "total edge weight must be below 2^24");
   h.wtot = wtot;
   const int32_t n = h.n;
-  h.out_ptr.assign(n + 1, 0);
-  h.in_ptr.assign(n + 1, 0);
-  h.kout.assign(n, 0);
-  h.kin.assign(n, 0);
-  for (int64_t i = 0; i < h.e; i++) {
-    int32_t ww = h.unit ? 1 : h.w[i];
-    h.out_ptr[h.src[i] + 1]++;
-    h.in_ptr[h.dst[i] + 1]++;
-    h.kout[h.src[i]] += ww;
-    h.kin[h.dst[i]] += ww;
-  }
-  for (int32_t v = 0; v < n; v++) {
-    h.out_ptr[v + 1] += h.out_ptr[v];
-    h.in_ptr[v + 1] += h.in_ptr[v];
-  }
-  h.out_idx.resize(h.e);
-  h.in_idx.resize(h.e);
-  if (!h.unit) {
-    h.out_w.resize(h.e);
-    h.in_w.resize(h.e);
-  }
-  {
-    std::vector<int32_t> fo(h.out_ptr.begin(), h.out_ptr.end() - 1), fi(h.in_ptr.begin(), h.in_ptr.end() - 1);
-    for (int64_t i = 0; i < h.e; i++) {   // stable: edge order within each list
-      int32_t po = fo[h.src[i]]++, pi = fi[h.dst[i]]++;
-      h.out_idx[po] = h.dst[i];
-      h.in_idx[pi] = h.src[i];
-      if (!h.unit) {
-        h.out_w[po] = h.w[i];
-        h.in_w[pi] = h.w[i];
-      }
-    }
-  }
+  build_csr(h);
   scc_prepare(h);
   // per-vertex global hash regions for degrees beyond the shared-memory table
   std::vector<int64_t> hi_off(n, -1);

@@ -20,6 +20,9 @@ struct HostGraph {
   // in-lists ordered by source vertex id (the transpose _scc builds,
   // graph_parallel.hpp:518-523), prepared once at load
   std::vector<int32_t> tptr, tidx;
+  // the edge list was ordered by source: the in-lists are that transpose
+  // already, and tptr/tidx stay empty
+  bool transpose_is_in = false;
   // first 32-edge chunk of each vertex (n + 1 entries; GraphDev::chunks)
   std::vector<int64_t> chunk_ptr;
 };
@@ -27,6 +30,8 @@ struct HostGraph {
 // _scc + _dfs_itr (graph_parallel.hpp:514-603), host side; scc_prepare
 // builds the transpose it walks (once per graph)
 void scc_prepare(HostGraph& g);
+// out- and in-lists (and weighted degrees) from h.src/dst/w in file order
+void build_csr(HostGraph& h);
 int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part);
 
 // host evaluation (evaluate.hpp:18-266 scores + NMI + Hungarian accuracy)
@@ -95,6 +100,10 @@ class Job {
     trace_user_ = user;
   }
   void partition(const usap_params& p, int32_t* out_assign, usap_result* res);
+  // drops the graph (its device memory is freed when no job holds it);
+  // the solver state stays allocated for the next graph
+  void detach() { free_graph(); }
+  int device() const { return device_; }
 
   // phase-level operations on host buffers
   int32_t op_scc(int32_t depth, int32_t* part);

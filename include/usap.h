@@ -79,7 +79,8 @@ typedef struct usap_params {
   int32_t persistent;  /* 1 (default): run each stage's nodal phase as one cooperative kernel
                           when the tile is dense and B <= 4096; 0: one launch per batch.
                           usap_batch_partition always uses per-batch launches. */
-  int32_t reserved[3];
+  int32_t persistent_ctas; /* CTAs of the cooperative kernel (one per SM); 0 = every SM */
+  int32_t reserved[2];
 } usap_params;
 
 typedef struct usap_result {
@@ -204,6 +205,50 @@ usap_status usap_op_nodal_batch(usap_ctx* ctx, int32_t* part, int32_t B, int32_t
                                 uint64_t seed, int32_t* prop_s, int64_t* prop_q,
                                 int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
                                 int64_t* moves);
+
+/* --- served form: a partition service on one GPU --------------------------
+ * The reference has no service; this replaces a caller running Graph_P
+ * objects on its own threads.  usap_server_submit copies the edge list and
+ * returns a ticket at once; worker threads (each with its own streams and
+ * solver state) take requests in arrival order whenever a worker is free
+ * and the request's device-memory footprint fits in what running requests
+ * leave of the budget, so requests that arrive while others run start as
+ * soon as a slot and memory free up and their kernels overlap on the GPU.
+ * out_assign must stay valid until the request is taken with poll or
+ * wait.  A request's result is the same as usap_partition's for the same
+ * graph and parameters (the cooperative nodal kernel is not used, since it
+ * would hold every SM). */
+typedef struct usap_server usap_server;
+typedef struct usap_server_config {
+  int32_t device;
+  int32_t workers;        /* concurrent requests (0: min(32, 2 x host threads)) */
+  int64_t memory_budget;  /* bytes of device memory for admitted requests (0: 80% of free) */
+  int32_t reserved[4];
+} usap_server_config;
+typedef struct usap_server_timing {
+  double ms_queued;   /* submit to start */
+  double ms_running;  /* start to finish */
+  double ms_latency;  /* submit to finish */
+} usap_server_timing;
+typedef struct usap_server_stats {
+  int32_t queued, running, workers, peak_running;
+  int64_t completed, failed;
+  int64_t admitted_bytes, peak_admitted_bytes, memory_budget;
+} usap_server_stats;
+void usap_server_config_default(usap_server_config* c);
+usap_status usap_server_create(const usap_server_config* cfg, usap_server** out);
+/* finishes every submitted request first */
+void usap_server_destroy(usap_server* s);
+/* USAP_ERR_LIMIT when the request alone exceeds the memory budget */
+usap_status usap_server_submit(usap_server* s, const usap_graph* g, const usap_params* p,
+                               int32_t* out_assign, int64_t* ticket);
+/* *done = 0: still queued or running.  *done = 1: finished and forgotten;
+ * the call returns the request's own status (and message). */
+usap_status usap_server_poll(usap_server* s, int64_t ticket, int32_t* done, usap_result* result,
+                             usap_server_timing* timing);
+usap_status usap_server_wait(usap_server* s, int64_t ticket, usap_result* result,
+                             usap_server_timing* timing);
+usap_status usap_server_get_stats(usap_server* s, usap_server_stats* out);
 
 /* --- allocation-free scoring (no counterpart in the reference) ----------- */
 /* The reference has no such entry point: it exists for callers that cannot

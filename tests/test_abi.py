@@ -107,3 +107,27 @@ def test_batch_rejects_bad_job_index():
     jobs[0].graph = 3
     rc = nat.lib().usap_batch_partition(garr, 1, None, jobs, 1, 0, 0, C.byref(nat.BatchStats()))
     assert rc == -1
+
+
+def test_server_null_and_no_device():
+    """The service's entry points reject null handles, and without a GPU
+    usap_server_create reports the missing device instead of crashing."""
+    L = nat.lib()
+    assert L.usap_server_submit(None, None, None, None, None) == -1
+    done = C.c_int32()
+    assert L.usap_server_poll(None, 1, C.byref(done), None, None) == -1
+    assert L.usap_server_wait(None, 1, None, None) == -1
+    assert L.usap_server_get_stats(None, None) == -1
+    L.usap_server_destroy(None)
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return
+    except ImportError:
+        pass
+    h = C.c_void_p()
+    cfg = nat.ServerConfig()
+    L.usap_server_config_default(C.byref(cfg))
+    rc = L.usap_server_create(C.byref(cfg), C.byref(h))
+    assert rc in (-5, -2) and not h.value
+    assert L.usap_last_error()

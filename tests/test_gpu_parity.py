@@ -229,6 +229,21 @@ def test_persistent_phase_exact(api, oracle, graph, params):
             assert res[k] == res_o[k], k
 
 
+def test_persistent_cta_cap_same_result(api):
+    """Fewer CTAs in the cooperative kernel (more work units per warp, more
+    hubs per CTA) give the same solve."""
+    from usap_b200 import native as nat
+    n, src, dst, w = GRAPHS["hub"]()
+    ctx = api.Context(0)
+    ctx.load(src, dst, w, n)
+    base = nat.default_params(num_batch_nodal_update=10, seed=9)
+    part0, res0 = ctx.partition(base)
+    for ctas in (1, 3, 16):
+        part, res = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=9, persistent_ctas=ctas))
+        assert np.array_equal(part, part0) and res["S_q"] == res0["S_q"], ctas
+    ctx.close()
+
+
 @pytest.mark.parametrize("within,alpha,seed", [(0.8, 10.0, 0), (0.5, 1.0, 1), (0.8, 1.0, 2),
                                                (0.5, 10.0, 3)])
 def test_c1_solve_exact(api, oracle, within, alpha, seed):

@@ -8,15 +8,16 @@ Public API (all GPU work goes through the C ABI in include/usap.h):
 * ``batch_partition``  many graphs x chains at once on one GPU
 * ``evaluate``    bf::evaluate's scores, returned as a dict
 * ``Context``     a graph resident in HBM, plus phase-level replay ops
+* ``Server``      a partition service: submit requests, collect by ticket
 * ``generator``   seeded DC-SBM graphs
 """
 from . import generator  # noqa: F401
 
-__all__ = ["Graph_P", "Context", "partition", "batch_partition", "evaluate", "generator"]
+__all__ = ["Graph_P", "Context", "Server", "partition", "batch_partition", "evaluate", "generator"]
 
 
 def __getattr__(name):
-    if name in ("Graph_P", "Context", "partition", "batch_partition", "evaluate"):
+    if name in ("Graph_P", "Context", "Server", "partition", "batch_partition", "evaluate"):
         from . import api
         return getattr(api, name)
     raise AttributeError(name)

@@ -176,6 +176,71 @@ def batch_partition(graphs, seeds_per_graph, params: Optional[nat.Params] = None
     return jobs, {f: getattr(st, f) for f, _ in nat.BatchStats._fields_}
 
 
+class Server:
+    """Partition service on one GPU (usap_server_*): submit requests at any
+    time, collect them by ticket.  Requests run concurrently on worker
+    threads with their own streams, admitted in arrival order as workers and
+    device memory (``memory_budget`` bytes, 0 = 80% of free) free up."""
+
+    def __init__(self, device: int = 0, workers: int = 0, memory_budget: int = 0):
+        cfg = nat.ServerConfig()
+        nat.lib().usap_server_config_default(C.byref(cfg))
+        cfg.device, cfg.workers, cfg.memory_budget = int(device), int(workers), int(memory_budget)
+        h = C.c_void_p()
+        nat.check(nat.lib().usap_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._out = {}
+
+    def submit(self, src, dst, weight=None, n: int = 0, one_based: bool = False,
+               params: Optional[nat.Params] = None) -> int:
+        g, keep = nat.make_graph(src, dst, weight, n, one_based)
+        nn = n if n > 0 else int(np.max(keep[0])) + (0 if one_based else 1)
+        out = np.empty(nn, np.int32)
+        p = params if params is not None else nat.default_params()
+        t = C.c_int64()
+        nat.check(nat.lib().usap_server_submit(self._h, C.byref(g), C.byref(p), nat.p32(out), C.byref(t)))
+        self._out[int(t.value)] = out
+        return int(t.value)
+
+    def _finish(self, ticket, rc, res, tm):
+        out = self._out.pop(ticket)
+        nat.check(rc)
+        timing = {f: getattr(tm, f) for f, _ in nat.ServerTiming._fields_}
+        return out, nat.result_dict(res), timing
+
+    def poll(self, ticket: int):
+        """None while the request runs, else (assign, result, timing)."""
+        done = C.c_int32()
+        res, tm = nat.Result(), nat.ServerTiming()
+        rc = nat.lib().usap_server_poll(self._h, int(ticket), C.byref(done), C.byref(res), C.byref(tm))
+        if rc == 0 and not done.value:
+            return None
+        if not done.value:
+            nat.check(rc)
+        return self._finish(int(ticket), rc, res, tm)
+
+    def wait(self, ticket: int):
+        res, tm = nat.Result(), nat.ServerTiming()
+        rc = nat.lib().usap_server_wait(self._h, int(ticket), C.byref(res), C.byref(tm))
+        return self._finish(int(ticket), rc, res, tm)
+
+    def stats(self) -> dict:
+        st = nat.ServerStats()
+        nat.check(nat.lib().usap_server_get_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in nat.ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            nat.lib().usap_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def evaluate(truth, given) -> dict:
     """bf::evaluate's scores (plus NMI) as a dict instead of printed lines."""
     t = np.ascontiguousarray(truth, np.int32)

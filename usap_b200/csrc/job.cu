@@ -850,8 +850,9 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
                               !trace_on(2)
                           ? nodal_phase_grid(device_)
                           : 0;
+    const int pctas = p.persistent_ctas > 0 ? std::min(pgrid, static_cast<int>(p.persistent_ctas)) : pgrid;
     if (pgrid > 0) {
-      const float ms = nodal_phase(part, B, stage, seed, W, thr, model_q, maxitr, stats, pgrid, stats != 0);
+      const float ms = nodal_phase(part, B, stage, seed, W, thr, model_q, maxitr, stats, pctas, stats != 0);
       d2h += sizeof(NodalCtl);
       if (stats) {
         res->ms_nodal_kernel += ms;

@@ -1296,9 +1296,12 @@ void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const Stre
   const int count = a.end - a.beg;
   if (count <= 0) return;
   const bool has_hubs = hubs.hi > hubs.lo;
-  if (has_hubs) {
+  const bool fork = has_hubs && sp.side != sp.main;   // hubs overlap the warp kernel on the side stream
+  if (fork) {
     USAP_CUDA(cudaEventRecord(sp.fork, sp.main));
     USAP_CUDA(cudaStreamWaitEvent(sp.side, sp.fork, 0));
+  }
+  if (has_hubs) {
     const size_t smem = sizeof(int) * 3 * static_cast<size_t>(hubs.smem_cap);
     k_nodal_propose_hub<Ops><<<hubs.hi - hubs.lo, kHubThreads, smem, sp.side>>>(a, ops, hubs.ids, hubs.lo,
                                                                                 hubs.hi, hubs.smem_cap);
@@ -1308,7 +1311,7 @@ void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const Stre
   if (blocks > 148 * 8) blocks = 148 * 8;
   k_nodal_propose<Ops><<<blocks, kThreads, 0, sp.main>>>(a, ops);
   USAP_LAUNCHED();
-  if (has_hubs) {
+  if (fork) {
     USAP_CUDA(cudaEventRecord(sp.join, sp.side));
     USAP_CUDA(cudaStreamWaitEvent(sp.main, sp.join, 0));
   }

@@ -43,7 +43,8 @@ class Params(C.Structure):
                 ("dfs_depth", C.c_int32), ("t_block_num", C.c_int32), ("seed", C.c_uint64),
                 ("init_mode", C.c_int32), ("dense_max", C.c_int32), ("device", C.c_int32),
                 ("stats", C.c_int32), ("trace_kinds", C.c_int32), ("sweep_graphs", C.c_int32),
-                ("persistent", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("persistent", C.c_int32), ("persistent_ctas", C.c_int32),
+                ("reserved", C.c_int32 * 2)]
 
 
 class Result(C.Structure):
@@ -87,12 +88,30 @@ class BatchStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_load", C.c_double), ("workers", C.c_int32),
                 ("kernel_launches", C.c_int64)]
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("workers", C.c_int32), ("memory_budget", C.c_int64),
+                ("reserved", C.c_int32 * 4)]
+
+
+class ServerTiming(C.Structure):
+    _fields_ = [("ms_queued", C.c_double), ("ms_running", C.c_double), ("ms_latency", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("queued", C.c_int32), ("running", C.c_int32), ("workers", C.c_int32),
+                ("peak_running", C.c_int32), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("admitted_bytes", C.c_int64), ("peak_admitted_bytes", C.c_int64),
+                ("memory_budget", C.c_int64)]
+
+
 # every exported symbol of include/usap.h
 EXPORTS = ("usap_version", "usap_last_error", "usap_params_default", "usap_partition",
            "usap_evaluate", "usap_ctx_create", "usap_ctx_destroy", "usap_ctx_load",
            "usap_ctx_num_nodes", "usap_ctx_partition", "usap_ctx_set_trace", "usap_op_scc",
            "usap_op_build", "usap_op_entropy", "usap_op_merge_phase", "usap_op_merge_apply",
-           "usap_op_nodal_batch", "usap_batch_partition", "usap_entropy_static")
+           "usap_op_nodal_batch", "usap_batch_partition", "usap_entropy_static",
+           "usap_server_config_default", "usap_server_create", "usap_server_destroy",
+           "usap_server_submit", "usap_server_poll", "usap_server_wait", "usap_server_get_stats")
 
 _lib = None
 
@@ -133,10 +152,20 @@ def lib() -> C.CDLL:
                                        C.POINTER(BatchStats)]
     L.usap_entropy_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32,
                                       C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+    L.usap_server_config_default.argtypes = [C.POINTER(ServerConfig)]
+    L.usap_server_config_default.restype = None
+    L.usap_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]
+    L.usap_server_destroy.argtypes = [C.c_void_p]
+    L.usap_server_destroy.restype = None
+    L.usap_server_submit.argtypes = [C.c_void_p, C.POINTER(Graph), C.POINTER(Params), i32p, i64p]
+    L.usap_server_poll.argtypes = [C.c_void_p, C.c_int64, i32p, C.POINTER(Result), C.POINTER(ServerTiming)]
+    L.usap_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Result), C.POINTER(ServerTiming)]
+    L.usap_server_get_stats.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
     for name in EXPORTS:
         fn = getattr(L, name)
         if name.startswith("usap_") and name not in ("usap_version", "usap_last_error",
-                                                     "usap_params_default"):
+                                                     "usap_params_default", "usap_server_config_default",
+                                                     "usap_server_destroy"):
             fn.restype = C.c_int32
     _lib = L
     return L

@@ -28,6 +28,12 @@ cpu_baseline  the reference's own partition() (compiled from its sources
        against the Taskflow-API shim, oracle/_ref/ref_main) on the same
        graph with all host threads, one full solve.
 
+batched  64 graphs x 4 chains through usap_batch_partition vs one at a time;
+served  a bounded sample of the served workload: Poisson arrivals (50/s) of
+       requests with N log-uniform in [1000, 200000] submitted to usap_server,
+       p50/p99 latency (submit to finish) and graphs/s, beside the same
+       requests solved one at a time.
+
 --impl reference times that reference binary alone (rank 0), K full solves.
 """
 from __future__ import annotations
@@ -194,6 +200,61 @@ def batched_vs_plain(local_rank: int, chains: int = 4):
             "mean_nmi": float(np.mean(nmi)), "plain_mean_nmi": float(np.mean(nmi)) if same else None}
 
 
+def served_sample(local_rank: int, jobs: int = 240, rate: float = 50.0, pool: int = 12,
+                  plain_jobs: int = 48, seed: int = 0):
+    """The served workload, bounded: `jobs` requests arriving as a Poisson
+    stream of `rate` per second, each a graph drawn from a pool of `pool`
+    seeded graphs with N log-uniform in [1000, 200000] (a distinct Philox
+    seed per request), submitted to usap_server at their arrival times.
+    Latency is measured by the service from submit to finish.  Beside it,
+    `plain_jobs` of the same requests solved one after another through
+    usap_partition."""
+    import numpy as np
+    from usap_b200 import api, generator as gen, native as nat
+    graphs = [gen.generate(c) for c in gen.config_c4(seed=seed, graphs=pool)]
+    rng = np.random.default_rng(seed + 1)
+    picks = rng.integers(0, pool, jobs)
+    gaps = rng.exponential(1.0 / rate, jobs)
+    srv = api.Server(device=local_rank)
+    warm = graphs[int(np.argmin([g.n for g in graphs]))]
+    srv.wait(srv.submit(warm.src, warm.dst, None, warm.n))
+    tickets = []
+    t0 = time.perf_counter()
+    t_next = t0
+    for k in range(jobs):
+        t_next += gaps[k]
+        d = t_next - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        G = graphs[picks[k]]
+        p = nat.default_params(num_batch_nodal_update=10, seed=1000 + k, device=local_rank)
+        tickets.append(srv.submit(G.src, G.dst, None, G.n, params=p))
+    lat, nmi = [], []
+    for k, t in enumerate(tickets):
+        part, res, timing = srv.wait(t)
+        lat.append(timing["ms_latency"])
+        nmi.append(api.evaluate(graphs[picks[k]].truth, part)["nmi"])
+    t_all = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    tp = time.perf_counter()
+    for k in range(plain_jobs):
+        G = graphs[picks[k]]
+        api.partition(G.src, G.dst, None, G.n,
+                      params=nat.default_params(num_batch_nodal_update=10, seed=1000 + k, device=local_rank))
+    t_plain = time.perf_counter() - tp
+    sizes = [graphs[i].n for i in picks]
+    return {"workload": f"{jobs} requests, Poisson {rate:g}/s, N log-uniform [1000, 200000] "
+                        f"(pool of {pool} graphs, largest N={max(g.n for g in graphs)}, "
+                        f"{max(g.num_edges for g in graphs)} edges)",
+            "jobs": jobs, "graphs_per_s": jobs / t_all, "offered_per_s": rate,
+            "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
+            "mean_nmi": float(np.mean(nmi)), "mean_n": float(np.mean(sizes)),
+            "plain_graphs_per_s": plain_jobs / t_plain, "plain_jobs": plain_jobs,
+            "workers": st["workers"], "peak_running": st["peak_running"],
+            "peak_admitted_mib": st["peak_admitted_bytes"] / 2**20}
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -339,6 +400,12 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             batched = batched_vs_plain(local_rank)
         except Exception as e:   # reported, not fatal
             batched = {"error": str(e)}
+    served = None
+    if rank == 0 and world == 1 and not args.no_served:
+        try:
+            served = served_sample(local_rank)
+        except Exception as e:   # reported, not fatal
+            served = {"error": str(e)}
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -359,6 +426,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "roofline": roofline,
         "cpu_baseline": cpu,
         "batched": batched,
+        "served": served,
         "clocks": clk,
         "mcmc_edge_visits_per_s": visits_per_s,
         "B": res["B"], "S": res["S"], "nmi": nmi, "sweeps": res["sweeps"], "stages": res["stages"],
@@ -378,6 +446,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched-vs-plain measurement of the 64-graph workload")
+    ap.add_argument("--no-served", action="store_true",
+                    help="skip the served-workload sample (Poisson arrivals, N up to 200k)")
     ap.add_argument("--profile", action="store_true",
                     help="one untimed solve of the workload (for ncu launch lists), no output")
     args = ap.parse_args()

@@ -230,3 +230,18 @@ def config_c3(seed: int = 0, graphs: int = 64):
                              alpha=float(rng.choice([1.0, 10.0])),
                              seed=int(rng.integers(0, 2**31 - 1))))
     return out
+
+
+def config_c4(seed: int = 0, graphs: int = 2000):
+    """Served workload: ``graphs`` requests with N log-uniform in
+    [1000, 200000] and the batched workload's other parameters (blocks
+    round(N^0.35), within-block fraction U[0.5, 0.8], alpha in {1, 10})."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(graphs):
+        n = int(round(np.exp(rng.uniform(np.log(1000), np.log(200000)))))
+        out.append(SBMConfig(n=n, blocks=max(1, int(round(n ** 0.35))),
+                             within=float(rng.uniform(0.5, 0.8)),
+                             alpha=float(rng.choice([1.0, 10.0])),
+                             seed=int(rng.integers(0, 2**31 - 1))))
+    return out

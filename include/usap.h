@@ -160,7 +160,9 @@ usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user);
 /* One job solves graphs[graph] with its own Philox seed (several jobs on the
  * same graph are independent chains).  Graphs are loaded once and shared.
  * Jobs run concurrently, each on its own stream driven by one of `workers`
- * host threads (0 = automatic); their kernels overlap on the GPU.  Every
+ * host threads (0 = automatic: 64); their kernels overlap on the GPU, and
+ * their dense nodal phases (B <= 4096) run together in cooperative "gang"
+ * launches that advance every waiting job by one batch a round.  Every
  * job's result equals the result of solving it alone with the same seed. */
 typedef struct usap_batch_job {
   int32_t graph;        /* index into graphs[] */
@@ -175,6 +177,9 @@ typedef struct usap_batch_stats {
   double ms_load;       /* loading the graphs */
   int32_t workers;
   int64_t kernel_launches;
+  int64_t gang_launches;  /* cooperative launches that ran several jobs' nodal phases */
+  int64_t gang_phases;    /* job nodal phases (or resumed parts of them) in those launches */
+  double ms_gang;         /* wall time of those launches */
 } usap_batch_stats;
 
 usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, const usap_params* p,

@@ -196,7 +196,12 @@ usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, cons
     auto t0 = std::chrono::steady_clock::now();
     int hw = static_cast<int>(std::thread::hardware_concurrency());
     if (hw <= 0) hw = 8;
-    int W = workers > 0 ? workers : std::min(32, 2 * hw);
+    // dense nodal phases of the concurrent solves run together in gang
+    // launches; solves mostly wait there, so more of them than host threads
+    std::unique_ptr<usap::NodalGang> gang;
+    USAP_CUDA(cudaSetDevice(device));
+    if (usap::nodal_gang_grid(device) > 0) gang = std::make_unique<usap::NodalGang>(device);
+    int W = workers > 0 ? workers : (gang ? usap::kGangMax : std::min(32, 2 * hw));
     W = std::max(1, std::min(W, std::max(njobs, ngraphs)));
     // load every graph once, in parallel
     std::vector<std::shared_ptr<usap::GraphResident>> res(ngraphs);
@@ -243,7 +248,13 @@ usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, cons
             bj.status = USAP_ERR_CUDA;
             continue;
           }
+          struct GangSeat {   // counts this solve as in progress for the gang
+            usap::NodalGang* g;
+            explicit GangSeat(usap::NodalGang* gg) : g(gg) { if (g) g->enter(); }
+            ~GangSeat() { if (g) g->leave(); }
+          } seat(gang.get());
           try {
+            job->set_gang(gang.get());
             job->attach(res[bj.graph]);
             usap_params prm = base;
             prm.persistent = 0;   // concurrent jobs: per-batch launches interleave
@@ -266,6 +277,9 @@ usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, cons
       stats->ms_load = std::chrono::duration<double, std::milli>(t1 - t0).count();
       stats->workers = W;
       stats->kernel_launches = launches.load();
+      stats->gang_launches = gang ? gang->launches() : 0;
+      stats->gang_phases = gang ? gang->phases() : 0;
+      stats->ms_gang = gang ? gang->ms() : 0.0;
     }
     for (int32_t j = 0; j < njobs; j++)
       if (jobs[j].status != USAP_OK) throw usap::Error(jobs[j].status, "a batch job failed");

@@ -145,6 +145,7 @@ struct NodalCtl {
   unsigned long long bar;   // arrivals (low 32 bits) + convergence flag (bit 32)
   int bar_err;
   unsigned int vnext;
+  int gang_batch;           // gang launches: next batch of the current sweep (0: a new sweep starts)
 };
 
 struct GraphDev {
@@ -219,6 +220,15 @@ struct PhaseArgs {
   int* ide_n;
 };
 
+// Control block of a gang launch (several jobs' nodal phases at once).
+constexpr int kGangMax = 64;
+struct GangCtl {
+  unsigned long long bar;   // grid barrier arrivals
+  int bar_err;
+  unsigned int vnext;       // work units handed out by the counter
+  int finished[kGangMax];   // 1: the job's nodal phase is complete; 0: resume it in a later launch
+};
+
 // --- launchers (kernels_*.cu) -------------------------------------------------
 void launch_dense_build(const GraphDev& g, const int32_t* part, int B, int ld, int* M, int* Mt,
                         cudaStream_t st);
@@ -241,9 +251,13 @@ void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int3
 void nodal_configure(int device);
 // grid of the persistent nodal kernel on `device` (0: not available)
 int nodal_phase_grid(int device);
+int nodal_gang_grid(int device);
 // largest B whose hub tables fit the persistent kernel's shared memory
 int nodal_phase_max_blocks();
 void launch_nodal_phase(const PhaseArgs& p, int grid, cudaStream_t st);
+// nodal phases of K <= kGangMax jobs (PhaseArgs array in device memory)
+// (the launch ends once fewer than exit_below jobs are unfinished)
+void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_below, int grid, cudaStream_t st);
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
                                 const StreamPair& sp);
 void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,

@@ -680,6 +680,12 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
   pa.model_q = model_q;
   pa.ide_q = ide_q_;
   pa.ide_n = ide_n_;
+  if (gang_ && !timed) {
+    gang_->run(pa, st_);
+    USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+    wait();
+    return 0.0f;
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (timed) {
     while (ev_pool_.size() < ev_used_ + 2) {
@@ -846,10 +852,9 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     const double thr = isf ? p.delta_entropy_threshold2 : p.delta_entropy_threshold1;
     const long long model_q = q32_host(model_S(n, hg_->e, B));
     trace_prev_moves_ = 0;
-    const int pgrid = p.persistent && dense && !use_graphs && maxitr > 0 && B <= nodal_phase_max_blocks() &&
-                              !trace_on(2)
-                          ? nodal_phase_grid(device_)
-                          : 0;
+    const bool phase_ok = dense && !use_graphs && maxitr > 0 && B <= nodal_phase_max_blocks() && !trace_on(2);
+    const bool in_gang = gang_ != nullptr && phase_ok && !stats;
+    const int pgrid = phase_ok && (p.persistent || in_gang) ? nodal_phase_grid(device_) : 0;
     const int pctas = p.persistent_ctas > 0 ? std::min(pgrid, static_cast<int>(p.persistent_ctas)) : pgrid;
     if (pgrid > 0) {
       const float ms = nodal_phase(part, B, stage, seed, W, thr, model_q, maxitr, stats, pctas, stats != 0);

@@ -2,6 +2,9 @@
 #pragma once
 
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
+#include <string>
 #include <cstdint>
 #include <vector>
 
@@ -77,6 +80,53 @@ struct GraphResident {
 // Graph_P constructor / load_graph_from_tsv (graph_parallel.hpp:251-317)
 std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in);
 
+// Runs the dense nodal phases of concurrent solves together in single
+// cooperative launches (k_nodal_gang); see gang.cpp.
+class NodalGang {
+ public:
+  explicit NodalGang(int device);
+  ~NodalGang();
+  NodalGang(const NodalGang&) = delete;
+  NodalGang& operator=(const NodalGang&) = delete;
+  // a solve starts / ends: a launch waits for every solve in progress to
+  // reach its nodal phase (or for kGangWait)
+  void enter();
+  void leave();
+  // runs this nodal phase in the next gang launch, after the work queued on
+  // job_stream; returns when it is done
+  void run(const PhaseArgs& pa, cudaStream_t job_stream);
+  long long launches() const { return launches_; }
+  long long phases() const { return jobs_run_; }
+  double ms() const { return ms_; }
+
+ private:
+  struct Pending {
+    PhaseArgs pa;
+    cudaEvent_t ready = nullptr;
+    std::chrono::steady_clock::time_point since;
+    bool done = false;
+    bool waited = false;
+    std::string error;
+  };
+  bool ready_to_launch() const;
+  void launch(const std::vector<Pending*>& batch);
+  int device_;
+  int grid_ = 0;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::vector<Pending*> pending_;
+  int live_ = 0;
+  bool busy_ = false;
+  cudaStream_t st_ = nullptr;
+  PhaseArgs* h_jobs_ = nullptr;
+  PhaseArgs* d_jobs_ = nullptr;
+  GangCtl* h_ctl_ = nullptr;
+  GangCtl* d_ctl_ = nullptr;
+  long long launches_ = 0, jobs_run_ = 0;
+  double ms_ = 0.0;
+  std::chrono::steady_clock::time_point last_end_{};
+};
+
 class Job {
  public:
   explicit Job(int device);
@@ -95,6 +145,8 @@ class Job {
   const std::shared_ptr<GraphResident>& graph() const { return gr_; }
   // host threads sleep (instead of spinning) while waiting for the device
   void set_blocking_wait(bool on) { blocking_wait_ = on; }
+  // dense nodal phases go to this gang instead of a launch of their own
+  void set_gang(NodalGang* g) { gang_ = g; }
   void set_trace(usap_trace_fn fn, void* user) {
     trace_ = fn;
     trace_user_ = user;
@@ -158,6 +210,7 @@ class Job {
   cudaEvent_t ev_sweep_[2] = {nullptr, nullptr};   // sweep done + control copied
   NodalCtl* h_ring_ = nullptr;                     // pinned, two control copies
   bool blocking_wait_ = false;
+  NodalGang* gang_ = nullptr;
   void wait();
   std::shared_ptr<GraphResident> gr_;
   const HostGraph* hg_ = nullptr;

@@ -905,6 +905,7 @@ struct LdPlain {
 struct DeltaTables {
   int *mkey, *mval, *ckey, *cval;
   int mlg, clg;   // capacities 1 << mlg, 1 << clg
+  int tag = 0;    // job number << 24 when the tables serve several jobs
 };
 
 __device__ __forceinline__ bool table_add(int* key, int* val, int lg, int k, int d) {
@@ -922,12 +923,12 @@ __device__ __forceinline__ bool table_add(int* key, int* val, int lg, int k, int
 }
 
 __device__ __forceinline__ void cs_add(const DeltaTables& t, int* CS, int key, int d) {
-  if (!table_add(t.ckey, t.cval, t.clg, key, d)) atomicAdd(CS + key, d);
+  if (!table_add(t.ckey, t.cval, t.clg, t.tag | key, d)) atomicAdd(CS + key, d);
 }
 
 __device__ __forceinline__ void tile_add(const DeltaTables& t, int* M, int* Mt, int* CS, int ld, int cld, int x,
                                          int y, int d) {
-  if (table_add(t.mkey, t.mval, t.mlg, x * ld + y, d)) return;
+  if (table_add(t.mkey, t.mval, t.mlg, t.tag | (x * ld + y), d)) return;
   atomicAdd(M + static_cast<long long>(x) * ld + y, d);
   atomicAdd(Mt + static_cast<long long>(y) * ld + x, d);
   cs_add(t, CS, x * cld + y / kChunk, d);
@@ -1124,7 +1125,8 @@ constexpr unsigned long long kBarDone = 1ull << 32;
 // every CTA then sees in the same load.  A wait gives up after
 // kBarrierTimeoutNs and sets bar_err.  Returns -1 on error (every CTA then
 // leaves at its next barrier), else 1 if kBarDone is set, else 0.
-__device__ __forceinline__ int grid_barrier(NodalCtl* ctl, unsigned* target, bool publish_done, int* s_state) {
+template <class CtlT>
+__device__ __forceinline__ int grid_barrier(CtlT* ctl, unsigned* target, bool publish_done, int* s_state) {
   *target += gridDim.x;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1290,6 +1292,263 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   if (p.a.stats && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
 }
 
+// --- gang of jobs: many nodal phases in one cooperative launch ---------------
+// first index j with pref[j + 1] > x (pref ascending, pref[0] = 0, x < pref[K])
+__device__ __forceinline__ int find_job(const long long* pref, int K, long long x) {
+  int lo = 0, hi = K;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pref[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// writes the deltas of the gang's jobs (key = job << 24 | index) to their
+// tiles (CTA-collective; tables cleared on the way)
+__device__ __forceinline__ void gang_tables_flush(const DeltaTables& t, const PhaseArgs* __restrict__ jobs) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < (1 << t.mlg); i += blockDim.x) {
+    const int k = t.mkey[i];
+    if (k < 0) continue;
+    const int d = t.mval[i];
+    t.mkey[i] = -1;
+    t.mval[i] = 0;
+    if (d == 0) continue;
+    const int j = k >> 24, idx = k & 0xffffff;
+    const PhaseArgs& p = jobs[j];
+    const int ld = p.v.ld, cld = p.v.cld;
+    const int x = idx / ld, y = idx - x * ld;
+    atomicAdd(p.M + static_cast<long long>(x) * ld + y, d);
+    atomicAdd(p.Mt + static_cast<long long>(y) * ld + x, d);
+    DeltaTables tj = t;
+    tj.tag = j << 24;
+    cs_add(tj, p.CS, x * cld + y / kChunk, d);
+    cs_add(tj, p.CS, y * cld + x / kChunk, d);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < (1 << t.clg); i += blockDim.x) {
+    const int k = t.ckey[i];
+    if (k < 0) continue;
+    const int d = t.cval[i];
+    t.ckey[i] = -1;
+    t.cval[i] = 0;
+    if (d) atomicAdd(jobs[k >> 24].CS + (k & 0xffffff), d);
+  }
+  __syncthreads();
+}
+
+// The nodal phases of K jobs (each at some stage of its own solve, dense
+// tile, B <= 4096) in one cooperative launch.  Every round advances each
+// unfinished job by one batch: jobs that start a sweep get their entropy
+// pass and sweep-start bookkeeping first; then the proposals of all jobs'
+// current batches (hubs one per CTA, then work units) share the grid, and
+// so do their apply passes, while one thread per job closes its batch.  A
+// job leaves the gang when its convergence test fires or its sweep budget
+// is spent; the launch ends with the last job.  The arithmetic per job is
+// that of k_nodal_phase (same device functions, same order of the integer
+// sums' terms is irrelevant), so each job's result equals its solo solve.
+__global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __restrict__ jobs, int K, GangCtl* gc,
+                                                             int exit_below) {
+  extern __shared__ int dyn[];
+  __shared__ CtaTally s_tally[kGangMax];
+  __shared__ HubShared<kPWarps> sh;
+  __shared__ int s_bi[kGangMax], s_sw[kGangMax], s_act[kGangMax], s_nb[kGangMax];
+  __shared__ long long s_hp[kGangMax + 1], s_up[kGangMax + 1], s_cp[kGangMax + 1];
+  __shared__ int s_base, s_state, s_flag;
+  using Ops = DenseOpsT<LdCG>;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int gw = blockIdx.x * kPWarps + wib;
+  const int nw = gridDim.x * kPWarps;
+  int* wtab = dyn + wib * kPWarpInts;
+  int* htab = dyn + kPWarps * kPWarpInts;
+  const DeltaTables dt{htab, htab + kPHubSlots, htab + 2 * kPHubSlots, htab + 2 * kPHubSlots + kPHubSlots / 2,
+                       kPHubLg, kPHubLg - 1};
+  unsigned target = 0;
+  unsigned long long unused_bytes = 0;
+  // a job may resume where an earlier launch left it: at batch gang_batch
+  // of the sweep it had started (ctl->sweeps counts started sweeps)
+  if (threadIdx.x < K) {
+    const PhaseArgs& p = jobs[threadIdx.x];
+    const int gb = __ldcg(&p.a.ctl->gang_batch);
+    const int started = static_cast<int>(__ldcg(&p.a.ctl->sweeps));
+    const int done = __ldcg(&p.a.ctl->done);
+    s_bi[threadIdx.x] = gb;
+    s_sw[threadIdx.x] = gb > 0 ? started - 1 : started;
+    s_act[threadIdx.x] = !done && s_sw[threadIdx.x] < p.maxitr ? 1 : 0;
+    s_nb[threadIdx.x] = (p.n + p.bs - 1) / p.bs;
+  }
+  __syncthreads();
+
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int any = 0, start = 0, count = 0;
+      for (int j = 0; j < K; j++) {
+        any |= s_act[j];
+        start |= s_act[j] && s_bi[j] == 0;
+        count += s_act[j];
+      }
+      s_flag = any | (start << 1) | (count << 2);
+    }
+    __syncthreads();
+    const int flag = s_flag;
+    if (!(flag & 1)) break;
+    if ((flag >> 2) < exit_below) break;   // enough jobs are done: the rest resume in the next launch
+    if (flag & 2) {
+      // data term of S for the jobs that start a sweep
+      if (threadIdx.x == 0) {
+        s_cp[0] = 0;
+        for (int j = 0; j < K; j++) {
+          const long long B = jobs[j].a.B;
+          s_cp[j + 1] = s_cp[j] + (s_act[j] && s_bi[j] == 0 ? B * B : 0);
+        }
+      }
+      __syncthreads();
+      const long long total = s_cp[K];
+      long long acc = 0;
+      int cj = -1;
+      for (long long c = static_cast<long long>(blockIdx.x) * kPThreads + threadIdx.x; c < total;
+           c += static_cast<long long>(gridDim.x) * kPThreads) {
+        const int j = find_job(s_cp, K, c);
+        if (j != cj) {
+          if (cj >= 0 && acc) atomicAdd(&jobs[cj].a.ctl->entropy_acc, static_cast<unsigned long long>(acc));
+          acc = 0;
+          cj = j;
+        }
+        const PhaseArgs& p = jobs[j];
+        const long long cc = c - s_cp[j];
+        const int B = p.a.B;
+        const int i = static_cast<int>(cc / B), jj = static_cast<int>(cc - static_cast<long long>(i) * B);
+        const int m = __ldcg(p.v.M + static_cast<long long>(i) * p.v.ld + jj);
+        if (m) acc += q32(g_term(p.a.L, m, __ldcg(p.din + jj), __ldcg(p.dout + i)));
+      }
+      if (cj >= 0 && acc) atomicAdd(&jobs[cj].a.ctl->entropy_acc, static_cast<unsigned long long>(acc));
+      if (grid_barrier(gc, &target, false, &s_state) < 0) return;
+      if (blockIdx.x == 0 && threadIdx.x < K && s_act[threadIdx.x] && s_bi[threadIdx.x] == 0) {
+        const PhaseArgs& p = jobs[threadIdx.x];
+        ctl_sweep_start(p.a.ctl, p.model_q, p.W, p.ide_q, p.ide_n);
+        p.a.ctl->entropy_acc = 0;
+      }
+      if (grid_barrier(gc, &target, false, &s_state) < 0) return;
+    }
+    // proposals of every unfinished job's current batch
+    if (threadIdx.x < K) s_tally[threadIdx.x] = CtaTally{0, 0, 0, 0};
+    if (threadIdx.x == 0) {
+      s_hp[0] = s_up[0] = 0;
+      for (int j = 0; j < K; j++) {
+        const PhaseArgs& p = jobs[j];
+        const int b = s_bi[j];
+        const bool on = s_act[j];
+        s_hp[j + 1] = s_hp[j] + (on ? __ldg(p.batch_hub + b + 1) - __ldg(p.batch_hub + b) : 0);
+        s_up[j + 1] = s_up[j] + (on ? __ldg(p.unit_ptr + b + 1) - __ldg(p.unit_ptr + b) : 0);
+      }
+    }
+    __syncthreads();
+    const int H = static_cast<int>(s_hp[K]);
+    const int U = static_cast<int>(s_up[K]);
+    for (int h = blockIdx.x; h < H; h += gridDim.x) {
+      const int j = find_job(s_hp, K, h);
+      const PhaseArgs& p = jobs[j];
+      const int v = __ldg(p.hubs + __ldg(p.batch_hub + s_bi[j]) + (h - static_cast<int>(s_hp[j])));
+      hub_vertex<Ops, kPThreads>(p.a, Ops{p.v, p.a.B}, v, static_cast<uint32_t>(s_sw[j]), htab, kPHubSlots, &sh,
+                                 &unused_bytes);
+    }
+    auto run_unit = [&](int u) {
+      const int j = find_job(s_up, K, u);
+      const PhaseArgs& p = jobs[j];
+      const int2 un = __ldg(p.units + __ldg(p.unit_ptr + s_bi[j]) + (u - static_cast<int>(s_up[j])));
+      const Ops ops{p.v, p.a.B};
+      const uint32_t itr = static_cast<uint32_t>(s_sw[j]);
+      if (un.y == kUnitWarp) {
+        group_vertex(p.a, ops, un.x, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap, &s_tally[j],
+                     Grp<32>(lane), &unused_bytes);
+      } else {
+        const int hh = lane >> 4;
+        const int vv = hh ? un.y : un.x;
+        if (vv >= 0)
+          group_vertex(p.a, ops, vv, itr, wtab + hh * (kHCap / 2), wtab + kHCap + hh * (kHCap / 2),
+                       wtab + 2 * kHCap + hh * (kHCap / 2), wtab + 3 * kHCap + hh * (kHubDegree / 2), &s_tally[j],
+                       Grp<16>(lane), &unused_bytes);
+      }
+    };
+    const int hcta = min(H, static_cast<int>(gridDim.x));
+    const int first = (gridDim.x - hcta) * kPWarps;
+    if (static_cast<int>(blockIdx.x) >= hcta) {
+      const int i = (blockIdx.x - hcta) * kPWarps + wib;
+      if (i < U) run_unit(i);
+    }
+    for (;;) {
+      __syncthreads();
+      if (threadIdx.x == 0) s_base = first + static_cast<int>(atomicAdd(&gc->vnext, static_cast<unsigned>(kPWarps)));
+      __syncthreads();
+      const int i0 = s_base;
+      if (i0 >= U) break;
+      if (i0 + wib < U) run_unit(i0 + wib);
+    }
+    __syncthreads();
+    if (threadIdx.x < K && s_act[threadIdx.x]) tally_flush(&s_tally[threadIdx.x], jobs[threadIdx.x].a.ctl);
+    if (grid_barrier(gc, &target, false, &s_state) < 0) return;
+    // apply + commit of every job's batch; one thread per job closes it
+    if (blockIdx.x == 0) {
+      if (threadIdx.x < K && s_act[threadIdx.x]) {
+        const PhaseArgs& p = jobs[threadIdx.x];
+        const int beg = s_bi[threadIdx.x] * p.bs, end = min(p.n, beg + p.bs);
+        const long long edges = (static_cast<long long>(__ldg(p.a.out_ptr + end)) - __ldg(p.a.out_ptr + beg)) +
+                                (static_cast<long long>(__ldg(p.a.in_ptr + end)) - __ldg(p.a.in_ptr + beg));
+        const CtlArgs ca{1, p.W, p.thr, p.ide_q, p.ide_n, end - beg, edges};
+        ctl_batch_end(p.a.ctl, ca);
+      }
+      if (threadIdx.x == 0) gc->vnext = 0;
+    }
+    if (threadIdx.x == 0) {
+      s_cp[0] = 0;
+      for (int j = 0; j < K; j++) {
+        const PhaseArgs& p = jobs[j];
+        long long c = 0;
+        if (s_act[j]) {
+          const int beg = s_bi[j] * p.bs, end = min(p.n, beg + p.bs);
+          c = __ldg(p.chunk_ptr + end) - __ldg(p.chunk_ptr + beg);
+        }
+        s_cp[j + 1] = s_cp[j] + c;
+      }
+    }
+    tables_clear(dt);
+    __syncthreads();
+    const long long C = s_cp[K];
+    for (long long q = gw; q < C; q += nw) {
+      const int j = find_job(s_cp, K, q);
+      const PhaseArgs& p = jobs[j];
+      const int beg = s_bi[j] * p.bs, end = min(p.n, beg + p.bs);
+      const int2 ch = __ldg(p.g.chunks + __ldg(p.chunk_ptr + beg) + (q - s_cp[j]));
+      DeltaTables tj = dt;
+      tj.tag = j << 24;
+      apply_chunk<LdCG, LdCG>(ch, p.g, p.part, p.a.move_to, p.a.from, beg, end, tj, p.v.ld, p.M, p.Mt, p.v.cld,
+                              p.CS, p.dout, p.din, lane);
+    }
+    gang_tables_flush(dt, jobs);
+    if (grid_barrier(gc, &target, false, &s_state) < 0) return;
+    // advance every job by one batch
+    if (threadIdx.x < K && s_act[threadIdx.x]) {
+      const int j = threadIdx.x;
+      const PhaseArgs& p = jobs[j];
+      const int done = *reinterpret_cast<volatile int*>(&p.a.ctl->done);
+      if (++s_bi[j] == s_nb[j]) {
+        s_bi[j] = 0;
+        s_sw[j]++;
+      }
+      if (done || s_sw[j] >= p.maxitr) s_act[j] = 0;
+    }
+  }
+  // where each job stands: finished, or the batch to resume at
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x < K) {
+    const int j = threadIdx.x;
+    gc->finished[j] = s_act[j] ? 0 : 1;
+    jobs[j].a.ctl->gang_batch = s_act[j] ? s_bi[j] : 0;
+  }
+}
+
 // the hub CTAs run on a second stream, concurrently with the warp kernel
 template <class Ops>
 void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const StreamPair& sp) {
@@ -1321,6 +1580,7 @@ void launch_propose(const NodalArgs& a, Ops ops, const HubList& hubs, const Stre
 
 namespace {
 int g_phase_grid[64];
+int g_gang_grid[64];
 }
 
 // dynamic shared memory limits, set once per device, and the grid of the
@@ -1337,11 +1597,16 @@ void nodal_configure(int device) {
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     USAP_CUDA(cudaFuncSetAttribute(k_nodal_phase, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(kPSmemBytes)));
+    USAP_CUDA(cudaFuncSetAttribute(k_nodal_gang, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(kPSmemBytes)));
     int coop = 0, sms = 0, per_sm = 0;
     USAP_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
     USAP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nodal_phase, kPThreads, kPSmemBytes));
     g_phase_grid[device] = coop ? per_sm * sms : 0;
+    int per_sm_g = 0;
+    USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g, k_nodal_gang, kPThreads, kPSmemBytes));
+    g_gang_grid[device] = coop ? per_sm_g * sms : 0;
   });
 }
 
@@ -1351,7 +1616,24 @@ int nodal_phase_grid(int device) {
   return g_phase_grid[device];
 }
 
+int nodal_gang_grid(int device) {
+  if (device < 0 || device >= 64) return 0;
+  nodal_configure(device);
+  return g_gang_grid[device];
+}
+
 int nodal_phase_max_blocks() { return 2 * kPHubSlots / 4; }
+
+void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_below, int grid, cudaStream_t st) {
+  const PhaseArgs* j = jobs_dev;
+  int k = K;
+  GangCtl* c = gc;
+  int e = exit_below;
+  void* kargs[] = {&j, &k, &c, &e};
+  USAP_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_nodal_gang), dim3(grid), dim3(kPThreads),
+                                        kargs, kPSmemBytes, st));
+  USAP_LAUNCHED();
+}
 
 void launch_nodal_phase(const PhaseArgs& p, int grid, cudaStream_t st) {
   PhaseArgs args = p;

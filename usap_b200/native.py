@@ -86,7 +86,8 @@ class BatchJob(C.Structure):
 
 class BatchStats(C.Structure):
     _fields_ = [("ms_total", C.c_double), ("ms_load", C.c_double), ("workers", C.c_int32),
-                ("kernel_launches", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("gang_launches", C.c_int64), ("gang_phases", C.c_int64),
+                ("ms_gang", C.c_double)]
 
 class ServerConfig(C.Structure):
     _fields_ = [("device", C.c_int32), ("workers", C.c_int32), ("memory_budget", C.c_int64),

@@ -288,18 +288,36 @@ def run_reference_arm(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def dist_init(world: int, local_rank: int, backend: str = "nccl"):
+    """One process per GPU: the process group (None on one GPU), with a short
+    timeout so that ranks waiting on a lost peer end with an error."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    kw = {"device_id": torch.device("cuda", local_rank)} if backend == "nccl" else {}
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+    return dist
+
+
+def ranks_max(x: float, dist, device: str = "cuda") -> float:
+    """The largest value over all ranks (x itself on one GPU)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import numpy as np
     import torch
     from usap_b200 import api, native as nat
 
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local_rank))
+    dist = dist_init(world, local_rank)
     G = graph_for(rank)
     ctx = api.Context(local_rank)
     ctx.load(G.src, G.dst, None, G.n)
@@ -330,11 +348,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         results.append(res)
     barrier()
     clk = clocks.stop()
-    total_ms = float(sum(step_ms))
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = ranks_max(float(sum(step_ms)), dist)
     value = total_ms / args.steps / 1000.0
     res = results[-1]
     launches = int(sum(r["kernel_launches"] for r in results))
@@ -356,11 +370,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         e1.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
     barrier()
-    e2e_total = float(sum(e2e_ms))
-    if dist is not None:
-        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = ranks_max(float(sum(e2e_ms)), dist)
     e2e_value = e2e_total / args.steps / 1000.0
     nmi = api.evaluate(G.truth, part)["nmi"]
 

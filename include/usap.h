@@ -86,8 +86,8 @@ typedef struct usap_params {
 typedef struct usap_result {
   int32_t B;               /* number of blocks of the returned partition */
   int32_t stages;          /* merge + nodal phases run */
-  double S;                /* description length of the result */
-  int64_t S_q;             /* the same in Q32 fixed point (exact) */
+  double S;                /* description length of the result: model term + data term */
+  int64_t S_q;             /* the same in Q32 fixed point, saturated beyond +-2^31 */
   int64_t sweeps, batches;
   int64_t nodal_proposals, nodal_moves;
   int64_t near_threshold;  /* nodal proposals with |dS| <= 1e-9 */
@@ -118,7 +118,8 @@ typedef struct usap_scores {
  * with checksums of the partition, of M's non-zeros and of the degrees. */
 typedef struct usap_trace_event {
   int32_t kind, stage, itr, batch_beg, B;
-  int64_t S_q;
+  int64_t S_q;     /* kind 2: data term of the running S (Q32; S = model term + S_q / 2^32);
+                      kind 3: S in Q32, saturated beyond +-2^31 */
   int32_t S_ninf;
   int64_t cum_q;
   int32_t cum_ninf;
@@ -192,7 +193,8 @@ usap_status usap_op_scc(usap_ctx* ctx, int32_t dfs_depth, int32_t* part, int32_t
 /* _initialize_edge_counts (:703-759): M (B*B row-major, may be NULL) and degrees */
 usap_status usap_op_build(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t dense_max,
                           int32_t* M, int32_t* dout, int32_t* din);
-/* _compute_overall_entropy (:1281-1319), Q32 */
+/* _compute_overall_entropy (:1281-1319), Q32, saturated beyond +-2^31 (reached
+ * when B is near N: the model term grows like B^2 log(B^2/E)) */
 usap_status usap_op_entropy(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t dense_max,
                             int64_t* S_q);
 /* block_merge task (:349-368): K proposals per block; prop_* may be NULL */

@@ -57,7 +57,7 @@ class OgTraceEvent(C.Structure):
 
 
 class OgResult(C.Structure):
-    _fields_ = [("B", C.c_int32), ("S_q", C.c_int64), ("stages", C.c_int32),
+    _fields_ = [("B", C.c_int32), ("S_q", C.c_int64), ("S", C.c_double), ("stages", C.c_int32),
                 ("sweeps", C.c_int64), ("batches", C.c_int64),
                 ("nodal_proposals", C.c_int64), ("nodal_moves", C.c_int64),
                 ("near_threshold", C.c_int64), ("merge_shortfall", C.c_int64)]
@@ -73,7 +73,8 @@ class OgScores(C.Structure):
 
 
 class OgGPoint(C.Structure):
-    _fields_ = [("B", C.c_int32), ("S", C.c_int64), ("finite", C.c_int32), ("slot", C.c_int32)]
+    _fields_ = [("B", C.c_int32), ("S", C.c_double), ("S_q", C.c_int64), ("finite", C.c_int32),
+                ("slot", C.c_int32)]
 
 
 class OgGolden(C.Structure):
@@ -132,7 +133,7 @@ def lib() -> C.CDLL:
                                      i32p, i64p, i32p, i64p]
         L.og_nodal_batch.restype = C.c_int64
         L.og_golden_init.argtypes = [C.POINTER(OgGolden)]
-        L.og_golden_step.argtypes = [C.POINTER(OgGolden), C.c_int32, C.c_int64, C.c_int32,
+        L.og_golden_step.argtypes = [C.POINTER(OgGolden), C.c_int32, C.c_double, C.c_int64, C.c_int32,
                                      C.c_float, i32p, i32p, i32p]
         L.og_golden_step.restype = C.c_int
         L.og_params_default.argtypes = [C.POINTER(OgParams)]
@@ -315,7 +316,7 @@ def golden_sequence(seq, rate: float = 0.5):
         restore = C.c_int32(-1)
         btm = C.c_int32(0)
         freed = C.c_int32(-1)
-        done = lib().og_golden_step(C.byref(gs), int(B), quantize(float(S)), slot, rate,
+        done = lib().og_golden_step(C.byref(gs), int(B), float(S), quantize(float(S)), slot, rate,
                                     C.byref(restore), C.byref(btm), C.byref(freed))
         if done:
             nextB = gs.med.B

@@ -252,7 +252,20 @@ void og_build(const og_graph* g, const int32_t* part, og_blocks* b) {
 /* Entropy terms.  The reference writes each as x*log(x/(a*b)) with x an
  * interblock count and a, b block degrees.  Here log is read from the
  * integer log table and every term is quantised to Q32 on its own.        */
-int64_t og_quantize(double t) { return llrint(t * OG_Q32_SCALE); }
+int64_t og_quantize(double t) {
+  double x = t * OG_Q32_SCALE;
+  if (x >= 9223372036854775807.0) return INT64_MAX;
+  if (x <= -9223372036854775807.0) return INT64_MIN;
+  return llrint(x);
+}
+
+int64_t og_add_sat(int64_t a, int64_t b) {
+  int64_t r;
+  if (__builtin_add_overflow(a, b, &r)) return a > 0 ? INT64_MAX : INT64_MIN;
+  return r;
+}
+
+double og_desc_length(double model, int64_t data_q) { return model + (double)data_q / OG_Q32_SCALE; }
 
 static inline double og_g(const double* L, int64_t x, int64_t din_arg, int64_t dout_arg) {
   if (x == 0) return 0.0;
@@ -279,7 +292,7 @@ double og_model_S(int64_t n, int64_t e, int32_t B) {
 }
 
 /* S = model + data, data = -sum M log(M/(dout*din)) (:1281-1319) */
-int64_t og_entropy_q(const og_graph* g, const og_blocks* b) {
+int64_t og_data_q(const og_graph* g, const og_blocks* b) {
   const double* L = g->logk;
   int32_t B = b->B;
   int64_t data = 0;
@@ -288,7 +301,12 @@ int64_t og_entropy_q(const og_graph* g, const og_blocks* b) {
       int64_t m = b->M[(size_t)i * B + j];
       if (m != 0) data += og_quantize(og_g(L, m, b->din[j], b->dout[i]));
     }
-  return -data + og_quantize(og_model_S(g->n, g->e, B));
+  return -data;
+}
+
+/* S in Q32: model term (saturated) + data term, saturated */
+int64_t og_entropy_q(const og_graph* g, const og_blocks* b) {
+  return og_add_sat(og_quantize(og_model_S(g->n, g->e, b->B)), og_data_q(g, b));
 }
 
 /* ------------------------------------------------------------------------ */
@@ -655,9 +673,9 @@ void og_golden_init(og_golden* gs) { memset(gs, 0, sizeof(*gs)); }
  * keeps it), *btm the merges to do next, and *free_slot a buffer no longer
  * referenced by the bracket.  Returns 1 when the search is over (the answer
  * is gs->med).                                                             */
-int og_golden_step(og_golden* gs, int32_t B, int64_t S, int32_t cur_slot, float rate,
+int og_golden_step(og_golden* gs, int32_t B, double S, int64_t S_q, int32_t cur_slot, float rate,
                    int32_t* restore_slot, int32_t* btm, int32_t* free_slot) {
-  og_gpoint cur = {B, S, 1, cur_slot};
+  og_gpoint cur = {B, S, S_q, 1, cur_slot};
   og_gpoint* med = &gs->med;
   int32_t freed;
   if (!med->finite || cur.S <= med->S) {
@@ -753,8 +771,9 @@ int og_partition(const og_graph* g, const og_params* p, int32_t* part_out,
     int isf = gs.large.finite && gs.med.finite && gs.small.finite;
     double thr = isf ? p->delta_entropy_threshold2 : p->delta_entropy_threshold1;
     int converged = 0;
+    const double model = og_model_S(n, g->e, B);
     for (int32_t itr = 0; itr < maxitr && !converged; itr++) {
-      int64_t S_q = og_entropy_q(g, &blk);
+      int64_t S_q = og_data_q(g, &blk);   /* data term; S = model + S_q / 2^32 */
       int32_t S_n = 0;
       double mean = 0.0;
       if (itr >= W - 1) {
@@ -782,25 +801,28 @@ int og_partition(const og_graph* g, const og_params* p, int32_t* part_out,
         ev.S_q = S_q; ev.S_ninf = S_n; ev.cum_q = cum_q; ev.cum_ninf = cum_n; ev.moves = mv;
         og_emit(trace, user, &ev, g, part, &blk);
         if (itr >= W - 1) {
-          double S_d = S_n ? -INFINITY : (double)S_q / OG_Q32_SCALE;
+          double S_d = S_n ? -INFINITY : og_desc_length(model, S_q);
           if (-mean < thr * S_d) { converged = 1; break; }
         }
       }
     }
-    int64_t S_fin = og_entropy_q(g, &blk);
+    const int64_t data_fin = og_data_q(g, &blk);
+    const double S_fin = og_desc_length(model, data_fin);
+    const int64_t S_fin_q = og_add_sat(og_quantize(model), data_fin);
     memset(&ev, 0, sizeof(ev));
-    ev.kind = 3; ev.stage = stage; ev.B = B; ev.S_q = S_fin;
+    ev.kind = 3; ev.stage = stage; ev.B = B; ev.S_q = S_fin_q;
     og_emit(trace, user, &ev, g, part, &blk);
     res->stages++;
     stage++;
 
     int32_t restore = -1, freed = -1;
-    int done = og_golden_step(&gs, B, S_fin, work, p->num_block_reduction_rate, &restore,
+    int done = og_golden_step(&gs, B, S_fin, S_fin_q, work, p->num_block_reduction_rate, &restore,
                               &btm, &freed);
     if (done) {
       memcpy(part_out, slots[gs.med.slot], pn);
       res->B = gs.med.B;
-      res->S_q = gs.med.S;
+      res->S_q = gs.med.S_q;
+      res->S = gs.med.S;
       break;
     }
     /* a buffer outside the bracket becomes the working state */

@@ -69,7 +69,8 @@ typedef struct {
   int32_t stage, itr;
   int32_t batch_beg;
   int32_t B;
-  int64_t S_q;       /* running S (batch) or final S (stage end) */
+  int64_t S_q;       /* batch end: data term of the running S (Q32); stage end: S in
+                        Q32, saturated beyond +-2^31 */
   int32_t S_ninf;
   int64_t cum_q;
   int32_t cum_ninf;
@@ -81,7 +82,8 @@ typedef void (*og_trace_fn)(void* user, const og_trace_event* ev);
 
 typedef struct {
   int32_t B;
-  int64_t S_q;
+  int64_t S_q;       /* Q32, saturated beyond +-2^31 */
+  double S;          /* model term + data term */
   int32_t stages;
   int64_t sweeps, batches;
   int64_t nodal_proposals, nodal_moves, near_threshold, merge_shortfall;
@@ -110,7 +112,11 @@ int32_t og_scc(const og_graph* g, int32_t dfs_depth, int32_t* part);
 int og_blocks_alloc(og_blocks* b, int32_t B);
 void og_blocks_free(og_blocks* b);
 void og_build(const og_graph* g, const int32_t* part, og_blocks* b);
-int64_t og_quantize(double t);
+int64_t og_quantize(double t);   /* saturated to the int64 range */
+int64_t og_add_sat(int64_t a, int64_t b);
+/* description length = model term + data term: S = model + data_q / 2^32 */
+double og_desc_length(double model, int64_t data_q);
+int64_t og_data_q(const og_graph* g, const og_blocks* b);   /* -(sum of Q32 terms) */
 double og_model_S(int64_t n, int64_t e, int32_t B);
 int64_t og_entropy_q(const og_graph* g, const og_blocks* b);
 int64_t og_merge_dq(const og_graph* g, const og_blocks* b, int32_t r, int32_t s);
@@ -134,10 +140,10 @@ int64_t og_nodal_batch(const og_graph* g, int32_t* part, og_blocks* b, int32_t b
                        int64_t* cum_q, int32_t* cum_ninf, int64_t* near_threshold);
 
 /* --- golden-section search over B (host-side in the product) ------------- */
-typedef struct { int32_t B; int64_t S; int32_t finite; int32_t slot; } og_gpoint;
+typedef struct { int32_t B; double S; int64_t S_q; int32_t finite; int32_t slot; } og_gpoint;
 typedef struct { og_gpoint large, med, small; } og_golden;
 void og_golden_init(og_golden* gs);
-int og_golden_step(og_golden* gs, int32_t B, int64_t S, int32_t cur_slot, float rate,
+int og_golden_step(og_golden* gs, int32_t B, double S, int64_t S_q, int32_t cur_slot, float rate,
                    int32_t* restore_slot, int32_t* btm, int32_t* free_slot);
 
 /* --- whole solve ---------------------------------------------------------- */

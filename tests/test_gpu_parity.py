@@ -304,6 +304,23 @@ def test_c2_scale_properties(api):
     ctx.close()
 
 
+def test_identity_init_large_B(api):
+    """Starting from one block per vertex (N=50000), the first stages have a
+    description length above 2^31 in Q32 units (model term ~2e10): the solve
+    must still close its bracket on a small B with a consistent S."""
+    from usap_b200 import native as nat
+    G = gen.generate(gen.config_c2())
+    ctx = api.Context(0)
+    ctx.load(G.src, G.dst, None, G.n)
+    part, res = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=0, init_mode=1))
+    B = res["B"]
+    assert 1 <= B < 1000 and part.max() < B
+    assert res["S"] > 0 and res["S_q"] == ctx.op_entropy(part, B)
+    assert abs(res["S_q"] / 2**32 - res["S"]) < 1e-6 * res["S"]
+    assert api.evaluate(G.truth, part)["nmi"] > 0.3
+    ctx.close()
+
+
 def test_batch_equals_solo(api):
     """Every job of a concurrent batch (several graphs x chains, several
     workers) returns exactly the partition of solving it alone."""

@@ -103,6 +103,7 @@ struct CtlArgs {
   int active;
   int W;
   double thr;
+  double model_d;      // model term of S; the convergence test uses model_d + S_q / 2^32
   long long* ide_q;
   int* ide_n;
   long long batch_vertices, batch_edges;
@@ -128,7 +129,7 @@ struct NodalCtl {
   int S_ninf;
   int cum_ninf;
   int itr;           // index of the current sweep (set by the sweep-start kernel)
-  long long S_q;     // running description length (Q32)
+  long long S_q;     // data term of the running description length (Q32); S = model + S_q / 2^32
   unsigned long long cum_q;   // accepted dS of the current sweep (Q32, two's complement)
   unsigned long long moves;   // accepted moves (whole phase)
   unsigned long long near;    // proposals with |dS| <= 1e-9
@@ -215,7 +216,7 @@ struct PhaseArgs {
   const int64_t* chunk_ptr;
   int n, bs, maxitr, W;
   double thr;
-  long long model_q;
+  double model_d;           // model term of S for this stage's B
   long long* ide_q;
   int* ide_n;
 };
@@ -272,7 +273,7 @@ void launch_nodal_apply_commit_dense(const GraphDev& g, int32_t* part, const int
 void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int beg, int end,
                          int update_degrees, int32_t* dout, int32_t* din, NodalCtl* ctl,
                          const CtlArgs& c, cudaStream_t st);
-void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const long long* ide_q,
+void launch_ctl_sweep_start(NodalCtl* ctl, int W, const long long* ide_q,
                             const int* ide_n, cudaStream_t st);
 void launch_merge_sort_keys(int B, const long long* best_q, unsigned long long* keys, int32_t* idx,
                             cudaStream_t st);

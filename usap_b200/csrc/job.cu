@@ -8,6 +8,7 @@
 #include "job.h"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -71,11 +72,22 @@ double model_S(int64_t n, int64_t e, int32_t B) {
          static_cast<double>(n) * std::log(static_cast<double>(B));
 }
 
-long long q32_host(double t) { return std::llrint(t * 4294967296.0); }
+long long q32_host(double t) {
+  const double x = t * 4294967296.0;
+  if (x >= 9223372036854775807.0) return LLONG_MAX;
+  if (x <= -9223372036854775807.0) return LLONG_MIN;
+  return std::llrint(x);
+}
 
-bool Golden::step(int32_t B, int64_t S, int32_t cur_slot, float rate, int32_t* restore_slot,
+long long add_sat(long long a, long long b) {
+  long long r;
+  if (__builtin_add_overflow(a, b, &r)) return a > 0 ? LLONG_MAX : LLONG_MIN;
+  return r;
+}
+
+bool Golden::step(int32_t B, double S, int64_t S_q, int32_t cur_slot, float rate, int32_t* restore_slot,
                   int32_t* btm) {
-  GoldenPoint cur{B, S, true, cur_slot};
+  GoldenPoint cur{B, S, S_q, true, cur_slot};
   if (!med.finite || cur.S <= med.S) {
     if (med.B > cur.B) large = med;
     else small = med;
@@ -596,7 +608,7 @@ void Job::nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t
 }
 
 float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, int W, double thr,
-                       long long model_q, int32_t maxitr, int stats, int grid, bool timed) {
+                       double model_d, int32_t maxitr, int stats, int grid, bool timed) {
   const int32_t n = hg_->n;
   const int32_t nb = (n + bs_ - 1) / bs_;
   if (batch_hub_bs_ != bs_) {   // first hub of each batch, for this batch size
@@ -677,7 +689,7 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
   pa.maxitr = maxitr;
   pa.W = W;
   pa.thr = thr;
-  pa.model_q = model_q;
+  pa.model_d = model_d;
   pa.ide_q = ide_q_;
   pa.ide_n = ide_n_;
   if (gang_ && !timed) {
@@ -708,16 +720,16 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
 }
 
 void Job::enqueue_sweep(int32_t* part, int32_t B, bool dense, uint32_t stage, uint64_t seed, int W,
-                        double thr, long long model_q, int stats) {
+                        double thr, double model_d, int stats) {
   const int32_t n = hg_->n;
   if (!dense) sb_.build(g_, part, B, false, true, st_);
   entropy_launch(part, B, dense);
-  launch_ctl_sweep_start(ctl_, model_q, W, ide_q_, ide_n_, st_);
+  launch_ctl_sweep_start(ctl_, W, ide_q_, ide_n_, st_);
   for (int32_t beg = 0; beg < n; beg += bs_) {
     const int32_t end = beg + bs_ < n ? beg + bs_ : n;
     const long long edges = (static_cast<long long>(hg_->out_ptr[end]) - hg_->out_ptr[beg]) +
                             (static_cast<long long>(hg_->in_ptr[end]) - hg_->in_ptr[beg]);
-    const CtlArgs ca{1, W, thr, ide_q_, ide_n_, end - beg, edges};
+    const CtlArgs ca{1, W, thr, model_d, ide_q_, ide_n_, end - beg, edges};
     nodal_batch(part, B, dense, beg, end, stage, seed, beg == 0, stats, ca);
   }
 }
@@ -850,14 +862,14 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     USAP_CUDA(cudaMemsetAsync(ide_n_, 0, sizeof(int) * std::max(maxitr, 1), st_));
     const bool isf = gs.large.finite && gs.med.finite && gs.small.finite;
     const double thr = isf ? p.delta_entropy_threshold2 : p.delta_entropy_threshold1;
-    const long long model_q = q32_host(model_S(n, hg_->e, B));
+    const double model_d = model_S(n, hg_->e, B);
     trace_prev_moves_ = 0;
     const bool phase_ok = dense && !use_graphs && maxitr > 0 && B <= nodal_phase_max_blocks() && !trace_on(2);
     const bool in_gang = gang_ != nullptr && phase_ok && !stats;
     const int pgrid = phase_ok && (p.persistent || in_gang) ? nodal_phase_grid(device_) : 0;
     const int pctas = p.persistent_ctas > 0 ? std::min(pgrid, static_cast<int>(p.persistent_ctas)) : pgrid;
     if (pgrid > 0) {
-      const float ms = nodal_phase(part, B, stage, seed, W, thr, model_q, maxitr, stats, pctas, stats != 0);
+      const float ms = nodal_phase(part, B, stage, seed, W, thr, model_d, maxitr, stats, pctas, stats != 0);
       d2h += sizeof(NodalCtl);
       if (stats) {
         res->ms_nodal_kernel += ms;
@@ -873,7 +885,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       if (maxitr > 0 && use_graphs) {
         const LaunchCount before = launch_count();
         USAP_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-        enqueue_sweep(part, B, dense, stage, seed, W, thr, model_q, 0);
+        enqueue_sweep(part, B, dense, stage, seed, W, thr, model_d, 0);
         USAP_CUDA(cudaStreamEndCapture(st_, &graph));
         USAP_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         per_sweep.kernels = launch_count().kernels - before.kernels;
@@ -883,7 +895,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       const size_t ev_mark = ev_used_;
       auto launch_one = [&] {
         if (exec) USAP_CUDA(cudaGraphLaunch(exec, st_));
-        else enqueue_sweep(part, B, dense, stage, seed, W, thr, model_q, stats);
+        else enqueue_sweep(part, B, dense, stage, seed, W, thr, model_d, stats);
         USAP_CUDA(cudaMemcpyAsync(h_ring_ + (launched & 1), ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
         USAP_CUDA(cudaEventRecord(ev_sweep_[launched & 1], st_));
         launched++;
@@ -926,12 +938,12 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
         {
           if (!dense) sb_.build(g_, part, B, false, true, st_);
           entropy_launch(part, B, dense);
-          launch_ctl_sweep_start(ctl_, model_q, W, ide_q_, ide_n_, st_);
+          launch_ctl_sweep_start(ctl_, W, ide_q_, ide_n_, st_);
           for (int32_t beg = 0; beg < n; beg += bs_) {
             const int32_t end = beg + bs_ < n ? beg + bs_ : n;
             const long long edges = (static_cast<long long>(hg_->out_ptr[end]) - hg_->out_ptr[beg]) +
                                     (static_cast<long long>(hg_->in_ptr[end]) - hg_->in_ptr[beg]);
-            const CtlArgs ca{1, W, thr, ide_q_, ide_n_, end - beg, edges};
+            const CtlArgs ca{1, W, thr, model_d, ide_q_, ide_n_, end - beg, edges};
             nodal_batch(part, B, dense, beg, end, stage, seed, beg == 0, stats, ca);
             USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
             wait();
@@ -970,16 +982,18 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     entropy_launch(part, B, dense);
     USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
     wait();
-    const long long S_fin = model_q - static_cast<long long>(h_ctl_->entropy_acc);
+    const long long data_fin = -static_cast<long long>(h_ctl_->entropy_acc);
+    const double S_fin = desc_length(model_d, data_fin);
+    const long long S_fin_q = add_sat(q32_host(model_d), data_fin);
     d2h += sizeof(NodalCtl);
     auto tn1 = std::chrono::steady_clock::now();
     ms_nodal += std::chrono::duration<double, std::milli>(tn1 - tm1).count();
-    if (trace_on(3)) emit_trace(3, stage, 0, 0, B, part, dense, S_fin, 0, 0, 0, 0);
+    if (trace_on(3)) emit_trace(3, stage, 0, 0, B, part, dense, S_fin_q, 0, 0, 0, 0);
     res->stages++;
     stage++;
 
     int32_t restore = -1;
-    bool done = gs.step(B, S_fin, work, p.num_block_reduction_rate, &restore, &btm);
+    bool done = gs.step(B, S_fin, S_fin_q, work, p.num_block_reduction_rate, &restore, &btm);
     if (done) {
       auto td0 = std::chrono::steady_clock::now();
       if (out_assign)
@@ -990,8 +1004,8 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       res->ms_d2h = std::chrono::duration<double, std::milli>(td1 - td0).count();
       if (out_assign) d2h += static_cast<long long>(sizeof(int32_t)) * n;
       res->B = gs.med.B;
-      res->S_q = gs.med.S;
-      res->S = static_cast<double>(gs.med.S) / 4294967296.0;
+      res->S_q = gs.med.S_q;
+      res->S = gs.med.S;
       break;
     }
     // continue from a bracket point: copy it into a slot outside the bracket
@@ -1068,7 +1082,7 @@ int64_t Job::op_entropy(const int32_t* part, int32_t B, int32_t dense_max) {
   entropy_launch(slots_[0], B, dense);
   USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
-  return q32_host(model_S(hg_->n, hg_->e, B)) - static_cast<long long>(h_ctl_->entropy_acc);
+  return add_sat(q32_host(model_S(hg_->n, hg_->e, B)), -static_cast<long long>(h_ctl_->entropy_acc));
 }
 
 void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
@@ -1116,7 +1130,7 @@ void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t be
   USAP_CUDA(cudaMemsetAsync(ctl_, 0, sizeof(NodalCtl), st_));
   h_ctl_->itr = itr;
   USAP_CUDA(cudaMemcpyAsync(&ctl_->itr, &h_ctl_->itr, sizeof(int), cudaMemcpyHostToDevice, st_));
-  const CtlArgs ca{0, 1, 0.0, ide_q_, ide_n_, 0, 0};
+  const CtlArgs ca{0, 1, 0.0, 0.0, ide_q_, ide_n_, 0, 0};
   nodal_batch(slots_[0], B, dense, beg, end, static_cast<uint32_t>(stage), seed, true, 2, ca);
   const int32_t cnt = end - beg;
   USAP_CUDA(cudaMemcpyAsync(part, slots_[0], sizeof(int32_t) * hg_->n, cudaMemcpyDeviceToHost, st_));

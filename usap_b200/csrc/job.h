@@ -43,7 +43,8 @@ void evaluate_host(const int32_t* truth, const int32_t* given, int64_t n, usap_s
 // _prepare_for_partition_next (graph_parallel.hpp:1322-1365) on slot ids
 struct GoldenPoint {
   int32_t B = 0;
-  int64_t S = 0;
+  double S = 0.0;      // description length (model term + Q32 data term)
+  int64_t S_q = 0;     // the same in Q32, saturated beyond +-2^31
   bool finite = false;
   int32_t slot = -1;
 };
@@ -51,13 +52,21 @@ struct GoldenPoint {
 struct Golden {
   GoldenPoint large, med, small;
   // returns true when the search is over (answer: med)
-  bool step(int32_t B, int64_t S, int32_t cur_slot, float rate, int32_t* restore_slot,
+  bool step(int32_t B, double S, int64_t S_q, int32_t cur_slot, float rate, int32_t* restore_slot,
             int32_t* btm);
 };
 
 int32_t reduce_blocks(int32_t B, float rate);   // (size_t)_P.B * rate, :340
 double model_S(int64_t n, int64_t e, int32_t B);   // :1314-1316
+// t in Q32, saturated to the int64 range (|t| >= 2^31 saturates)
 long long q32_host(double t);
+// a + b in int64, saturated
+long long add_sat(long long a, long long b);
+// description length from the model term and the Q32 data term, in the
+// order both the kernels and the oracle evaluate it
+inline double desc_length(double model, long long data_q) {
+  return model + static_cast<double>(data_q) / 4294967296.0;
+}
 
 // A graph loaded into HBM (CSR, edge list, log table, hub list); read-only
 // once loaded and shared by every job that solves it.  Its device arrays
@@ -189,11 +198,11 @@ class Job {
   // a stage's whole nodal phase in one persistent launch (dense tile);
   // returns the kernel's duration in ms when `timed`
   float nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, int W, double thr,
-                    long long model_q, int32_t maxitr, int stats, int grid, bool timed);
+                    double model_d, int32_t maxitr, int stats, int grid, bool timed);
   // one nodal sweep (entropy, sweep start, every batch), launched directly
   // or recorded into a CUDA graph
   void enqueue_sweep(int32_t* part, int32_t B, bool dense, uint32_t stage, uint64_t seed, int W,
-                     double thr, long long model_q, int stats);
+                     double thr, double model_d, int stats);
   void emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int32_t* part,
                   bool dense, long long S_q, int S_ninf, long long cum_q, int cum_ninf,
                   long long moves);

@@ -853,7 +853,7 @@ __device__ __forceinline__ bool ctl_batch_end(NodalCtl* ctl, const CtlArgs& c) {
   ctl->proposals = proposals + static_cast<unsigned long long>(c.batch_vertices);
   ctl->edge_visits = edge_visits + static_cast<unsigned long long>(c.batch_edges);
   if (itr >= c.W - 1) {
-    const double S_d = S_ninf ? -INFINITY : static_cast<double>(S_q) / kQ32;
+    const double S_d = S_ninf ? -INFINITY : c.model_d + static_cast<double>(S_q) / kQ32;
     if (-mean < c.thr * S_d) {
       ctl->done = 1;
       return true;
@@ -862,10 +862,11 @@ __device__ __forceinline__ bool ctl_batch_end(NodalCtl* ctl, const CtlArgs& c) {
   return false;
 }
 
-// prepare_batch (:381-395): S from the entropy accumulator, the moving
+// prepare_batch (:381-395): the data term of S from the entropy
+// accumulator (the model term is added where S is compared), the moving
 // average of the previous sweeps' dS, and a fresh cumulative sum for this
 // sweep.  One thread; reads as in ctl_batch_end.
-__device__ __forceinline__ void ctl_sweep_start(NodalCtl* ctl, long long model_q, int W,
+__device__ __forceinline__ void ctl_sweep_start(NodalCtl* ctl, int W,
                                                 const long long* ide_q, const int* ide_n) {
   const int done = __ldcg(&ctl->done);
   const unsigned long long sweeps = __ldcg(&ctl->sweeps);
@@ -883,7 +884,7 @@ __device__ __forceinline__ void ctl_sweep_start(NodalCtl* ctl, long long model_q
     mean = ninf ? -INFINITY : (static_cast<double>(sum) / kQ32) / static_cast<double>(W - 1);
   }
   ctl->itr = itr;
-  ctl->S_q = model_q - static_cast<long long>(eacc);
+  ctl->S_q = -static_cast<long long>(eacc);
   ctl->S_ninf = 0;
   ctl->mean = mean;
   ctl->cum_q = 0;
@@ -1082,9 +1083,9 @@ __global__ void k_nodal_commit(int32_t* __restrict__ part, int32_t* __restrict__
   }
 }
 
-__global__ void k_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const long long* ide_q,
+__global__ void k_ctl_sweep_start(NodalCtl* ctl, int W, const long long* ide_q,
                                   const int* ide_n) {
-  ctl_sweep_start(ctl, model_q, W, ide_q, ide_n);
+  ctl_sweep_start(ctl, W, ide_q, ide_n);
 }
 
 // --- persistent nodal phase ----------------------------------------------------
@@ -1206,7 +1207,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
     }
     if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-      ctl_sweep_start(ctl, p.model_q, p.W, p.ide_q, p.ide_n);
+      ctl_sweep_start(ctl, p.W, p.ide_q, p.ide_n);
       ctl->entropy_acc = 0;
     }
     if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
@@ -1262,7 +1263,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       if (blockIdx.x == 0 && threadIdx.x == 0) {
         const long long edges = (static_cast<long long>(__ldg(p.a.out_ptr + a.end)) - __ldg(p.a.out_ptr + a.beg)) +
                                 (static_cast<long long>(__ldg(p.a.in_ptr + a.end)) - __ldg(p.a.in_ptr + a.beg));
-        const CtlArgs ca{1, p.W, p.thr, p.ide_q, p.ide_n, count, edges};
+        const CtlArgs ca{1, p.W, p.thr, p.model_d, p.ide_q, p.ide_n, count, edges};
         done = ctl_batch_end(ctl, ca);
         ctl->vnext = 0;
       }
@@ -1427,7 +1428,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
       if (grid_barrier(gc, &target, false, &s_state) < 0) return;
       if (blockIdx.x == 0 && threadIdx.x < K && s_act[threadIdx.x] && s_bi[threadIdx.x] == 0) {
         const PhaseArgs& p = jobs[threadIdx.x];
-        ctl_sweep_start(p.a.ctl, p.model_q, p.W, p.ide_q, p.ide_n);
+        ctl_sweep_start(p.a.ctl, p.W, p.ide_q, p.ide_n);
         p.a.ctl->entropy_acc = 0;
       }
       if (grid_barrier(gc, &target, false, &s_state) < 0) return;
@@ -1496,7 +1497,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
         const int beg = s_bi[threadIdx.x] * p.bs, end = min(p.n, beg + p.bs);
         const long long edges = (static_cast<long long>(__ldg(p.a.out_ptr + end)) - __ldg(p.a.out_ptr + beg)) +
                                 (static_cast<long long>(__ldg(p.a.in_ptr + end)) - __ldg(p.a.in_ptr + beg));
-        const CtlArgs ca{1, p.W, p.thr, p.ide_q, p.ide_n, end - beg, edges};
+        const CtlArgs ca{1, p.W, p.thr, p.model_d, p.ide_q, p.ide_n, end - beg, edges};
         ctl_batch_end(p.a.ctl, ca);
       }
       if (threadIdx.x == 0) gc->vnext = 0;
@@ -1688,9 +1689,9 @@ void launch_nodal_commit(const GraphDev& g, int32_t* part, int32_t* move_to, int
   USAP_LAUNCHED();
 }
 
-void launch_ctl_sweep_start(NodalCtl* ctl, long long model_q, int W, const long long* ide_q,
+void launch_ctl_sweep_start(NodalCtl* ctl, int W, const long long* ide_q,
                             const int* ide_n, cudaStream_t st) {
-  k_ctl_sweep_start<<<1, 1, 0, st>>>(ctl, model_q, W, ide_q, ide_n);
+  k_ctl_sweep_start<<<1, 1, 0, st>>>(ctl, W, ide_q, ide_n);
   USAP_LAUNCHED();
 }
 

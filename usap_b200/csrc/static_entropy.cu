@@ -143,7 +143,11 @@ __global__ void k_static_entropy(StaticView v, int B) {
 __global__ void k_static_finish(StaticView v, long long model_q, int64_t* S_q) {
   const StaticCounters c = *v.ctr;
   const bool bad = c.bad || c.wsum > static_cast<unsigned long long>(kStaticMaxWeight);
-  *S_q = bad ? static_cast<int64_t>(LLONG_MIN) : model_q - static_cast<long long>(c.acc);
+  // model term (saturated on the host) plus data term, saturated
+  const long long b = -static_cast<long long>(c.acc);
+  long long r = static_cast<long long>(static_cast<unsigned long long>(model_q) + static_cast<unsigned long long>(b));
+  if ((model_q > 0 && b > 0 && r < 0) || (model_q < 0 && b < 0 && r >= 0)) r = model_q > 0 ? LLONG_MAX : LLONG_MIN;
+  *S_q = bad ? static_cast<int64_t>(LLONG_MIN) : r;
 }
 
 int grid_of(int64_t work) {

@@ -80,7 +80,18 @@ typedef struct usap_params {
                           when the tile is dense and B <= 4096; 0: one launch per batch.
                           usap_batch_partition always uses per-batch launches. */
   int32_t persistent_ctas; /* CTAs of the cooperative kernel (one per SM); 0 = every SM */
-  int32_t reserved[2];
+  int32_t precision;   /* 0 (default): every dS term in FP64, rounded to Q32 and summed exactly.
+                          1 and 2: dS also evaluated with single-precision operations only, and
+                          the nodal accept and merge choices taken on that value; the exact FP64
+                          value is computed beside it to count flipped decisions
+                          (usap_result.fp32_*).  1: compensated FP32 -- the log table held as
+                          float pairs (hi + lo), every term and sum in float-pair arithmetic
+                          (TwoSum, TwoProduct by fused multiply-add), about 44 bits.  2: plain
+                          FP32 terms from the rounded log table, compensated sums only (loses
+                          accuracy on large counts; kept to measure that).  The description
+                          length, the golden-section comparisons and the convergence test stay
+                          FP64 in every mode. */
+  int32_t reserved[1];
 } usap_params;
 
 typedef struct usap_result {
@@ -101,6 +112,16 @@ typedef struct usap_result {
   int64_t cub_calls;          /* CUB sort/scan/reduce calls during the call */
   int64_t h2d_bytes, d2h_bytes;  /* host<->device traffic of the call */
   int64_t sweep_graph_launches;  /* nodal sweeps replayed from a captured CUDA graph */
+  /* precision 1 or 2: the FP32 values and decisions against the FP64 values
+   * of the same evaluations (zero with precision = 0) */
+  int64_t fp32_nodal_evals;  /* nodal dS evaluations with a finite FP64 value */
+  int64_t fp32_nodal_flips;  /* ... whose FP32 accept decision differs from FP64's */
+  int64_t fp32_merge_evals;  /* merge proposals */
+  int64_t fp32_merge_flips;  /* blocks whose chosen merge target differs from FP64's choice */
+  int64_t fp32_order_flips;  /* adjacent pairs of the merge order that FP64 ranks the other way */
+  double fp32_flip_rate;     /* fp32_nodal_flips / fp32_nodal_evals */
+  double fp32_err_max;       /* largest |dS_fp32 - dS_fp64| over nodal and merge evaluations */
+  double fp32_err_mean;      /* mean |dS_fp32 - dS_fp64| over nodal evaluations */
 } usap_result;
 
 typedef struct usap_scores {
@@ -212,6 +233,24 @@ usap_status usap_op_nodal_batch(usap_ctx* ctx, int32_t* part, int32_t B, int32_t
                                 uint64_t seed, int32_t* prop_s, int64_t* prop_q,
                                 int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
                                 int64_t* moves);
+/* The same two operations in a given precision mode (usap_params.precision;
+ * no counterpart in the reference, whose dS is single precision throughout).
+ * In modes 1 and 2, dS is evaluated in FP32 beside the exact FP64 value and
+ * decisions are taken on the FP32 value: prop_q gets the exact FP64 values
+ * (Q32) and prop_f the FP32 ones (the float pair's value hi + lo, which is
+ * exact in a double); best_q is the merge key, the chosen proposal's FP32
+ * value in Q32; *flips counts the blocks whose chosen merge
+ * target, or the batch vertices whose accept decision, differs from the
+ * FP64 path's on the same state.  Mode 0 is the plain operation. */
+usap_status usap_op_merge_phase_prec(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t K,
+                                     int32_t stage, uint64_t seed, int32_t precision, int32_t* best_s,
+                                     int64_t* best_q, int32_t* prop_s, int64_t* prop_q, double* prop_f,
+                                     int64_t* flips);
+usap_status usap_op_nodal_batch_prec(usap_ctx* ctx, int32_t* part, int32_t B, int32_t dense_max,
+                                     int32_t beg, int32_t end, int32_t itr, int32_t stage,
+                                     uint64_t seed, int32_t precision, int32_t* prop_s, int64_t* prop_q,
+                                     double* prop_f, int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
+                                     int64_t* moves, int64_t* flips);
 
 /* --- served form: a partition service on one GPU --------------------------
  * The reference has no service; this replaces a caller running Graph_P

@@ -77,6 +77,11 @@ class OgGPoint(C.Structure):
                 ("slot", C.c_int32)]
 
 
+class OgFSum(C.Structure):
+    _fields_ = [("s", C.c_double), ("c", C.c_double), ("abs", C.c_double), ("n", C.c_int64),
+                ("mode", C.c_int32)]
+
+
 class OgGolden(C.Structure):
     _fields_ = [("large", OgGPoint), ("med", OgGPoint), ("small", OgGPoint)]
 
@@ -118,6 +123,12 @@ def lib() -> C.CDLL:
         L.og_nodal_dq.argtypes = [C.POINTER(OgGraph), i32p, C.POINTER(OgBlocks), C.c_int32,
                                   C.c_int32, i32p]
         L.og_nodal_dq.restype = C.c_int64
+        L.og_merge_dq_f32.argtypes = [C.POINTER(OgGraph), C.POINTER(OgBlocks), C.c_int32, C.c_int32,
+                                      C.c_int32, C.POINTER(OgFSum)]
+        L.og_merge_dq_f32.restype = C.c_int64
+        L.og_nodal_dq_f32.argtypes = [C.POINTER(OgGraph), i32p, C.POINTER(OgBlocks), C.c_int32,
+                                      C.c_int32, C.c_int32, i32p, C.POINTER(OgFSum)]
+        L.og_nodal_dq_f32.restype = C.c_int64
         L.og_merge_propose.argtypes = [C.POINTER(OgGraph), C.POINTER(OgBlocks), C.c_int32,
                                        C.c_int32, C.c_int32, C.c_uint64]
         L.og_merge_propose.restype = C.c_int32
@@ -259,6 +270,22 @@ class OracleBlocks:
         q = lib().og_nodal_dq(C.byref(self.g.g), _p32(self.part), C.byref(self.b), v, s,
                               C.byref(ninf))
         return int(q), int(ninf.value)
+
+    def merge_dq_f32(self, r: int, s: int, mode: int = 1):
+        """exact dS (Q32) and the sum of the FP32 terms of precision `mode`
+        (1: float pairs, 2: plain floats): (q, value, sum |term|, terms)"""
+        f = OgFSum()
+        q = lib().og_merge_dq_f32(C.byref(self.g.g), C.byref(self.b), r, s, mode, C.byref(f))
+        return int(q), f.s + f.c, f.abs, int(f.n)
+
+    def nodal_dq_f32(self, v: int, s: int, mode: int = 1):
+        """exact dS (Q32), -inf flag and the sum of the FP32 terms of precision
+        `mode`: (q, ninf, value, sum |term|, terms)"""
+        ninf = C.c_int32(0)
+        f = OgFSum()
+        q = lib().og_nodal_dq_f32(C.byref(self.g.g), _p32(self.part), C.byref(self.b), v, s, mode,
+                                  C.byref(ninf), C.byref(f))
+        return int(q), int(ninf.value), f.s + f.c, f.abs, int(f.n)
 
     def merge_propose(self, r: int, k: int, stage: int, seed: int) -> int:
         return int(lib().og_merge_propose(C.byref(self.g.g), C.byref(self.b), r, k, stage, seed))

@@ -284,6 +284,93 @@ static inline double og_h(const double* L, int64_t x, int64_t y) {
   return (a + b) - c;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Precision modes 1 and 2 of the CUDA path evaluate the same terms with
+ * single-precision operations only (C float arithmetic, no contraction):
+ *  - mode 1: float pairs (hi, lo) worth hi + lo, the log table held as
+ *    pairs (hi = log k rounded to float, lo = the remainder rounded), every
+ *    term in pair arithmetic built from Knuth's TwoSum and a TwoProduct by
+ *    fused multiply-add;
+ *  - mode 2: plain float terms from the rounded log values.
+ * The terms are summed here in double with Neumaier's compensation, which
+ * is exact enough to be the reference for the CUDA path's FP32 pair sums;
+ * `abs` and `n` give the error bound's scale (sum of |term|) and the number
+ * of terms.                                                                */
+typedef struct { float hi, lo; } og_ff;
+
+static inline og_ff og_two_sum(float a, float b) {
+  float s = a + b;
+  float z = s - a;
+  og_ff r = {s, (a - (s - z)) + (b - z)};
+  return r;
+}
+
+static inline og_ff og_ff_add(og_ff a, og_ff b) {
+  og_ff s = og_two_sum(a.hi, b.hi);
+  return og_two_sum(s.hi, s.lo + (a.lo + b.lo));
+}
+
+static inline og_ff og_ff_neg(og_ff a) { og_ff r = {-a.hi, -a.lo}; return r; }
+static inline og_ff og_ff_sub(og_ff a, og_ff b) { return og_ff_add(a, og_ff_neg(b)); }
+
+static inline og_ff og_ff_mul_ll(og_ff d, int64_t x) {
+  float xh = (float)x;
+  float xl = (float)(x - (int64_t)xh);
+  float p = xh * d.hi;
+  float e = fmaf(xh, d.hi, -p);
+  e = e + (xh * d.lo + xl * d.hi);
+  return og_two_sum(p, e);
+}
+
+static inline og_ff og_ff_log(const double* L, int64_t k) {
+  double x = L[k];
+  float hi = (float)x;
+  og_ff r = {hi, isinf(x) ? 0.0f : (float)(x - (double)hi)};
+  return r;
+}
+
+static const og_ff og_ff_zero = {0.0f, 0.0f};
+
+static inline og_ff og_g32(const double* L, int mode, int64_t x, int64_t din_arg, int64_t dout_arg) {
+  if (x == 0) return og_ff_zero;
+  og_ff a = og_ff_log(L, x), b = og_ff_log(L, din_arg), c = og_ff_log(L, dout_arg);
+  if (mode == 1) return og_ff_mul_ll(og_ff_sub(og_ff_sub(a, b), c), x);
+  og_ff r = {(float)x * ((a.hi - b.hi) - c.hi), 0.0f};
+  return r;
+}
+
+static inline og_ff og_coef32(const double* L, int mode, int64_t n, int64_t a_new, int64_t a_old) {
+  if (n == 0) return og_ff_zero;
+  og_ff a = og_ff_log(L, a_new), b = og_ff_log(L, a_old);
+  if (mode == 1) return og_ff_mul_ll(og_ff_sub(a, b), n);
+  og_ff r = {(float)n * (a.hi - b.hi), 0.0f};
+  return r;
+}
+
+static inline og_ff og_h32(const double* L, int mode, int64_t x, int64_t y) {
+  og_ff lx = og_ff_log(L, x), ly = og_ff_log(L, y), lxy = og_ff_log(L, x + y);
+  if (mode == 1)
+    return og_ff_sub(og_ff_add(og_ff_mul_ll(lx, x), og_ff_mul_ll(ly, y)), og_ff_mul_ll(lxy, x + y));
+  float a = (float)x * lx.hi;
+  float b = (float)y * ly.hi;
+  float c = (float)(x + y) * lxy.hi;
+  og_ff r = {(a + b) - c, 0.0f};
+  return r;
+}
+
+static inline void og_fadd(og_fsum* f, og_ff t) {
+  double x = (double)t.hi + (double)t.lo;   /* exact */
+  if (x == 0.0) return;
+  double s = f->s + x;
+  if (fabs(f->s) >= fabs(x)) f->c += (f->s - s) + x;
+  else f->c += (x - s) + f->s;
+  f->s = s;
+  f->abs += fabs(x);
+  f->n++;
+}
+
+double og_fsum_value(const og_fsum* f) { return f->s + f->c; }
+
 /* model term of _compute_overall_entropy (:1314-1316), evaluated in FP64;
  * the reference's precedence (x*log(x) not scaled by E) is kept */
 double og_model_S(int64_t n, int64_t e, int32_t B) {
@@ -316,7 +403,8 @@ int64_t og_entropy_q(const og_graph* g, const og_blocks* b) {
  *   = h(M_ri,M_si) + M_ri (L[dout_s'] - L[dout_r]) + M_si (L[dout_s'] - L[dout_s])
  * with h(x,y) = xL[x] + yL[y] - (x+y)L[x+y], which vanishes unless both
  * counts are non-zero; columns likewise.                                   */
-int64_t og_merge_dq(const og_graph* g, const og_blocks* b, int32_t r, int32_t s) {
+static int64_t og_merge_dq_impl(const og_graph* g, const og_blocks* b, int32_t r, int32_t s, og_fsum* f) {
+  const int FM = f ? f->mode : 0;
   const double* L = g->logk;
   int32_t B = b->B;
   const int64_t* M = b->M;
@@ -332,13 +420,24 @@ int64_t og_merge_dq(const og_graph* g, const og_blocks* b, int32_t r, int32_t s)
   acc += og_quantize(og_g(L, Msr, dr_in, ds_out));
   acc += og_quantize(og_g(L, Mss, ds_in, ds_out));
   acc -= og_quantize(og_g(L, Mrr + Mrs + Msr + Mss, ds_in_new, ds_out_new));
+  if (f) og_fadd(f, og_g32(L, FM, Mrr, dr_in, dr_out));
+  if (f) og_fadd(f, og_g32(L, FM, Mrs, ds_in, dr_out));
+  if (f) og_fadd(f, og_g32(L, FM, Msr, dr_in, ds_out));
+  if (f) og_fadd(f, og_g32(L, FM, Mss, ds_in, ds_out));
+  if (f) og_fadd(f, og_ff_neg(og_g32(L, FM, Mrr + Mrs + Msr + Mss, ds_in_new, ds_out_new)));
   for (int32_t i = 0; i < B; i++) {
     if (i == r || i == s) continue;
     int64_t x = M[(size_t)r * B + i], y = M[(size_t)s * B + i];
-    if (x > 0 && y > 0) acc += og_quantize(og_h(L, x, y));
+    if (x > 0 && y > 0) {
+      acc += og_quantize(og_h(L, x, y));
+      if (f) og_fadd(f, og_h32(L, FM, x, y));
+    }
     x = M[(size_t)i * B + r];
     y = M[(size_t)i * B + s];
-    if (x > 0 && y > 0) acc += og_quantize(og_h(L, x, y));
+    if (x > 0 && y > 0) {
+      acc += og_quantize(og_h(L, x, y));
+      if (f) og_fadd(f, og_h32(L, FM, x, y));
+    }
   }
   int64_t Ar, As, Cr, Cs;
   if (s != r) {
@@ -354,7 +453,22 @@ int64_t og_merge_dq(const og_graph* g, const og_blocks* b, int32_t r, int32_t s)
   acc += og_quantize(og_coef(L, As, ds_out_new, ds_out));
   acc += og_quantize(og_coef(L, Cr, ds_in_new, dr_in));
   acc += og_quantize(og_coef(L, Cs, ds_in_new, ds_in));
+  if (f) og_fadd(f, og_coef32(L, FM, Ar, ds_out_new, dr_out));
+  if (f) og_fadd(f, og_coef32(L, FM, As, ds_out_new, ds_out));
+  if (f) og_fadd(f, og_coef32(L, FM, Cr, ds_in_new, dr_in));
+  if (f) og_fadd(f, og_coef32(L, FM, Cs, ds_in_new, ds_in));
   return acc;
+}
+
+int64_t og_merge_dq(const og_graph* g, const og_blocks* b, int32_t r, int32_t s) {
+  return og_merge_dq_impl(g, b, r, s, NULL);
+}
+
+int64_t og_merge_dq_f32(const og_graph* g, const og_blocks* b, int32_t r, int32_t s, int32_t mode, og_fsum* f) {
+  f->s = f->c = f->abs = 0.0;
+  f->n = 0;
+  f->mode = mode;
+  return og_merge_dq_impl(g, b, r, s, f);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -366,8 +480,9 @@ int64_t og_merge_dq(const og_graph* g, const og_blocks* b, int32_t r, int32_t s)
  * with the counts known exactly from the block degrees.  A new-state term
  * with a zero degree is +inf, as log(x/0) is in the reference; dS is then
  * -inf and *neg_inf is set.                                               */
-int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
-                    int32_t v, int32_t s, int32_t* neg_inf) {
+static int64_t og_nodal_dq_impl(const og_graph* g, const int32_t* part, const og_blocks* b,
+                                int32_t v, int32_t s, int32_t* neg_inf, og_fsum* f) {
+  const int FM = f ? f->mode : 0;
   const double* L = g->logk;
   int32_t B = b->B;
   const int64_t* M = b->M;
@@ -406,6 +521,10 @@ int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
       acc += og_quantize(og_g(L, S, dinb, ds_out));
       acc -= og_quantize(og_g(L, R - wo[bb], dinb, dr_out_n));
       acc -= og_quantize(og_g(L, S + wo[bb], dinb, ds_out_n));
+      if (f) og_fadd(f, og_g32(L, FM, R, dinb, dr_out));
+      if (f) og_fadd(f, og_g32(L, FM, S, dinb, ds_out));
+      if (f) og_fadd(f, og_ff_neg(og_g32(L, FM, R - wo[bb], dinb, dr_out_n)));
+      if (f) og_fadd(f, og_ff_neg(og_g32(L, FM, S + wo[bb], dinb, ds_out_n)));
       sumXR += R;
       sumXS += S;
     }
@@ -415,6 +534,10 @@ int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
       acc += og_quantize(og_g(L, Sc, ds_in, doutb));
       acc -= og_quantize(og_g(L, Rc - wi[bb], dr_in_n, doutb));
       acc -= og_quantize(og_g(L, Sc + wi[bb], ds_in_n, doutb));
+      if (f) og_fadd(f, og_g32(L, FM, Rc, dr_in, doutb));
+      if (f) og_fadd(f, og_g32(L, FM, Sc, ds_in, doutb));
+      if (f) og_fadd(f, og_ff_neg(og_g32(L, FM, Rc - wi[bb], dr_in_n, doutb)));
+      if (f) og_fadd(f, og_ff_neg(og_g32(L, FM, Sc + wi[bb], ds_in_n, doutb)));
       sumYR += Rc;
       sumYS += Sc;
     }
@@ -424,18 +547,49 @@ int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
   acc += og_quantize(og_g(L, Rs, ds_in, dr_out));
   acc += og_quantize(og_g(L, Sr, dr_in, ds_out));
   acc += og_quantize(og_g(L, Ss, ds_in, ds_out));
+  if (f) og_fadd(f, og_g32(L, FM, Rr, dr_in, dr_out));
+  if (f) og_fadd(f, og_g32(L, FM, Rs, ds_in, dr_out));
+  if (f) og_fadd(f, og_g32(L, FM, Sr, dr_in, ds_out));
+  if (f) og_fadd(f, og_g32(L, FM, Ss, ds_in, ds_out));
   double nt[4] = {og_g(L, Rr - wor, dr_in_n, dr_out_n), og_g(L, Rs - wos, ds_in_n, dr_out_n),
                   og_g(L, Sr + wor, dr_in_n, ds_out_n), og_g(L, Ss + wos, ds_in_n, ds_out_n)};
+  og_ff nt32[4] = {og_ff_zero, og_ff_zero, og_ff_zero, og_ff_zero};
+  if (f) {
+    nt32[0] = og_g32(L, FM, Rr - wor, dr_in_n, dr_out_n);
+    nt32[1] = og_g32(L, FM, Rs - wos, ds_in_n, dr_out_n);
+    nt32[2] = og_g32(L, FM, Sr + wor, dr_in_n, ds_out_n);
+    nt32[3] = og_g32(L, FM, Ss + wos, ds_in_n, ds_out_n);
+  }
   for (int t = 0; t < 4; t++) {
     if (isinf(nt[t])) *neg_inf = 1;
-    else acc -= og_quantize(nt[t]);
+    else {
+      acc -= og_quantize(nt[t]);
+      if (f) og_fadd(f, og_ff_neg(nt32[t]));
+    }
   }
   acc += og_quantize(og_coef(L, dr_out - Rr - Rs - sumXR, dr_out_n, dr_out));
   acc += og_quantize(og_coef(L, ds_out - Sr - Ss - sumXS, ds_out_n, ds_out));
   acc += og_quantize(og_coef(L, dr_in - Rr - Sr - sumYR, dr_in_n, dr_in));
   acc += og_quantize(og_coef(L, ds_in - Rs - Ss - sumYS, ds_in_n, ds_in));
+  if (f) og_fadd(f, og_coef32(L, FM, dr_out - Rr - Rs - sumXR, dr_out_n, dr_out));
+  if (f) og_fadd(f, og_coef32(L, FM, ds_out - Sr - Ss - sumXS, ds_out_n, ds_out));
+  if (f) og_fadd(f, og_coef32(L, FM, dr_in - Rr - Sr - sumYR, dr_in_n, dr_in));
+  if (f) og_fadd(f, og_coef32(L, FM, ds_in - Rs - Ss - sumYS, ds_in_n, ds_in));
   free(wo); free(wi); free(seen); free(list);
   return acc;
+}
+
+int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
+                    int32_t v, int32_t s, int32_t* neg_inf) {
+  return og_nodal_dq_impl(g, part, b, v, s, neg_inf, NULL);
+}
+
+int64_t og_nodal_dq_f32(const og_graph* g, const int32_t* part, const og_blocks* b,
+                        int32_t v, int32_t s, int32_t mode, int32_t* neg_inf, og_fsum* f) {
+  f->s = f->c = f->abs = 0.0;
+  f->n = 0;
+  f->mode = mode;
+  return og_nodal_dq_impl(g, part, b, v, s, neg_inf, f);
 }
 
 /* ------------------------------------------------------------------------ */

@@ -33,6 +33,15 @@ extern "C" {
 
 #define OG_Q32_SCALE 4294967296.0
 
+/* FP32 terms of precision mode 1 (float-pair terms) or 2 (plain float
+ * terms), summed in double with compensation: value = s + c; abs = sum of
+ * |term|; n = number of non-zero terms */
+typedef struct {
+  double s, c, abs;
+  int64_t n;
+  int32_t mode;
+} og_fsum;
+
 typedef struct {
   int32_t n;
   int64_t e;
@@ -122,6 +131,12 @@ int64_t og_entropy_q(const og_graph* g, const og_blocks* b);
 int64_t og_merge_dq(const og_graph* g, const og_blocks* b, int32_t r, int32_t s);
 int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
                     int32_t v, int32_t s, int32_t* neg_inf);
+/* the same dS with the FP32 terms of precision mode 1 summed into *f */
+int64_t og_merge_dq_f32(const og_graph* g, const og_blocks* b, int32_t r, int32_t s, int32_t mode,
+                        og_fsum* f);
+int64_t og_nodal_dq_f32(const og_graph* g, const int32_t* part, const og_blocks* b,
+                        int32_t v, int32_t s, int32_t mode, int32_t* neg_inf, og_fsum* f);
+double og_fsum_value(const og_fsum* f);
 int32_t og_merge_propose(const og_graph* g, const og_blocks* b, int32_t r, int32_t k,
                          int32_t stage, uint64_t seed);
 int32_t og_nodal_propose(const og_graph* g, const int32_t* part, const og_blocks* b,

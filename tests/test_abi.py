@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _declared():
     text = open(os.path.join(ROOT, "include", "usap.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)     # drop comments
-    return sorted(set(re.findall(r"\b(usap_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(usap_[a-z0-9_]+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():

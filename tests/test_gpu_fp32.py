@@ -1,0 +1,179 @@
+"""Precision modes 1 and 2 (FP32 dS) against the oracle, through the C ABI.
+
+In these modes the CUDA path evaluates every dS term with single-precision
+operations only -- mode 1 in float-pair arithmetic from a float-pair log
+table, mode 2 as plain floats from the rounded log values -- and sums the
+terms in float pairs; decisions are taken on that value while the exact
+FP64 value is computed beside it.  The oracle computes the same float terms
+bit for bit and sums them in double.  From the same state the checks are:
+
+* the proposals and the exact FP64 dS (Q32) are bit-exact with the oracle;
+* the FP32 dS is within the pair sum's error bound of the oracle's sum of
+  the same terms:  |f - F| <= 2^-44 (n + 4) sum|t|  for n terms;
+* every decision follows the FP32 value (accept iff f < 0 or dS = -inf; the
+  merge choice is the first strict minimum of the FP32 keys), and agrees
+  with the oracle's sum wherever that sum is farther from zero than the
+  bound;
+* the flip counts equal the decisions whose FP32 and FP64 signs (choices)
+  differ.
+Whole solves in modes 1 and 2 are compared with the FP64 solve of the same
+seed.
+"""
+import numpy as np
+import pytest
+
+from usap_b200 import generator as gen
+
+pytestmark = pytest.mark.gpu
+
+
+def fp32_bound(abs_sum, n):
+    return 2.0 ** -44 * (n + 4) * abs_sum + 1e-300
+
+
+@pytest.fixture(scope="module")
+def api():
+    from usap_b200 import api as a
+    return a
+
+
+def _hub_graph(seed=3):
+    G = gen.generate(gen.SBMConfig(n=600, blocks=6, within=0.7, alpha=2, seed=seed))
+    rng = np.random.default_rng(seed)
+    ins = rng.choice(G.n, 320, replace=False)
+    outs = rng.choice(G.n, 160, replace=False)
+    src = np.concatenate([G.src, ins, np.full(160, 5), G.src[:20]])
+    dst = np.concatenate([G.dst, np.full(320, 5), outs, G.dst[:20]])
+    return G.n, src.astype(np.int32), dst.astype(np.int32), None
+
+
+def _weighted_graph(seed=4):
+    G = gen.generate(gen.SBMConfig(n=400, blocks=5, within=0.75, alpha=5, seed=seed))
+    w = np.random.default_rng(seed).integers(1, 5, G.num_edges).astype(np.int32)
+    return G.n, G.src, G.dst, w
+
+
+GRAPHS = {
+    "c0": lambda: (lambda G: (G.n, G.src, G.dst, None))(gen.generate(gen.config_c0())),
+    "hub": _hub_graph,
+    "weighted": _weighted_graph,
+}
+
+
+@pytest.fixture(scope="module", params=sorted(GRAPHS))
+def case(request, api, oracle):
+    n, src, dst, w = GRAPHS[request.param]()
+    ctx = api.Context(0)
+    ctx.load(src, dst, w, n)
+    og = oracle.OracleGraph(n, src, dst, w)
+    B_scc, part_scc = og.scc(20)
+    rng = np.random.default_rng(11)
+    part_rand = rng.integers(0, 7, n).astype(np.int32)
+    part_rand[:7] = np.arange(7)
+    states = {"scc": (B_scc, part_scc), "rand7": (7, part_rand)}
+    yield request.param, ctx, og, states
+    ctx.close()
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("dense_max", [4096, 1])
+def test_nodal_batch_fp32(case, dense_max, mode):
+    name, ctx, og, states = case
+    for sname, (B, part) in states.items():
+        n = part.size
+        for beg, end, itr, stage, seed in ((0, n, 0, 0, 1), (n // 3, n // 3 + n // 4, 5, 2, 99)):
+            gpart, g = ctx.op_nodal_batch(part, B, beg, end, itr, stage, seed, dense_max, precision=mode)
+            blk = og.blocks(part, B)
+            o = blk.nodal_batch(beg, end, itr, stage, seed)   # FP64 decisions, same proposals
+            assert np.array_equal(g["prop_s"], o["prop_s"]), (name, sname)
+            assert np.array_equal(g["prop_ninf"], o["prop_ninf"]), (name, sname)
+            assert np.array_equal(g["prop_q"], o["prop_q"]), (name, sname)
+            blk0 = og.blocks(part, B)
+            flips = moves = cum = 0
+            for i in range(end - beg):
+                v = beg + i
+                s = int(g["prop_s"][i])
+                f = float(g["prop_f"][i])
+                if s < 0:
+                    assert gpart[v] == part[v]
+                    continue
+                q, ninf, F, abs_sum, nt = blk0.nodal_dq_f32(v, s, mode)
+                assert q == g["prop_q"][i] and ninf == g["prop_ninf"][i]
+                accept = bool(ninf) or f < 0.0
+                assert gpart[v] == (s if accept else part[v]), (name, sname, v)
+                if accept:
+                    moves += 1
+                    cum += 0 if ninf else q
+                if ninf:
+                    continue
+                tol = fp32_bound(abs_sum, nt)
+                assert abs(f - F) <= tol, (name, sname, v, f, F, tol)
+                if abs(F) > tol:
+                    assert (f < 0.0) == (F < 0.0), (name, sname, v)
+                flips += (q < 0) != (f < 0.0)
+            assert g["moves"] == moves and g["flips"] == flips, (name, sname)
+            assert g["cum_q"] == cum
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_merge_phase_fp32(case, mode):
+    name, ctx, og, states = case
+    K = 10
+    for sname, (B, part) in states.items():
+        for stage, seed in ((0, 0), (3, 12345678901)):
+            best_s, best_q, ps, pq, pf, flips = ctx.op_merge_phase(part, B, K, stage, seed, precision=mode)
+            blk = og.blocks(part, B)
+            keys = np.rint(pf * 2.0 ** 32).astype(np.int64)
+            want_flips = 0
+            for r in range(B):
+                for k in range(K):
+                    s = blk.merge_propose(r, k, stage, seed)
+                    assert ps[r, k] == s, (name, sname, r, k)
+                    q, F, abs_sum, nt = blk.merge_dq_f32(r, s, mode)
+                    assert pq[r, k] == q, (name, sname, r, k)
+                    tol = fp32_bound(abs_sum, nt)
+                    assert abs(float(pf[r, k]) - F) <= tol, (name, sname, r, k, float(pf[r, k]), F)
+                kf = int(np.argmin(keys[r]))     # first strict minimum
+                kx = int(np.argmin(pq[r]))
+                assert best_s[r] == ps[r, kf] and best_q[r] == keys[r, kf], (name, sname, r)
+                want_flips += ps[r, kf] != ps[r, kx]
+            assert flips == want_flips, (name, sname)
+
+
+@pytest.mark.parametrize("mode,persistent", [(1, 1), (1, 0), (2, 1)])
+def test_fp32_solve_close_to_fp64(api, oracle, mode, persistent):
+    """N=5000: a solve in precision mode 1 or 2 against the FP64 solve of the
+    same seed.  Mode 1's dS is within about 1e-6 of FP64's, so its decisions
+    almost never differ; mode 2 (plain float terms) errs by up to ~0.05 on
+    counts of a few thousand and flips more often.  A flipped decision sends
+    the chain elsewhere, so whole-solve agreement is statistical: S and NMI
+    within the tolerances below."""
+    from usap_b200 import native as nat
+    G = gen.generate(gen.config_c1(within=0.5, alpha=1.0, seed=1))
+    ctx = api.Context(0)
+    ctx.load(G.src, G.dst, None, G.n)
+    base = dict(num_batch_nodal_update=10, seed=7, persistent=persistent)
+    p64, r64 = ctx.partition(nat.default_params(**base))
+    p32, r32 = ctx.partition(nat.default_params(precision=mode, **base))
+    p32b, r32b = ctx.partition(nat.default_params(precision=mode, **base))
+    ctx.close()
+    # precision 0 reports nothing; precision 1, 2 are deterministic
+    assert r64["fp32_nodal_evals"] == 0 and r64["fp32_flip_rate"] == 0.0
+    assert np.array_equal(p32, p32b) and r32["S_q"] == r32b["S_q"]
+    assert r32["fp32_nodal_evals"] > 0 and r32["fp32_merge_evals"] > 0
+    assert r32["fp32_flip_rate"] == r32["fp32_nodal_flips"] / r32["fp32_nodal_evals"]
+    assert 0.0 < r32["fp32_err_mean"] <= r32["fp32_err_max"]
+    if mode == 1:
+        assert r32["fp32_flip_rate"] < 1e-4 and r32["fp32_err_max"] < 1e-4
+    else:
+        assert r32["fp32_flip_rate"] < 1e-2 and r32["fp32_err_max"] < 1.0
+    # the description length of the result is the exact one of its partition
+    og = oracle.OracleGraph(G.n, G.src, G.dst, None)
+    assert og.blocks(p32, r32["B"]).entropy_q() == r32["S_q"]
+    assert abs(r32["S"] - r64["S"]) <= 2e-3 * abs(r64["S"])
+    e64 = api.evaluate(G.truth, p64)
+    e32 = api.evaluate(G.truth, p32)
+    assert abs(e32["nmi"] - e64["nmi"]) <= 0.02
+    print("precision", mode, "persistent", persistent, r32["fp32_nodal_evals"], r32["fp32_nodal_flips"],
+          r32["fp32_merge_flips"], r32["fp32_order_flips"], r32["fp32_err_max"], r32["fp32_err_mean"],
+          r32["S"], r64["S"], e32["nmi"], e64["nmi"])

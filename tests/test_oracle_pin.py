@@ -113,6 +113,36 @@ def test_nodal_delta_entropy(oracle, ref_fixtures):
                         assert (q < 0) == bool(acc), (name, sname, v)
 
 
+def test_fp32_terms(oracle, ref_fixtures):
+    """Precision modes 1 (float-pair terms) and 2 (plain float terms): the
+    sum of the FP32 terms stays within the reference's own float build's
+    tolerance (mode 2, the same arithmetic class as the reference) or within
+    the pair arithmetic's error of the exact FP64 value (mode 1: about 2^-44
+    of the terms' magnitudes, plus the Q32 rounding of the exact terms)."""
+    for name in _cases(ref_fixtures):
+        og = _graph(oracle, ref_fixtures, name)
+        for sname, st in ref_fixtures["cases"][name]["states"].items():
+            blk = og.blocks(np.array(st["part"]), st["B"])
+            for r, s, d in st["merge_f32"]:
+                q, F, abs_sum, nt = blk.merge_dq_f32(r, s, 2)
+                assert q == blk.merge_dq(r, s)
+                assert abs(F - d) <= F32_DS_ABS, (name, sname, r, s, F, d)
+                q1, F1, abs1, nt1 = blk.merge_dq_f32(r, s, 1)
+                assert q1 == q
+                assert abs(F1 - q / Q) <= (nt1 + 1) * 2.0 ** -32 + 2.0 ** -40 * abs1, (name, sname, r, s)
+            for v, r, s, d, acc in st["nodal_f32"]:
+                if r == s:
+                    continue
+                q, ninf, F, abs_sum, nt = blk.nodal_dq_f32(v, s, 2)
+                assert (q, ninf) == blk.nodal_dq(v, s)
+                if ninf:
+                    continue
+                assert abs(F - d) <= F32_DS_ABS, (name, sname, v, F, d)
+                q1, ninf1, F1, abs1, nt1 = blk.nodal_dq_f32(v, s, 1)
+                assert (q1, ninf1) == (q, ninf)
+                assert abs(F1 - q / Q) <= (nt1 + 1) * 2.0 ** -32 + 2.0 ** -40 * abs1, (name, sname, v)
+
+
 def test_merge_application_exact(oracle, ref_fixtures):
     for name in _cases(ref_fixtures):
         for sname, st in ref_fixtures["cases"][name]["states"].items():

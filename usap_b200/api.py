@@ -90,16 +90,25 @@ class Context:
         nat.check(nat.lib().usap_op_entropy(self._h, nat.p32(part), B, dense_max, C.byref(S)))
         return int(S.value)
 
-    def op_merge_phase(self, part, B: int, K: int, stage: int, seed: int):
+    def op_merge_phase(self, part, B: int, K: int, stage: int, seed: int, precision: int = 0):
+        """block_merge task; in precision mode 1 or 2 also returns the FP32 dS
+        of every proposal and the number of blocks whose choice flipped."""
         part = np.ascontiguousarray(part, np.int32)
         best_s = np.empty(B, np.int32)
         best_q = np.empty(B, np.int64)
         ps = np.empty(B * K, np.int32)
         pq = np.empty(B * K, np.int64)
-        nat.check(nat.lib().usap_op_merge_phase(self._h, nat.p32(part), B, K, stage, seed,
-                                                nat.p32(best_s), nat.p64(best_q), nat.p32(ps),
-                                                nat.p64(pq)))
-        return best_s, best_q, ps.reshape(B, K), pq.reshape(B, K)
+        if not precision:
+            nat.check(nat.lib().usap_op_merge_phase(self._h, nat.p32(part), B, K, stage, seed,
+                                                    nat.p32(best_s), nat.p64(best_q), nat.p32(ps),
+                                                    nat.p64(pq)))
+            return best_s, best_q, ps.reshape(B, K), pq.reshape(B, K)
+        pf = np.empty(B * K, np.float64)
+        flips = C.c_int64()
+        nat.check(nat.lib().usap_op_merge_phase_prec(self._h, nat.p32(part), B, K, stage, seed, precision,
+                                                     nat.p32(best_s), nat.p64(best_q), nat.p32(ps),
+                                                     nat.p64(pq), nat.pf64(pf), C.byref(flips)))
+        return best_s, best_q, ps.reshape(B, K), pq.reshape(B, K), pf.reshape(B, K), int(flips.value)
 
     def op_merge_apply(self, part, B: int, best_s, best_q, b_to_merge: int):
         part = np.ascontiguousarray(part, np.int32).copy()
@@ -113,7 +122,9 @@ class Context:
         return part, int(Bn.value), int(merged.value)
 
     def op_nodal_batch(self, part, B: int, beg: int, end: int, itr: int, stage: int, seed: int,
-                       dense_max: int = 4096):
+                       dense_max: int = 4096, precision: int = 0):
+        """one nodal batch; in precision mode 1 or 2 the accept decisions are
+        taken on the FP32 dS, returned as prop_f beside the exact prop_q."""
         part = np.ascontiguousarray(part, np.int32).copy()
         cnt = end - beg
         ps = np.empty(cnt, np.int32)
@@ -122,12 +133,22 @@ class Context:
         cq = C.c_int64()
         cn = C.c_int32()
         mv = C.c_int64()
-        nat.check(nat.lib().usap_op_nodal_batch(self._h, nat.p32(part), B, dense_max, beg, end,
-                                                itr, stage, seed, nat.p32(ps), nat.p64(pq),
-                                                nat.p32(pn), C.byref(cq), C.byref(cn),
-                                                C.byref(mv)))
-        return part, {"prop_s": ps, "prop_q": pq, "prop_ninf": pn, "cum_q": int(cq.value),
-                      "cum_ninf": int(cn.value), "moves": int(mv.value)}
+        if not precision:
+            nat.check(nat.lib().usap_op_nodal_batch(self._h, nat.p32(part), B, dense_max, beg, end,
+                                                    itr, stage, seed, nat.p32(ps), nat.p64(pq),
+                                                    nat.p32(pn), C.byref(cq), C.byref(cn),
+                                                    C.byref(mv)))
+            return part, {"prop_s": ps, "prop_q": pq, "prop_ninf": pn, "cum_q": int(cq.value),
+                          "cum_ninf": int(cn.value), "moves": int(mv.value)}
+        pf = np.empty(cnt, np.float64)
+        flips = C.c_int64()
+        nat.check(nat.lib().usap_op_nodal_batch_prec(self._h, nat.p32(part), B, dense_max, beg, end,
+                                                     itr, stage, seed, precision, nat.p32(ps), nat.p64(pq),
+                                                     nat.pf64(pf), nat.p32(pn), C.byref(cq),
+                                                     C.byref(cn), C.byref(mv), C.byref(flips)))
+        return part, {"prop_s": ps, "prop_q": pq, "prop_f": pf, "prop_ninf": pn,
+                      "cum_q": int(cq.value), "cum_ninf": int(cn.value), "moves": int(mv.value),
+                      "flips": int(flips.value)}
 
 
 def partition(src, dst, weight=None, n: int = 0, one_based: bool = False,

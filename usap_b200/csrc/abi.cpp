@@ -358,4 +358,29 @@ usap_status usap_op_nodal_batch(usap_ctx* ctx, int32_t* part, int32_t B, int32_t
   });
 }
 
+usap_status usap_op_merge_phase_prec(usap_ctx* ctx, const int32_t* part, int32_t B, int32_t K,
+                                     int32_t stage, uint64_t seed, int32_t precision, int32_t* best_s,
+                                     int64_t* best_q, int32_t* prop_s, int64_t* prop_q, double* prop_f,
+                                     int64_t* flips) {
+  return guarded([&] {
+    check_ctx(ctx);
+    check_part(ctx, part, B);
+    if (!best_s || !best_q) throw usap::Error(USAP_ERR_INVALID, "null output");
+    ctx->job->op_merge_phase(part, B, K, stage, seed, best_s, best_q, prop_s, prop_q, precision, prop_f, flips);
+  });
+}
+
+usap_status usap_op_nodal_batch_prec(usap_ctx* ctx, int32_t* part, int32_t B, int32_t dense_max,
+                                     int32_t beg, int32_t end, int32_t itr, int32_t stage,
+                                     uint64_t seed, int32_t precision, int32_t* prop_s, int64_t* prop_q,
+                                     double* prop_f, int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
+                                     int64_t* moves, int64_t* flips) {
+  return guarded([&] {
+    check_ctx(ctx);
+    check_part(ctx, part, B);
+    ctx->job->op_nodal_batch(part, B, dense_max > 0 ? dense_max : 4096, beg, end, itr, stage, seed,
+                             prop_s, prop_q, prop_ninf, cum_q, cum_ninf, moves, precision, prop_f, flips);
+  });
+}
+
 }  // extern "C"

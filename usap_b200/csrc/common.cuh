@@ -19,6 +19,14 @@ constexpr uint32_t kTagNodal = 0x4E4F4441u;  // 'NODA'
 constexpr double kQ32 = 4294967296.0;
 constexpr long long kNearQ = 4;              // |dS| <= 1e-9 in Q32 units
 
+// statistics of precision modes 1 and 2 (FP32 dS beside the exact FP64 value):
+// evaluations, decisions whose sign differs, the largest and the summed
+// |dS_fp32 - dS_fp64|
+struct F32Tally {
+  unsigned long long evals, flips, err_max;   // err_max: bits of a non-negative double
+  double err_sum;
+};
+
 struct Draws {
   uint32_t x0, x1, x2, x3;
 };
@@ -98,6 +106,115 @@ __device__ __forceinline__ double h_term(const double* __restrict__ L, long long
 
 __device__ __forceinline__ long long q32(double t) {
   return __double2ll_rn(__dmul_rn(t, kQ32));
+}
+
+// --- FP32 evaluation of the same terms (precision modes 1 and 2) --------
+// Only single-precision operations, each rounded to nearest as written.
+// Values are float pairs (hi, lo) worth hi + lo, |lo| <= ulp(hi) / 2.  The
+// log table is held as such pairs too: hi = log k rounded to float, lo = the
+// remainder rounded to float.
+//  * mode 1: every term in pair arithmetic (Dekker / Knuth error-free
+//    transformations: TwoSum, and TwoProduct by fused multiply-add), about
+//    44 significant bits;
+//  * mode 2: every term in plain float from the hi parts; only the sum is
+//    compensated.
+// Terms are accumulated in pairs in both modes.
+struct FF {
+  float hi, lo;
+};
+
+// a + b = s + e exactly (TwoSum; needs no ordering of a, b)
+__device__ __forceinline__ FF two_sum(float a, float b) {
+  const float s = __fadd_rn(a, b);
+  const float z = __fsub_rn(s, a);
+  return FF{s, __fadd_rn(__fsub_rn(a, __fsub_rn(s, z)), __fsub_rn(b, z))};
+}
+
+// pair sum; the result does not depend on the operands' order, so every
+// lane of a butterfly reduction ends with the same value
+__device__ __forceinline__ FF ff_add(FF a, FF b) {
+  const FF s = two_sum(a.hi, b.hi);
+  return two_sum(s.hi, __fadd_rn(s.lo, __fadd_rn(a.lo, b.lo)));
+}
+
+__device__ __forceinline__ FF ff_neg(FF a) { return FF{-a.hi, -a.lo}; }
+__device__ __forceinline__ FF ff_sub(FF a, FF b) { return ff_add(a, ff_neg(b)); }
+
+// the integer x (|x| < 2^48) times a pair: x = xh + xl in floats, xh * d.hi
+// split exactly by a fused multiply-add, the cross terms added to the error
+__device__ __forceinline__ FF ff_mul_ll(FF d, long long x) {
+  const float xh = __ll2float_rn(x);
+  const float xl = __ll2float_rn(x - __float2ll_rn(xh));
+  const float p = __fmul_rn(xh, d.hi);
+  float e = __fmaf_rn(xh, d.hi, -p);
+  e = __fadd_rn(e, __fadd_rn(__fmul_rn(xh, d.lo), __fmul_rn(xl, d.hi)));
+  return two_sum(p, e);
+}
+
+// the exact value hi + lo (at most 48 significant bits, so exact in FP64)
+__device__ __forceinline__ double ff_value(FF a) {
+  return __dadd_rn(static_cast<double>(a.hi), static_cast<double>(a.lo));
+}
+
+__device__ __forceinline__ FF ld_ff(const float2* __restrict__ T, long long k) {
+  const float2 v = __ldg(T + k);
+  return FF{v.x, v.y};
+}
+
+// x * ((L[x] - L[d1]) - L[d2]) from loaded table pairs
+template <int P>
+__device__ __forceinline__ FF g_ff(long long x, FF Lx, FF L1, FF L2) {
+  if (x == 0) return FF{0.0f, 0.0f};
+  if constexpr (P == 1) return ff_mul_ll(ff_sub(ff_sub(Lx, L1), L2), x);
+  return FF{__fmul_rn(__ll2float_rn(x), __fsub_rn(__fsub_rn(Lx.hi, L1.hi), L2.hi)), 0.0f};
+}
+
+template <int P>
+__device__ __forceinline__ FF g_term_ff(const float2* __restrict__ T, long long x, long long din_arg,
+                                        long long dout_arg) {
+  if (x == 0) return FF{0.0f, 0.0f};
+  return g_ff<P>(x, ld_ff(T, x), ld_ff(T, din_arg), ld_ff(T, dout_arg));
+}
+
+// n * (L[a_new] - L[a_old])
+template <int P>
+__device__ __forceinline__ FF coef_ff(long long n, FF Lnew, FF Lold) {
+  if (n == 0) return FF{0.0f, 0.0f};
+  if constexpr (P == 1) return ff_mul_ll(ff_sub(Lnew, Lold), n);
+  return FF{__fmul_rn(__ll2float_rn(n), __fsub_rn(Lnew.hi, Lold.hi)), 0.0f};
+}
+
+// x L[x] + y L[y] - (x+y) L[x+y]
+template <int P>
+__device__ __forceinline__ FF h_term_ff(const float2* __restrict__ T, long long x, long long y) {
+  const FF Lx = ld_ff(T, x), Ly = ld_ff(T, y), Lxy = ld_ff(T, x + y);
+  if constexpr (P == 1) return ff_sub(ff_add(ff_mul_ll(Lx, x), ff_mul_ll(Ly, y)), ff_mul_ll(Lxy, x + y));
+  const float a = __fmul_rn(__ll2float_rn(x), Lx.hi);
+  const float b = __fmul_rn(__ll2float_rn(y), Ly.hi);
+  const float c = __fmul_rn(__ll2float_rn(x + y), Lxy.hi);
+  return FF{__fsub_rn(__fadd_rn(a, b), c), 0.0f};
+}
+
+// |dS_fp32 - dS_fp64| of one evaluation; f is the FP32 pair's value, the
+// FP64 value is the exact sum acc / 2^32
+__device__ __forceinline__ double f32_err(double f, long long acc) {
+  return fabs(__dsub_rn(f, __dmul_rn(static_cast<double>(acc), 1.0 / kQ32)));
+}
+
+__device__ __forceinline__ void f32_tally(F32Tally* t, double f, long long acc) {
+  const double err = f32_err(f, acc);
+  atomicAdd(&t->evals, 1ull);
+  if ((acc < 0) != (f < 0.0)) atomicAdd(&t->flips, 1ull);
+  atomicMax(&t->err_max, static_cast<unsigned long long>(__double_as_longlong(err)));
+  atomicAdd(&t->err_sum, err);
+}
+
+__device__ __forceinline__ void f32_tally_flush(const F32Tally* t, F32Tally* dst) {
+  if (!t->evals) return;
+  atomicAdd(&dst->evals, t->evals);
+  if (t->flips) atomicAdd(&dst->flips, t->flips);
+  atomicMax(&dst->err_max, t->err_max);
+  atomicAdd(&dst->err_sum, t->err_sum);
 }
 
 // --- warp helpers ------------------------------------------------------------

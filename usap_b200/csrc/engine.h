@@ -18,6 +18,8 @@
 #include <cstdint>
 #include <functional>
 #include <memory>
+
+#include "common.cuh"
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -147,6 +149,7 @@ struct NodalCtl {
   int bar_err;
   unsigned int vnext;
   int gang_batch;           // gang launches: next batch of the current sweep (0: a new sweep starts)
+  F32Tally f32;             // precision mode 1: FP32 decisions against the FP64 values
 };
 
 struct GraphDev {
@@ -164,6 +167,7 @@ struct GraphDev {
   int64_t* chunk_ptr = nullptr;   // first chunk of each vertex (n + 1)
   int32_t *kout = nullptr, *kin = nullptr;
   double* logk = nullptr;
+  float2* logk2 = nullptr;   // the same table as float pairs (hi, lo) for the FP32 precision modes
   // per-vertex global hash region for vertices too large for shared memory
   int64_t* hi_off = nullptr;
   int64_t hi_slots = 0;
@@ -186,20 +190,29 @@ struct NodalArgs {
   int32_t* prop_s;        // optional, [end-beg]
   long long* prop_q;
   int32_t* prop_ninf;
+  double* prop_f;         // optional: FP32 dS, the float pair's exact value (precision modes 1, 2)
   NodalCtl* ctl;
   const int64_t* hi_off;
   int32_t *hkey, *hwo, *hwi;
   int stats;
+  int prec;               // precision mode: 0 FP64; 1, 2 decide on the FP32 dS
+  const float2* L2;       // the log table as float pairs (precision modes 1, 2)
 };
 
 struct MergeArgs {
   const double* L;
+  const float2* L2;  // the log table as float pairs
+  int prec;          // precision mode
   int B, K;
   uint32_t stage;
   uint64_t seed;
   const int32_t *dout, *din;
   int32_t* prop_s;   // [B*K]
-  long long* prop_q;
+  long long* prop_q; // the merge key: exact FP64 dS in Q32, or in precision modes 1, 2 the FP32 dS in Q32
+  // precision modes 1, 2 only: the exact FP64 dS (Q32), the FP32 dS, the statistics
+  long long* prop_x;
+  double* prop_f;
+  F32Tally* f32;
 };
 
 // Arguments of the persistent nodal-phase kernel (dense tile only).
@@ -235,6 +248,7 @@ void launch_dense_build(const GraphDev& g, const int32_t* part, int B, int ld, i
                         cudaStream_t st);
 void launch_degrees(const GraphDev& g, const int32_t* part, int B, int32_t* dout, int32_t* din,
                     cudaStream_t st);
+void launch_log_pairs(const double* L, float2* T, int64_t n, cudaStream_t st);
 void launch_entropy_dense(const GraphDev& g, DenseView v, int B, const int32_t* dout,
                           const int32_t* din, unsigned long long* acc, cudaStream_t st);
 void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, int64_t max_nnz,
@@ -242,8 +256,11 @@ void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, 
                            unsigned long long* acc, cudaStream_t st);
 
 void launch_merge_propose(const GraphDev& g, SortedView v, const MergeArgs& a, cudaStream_t st);
-void launch_merge_argmin(int B, int K, const int32_t* prop_s, const long long* prop_q,
-                         int32_t* best_s, long long* best_q, cudaStream_t st);
+// prop_x / best_x / f32: precision modes 1, 2 only (else null)
+void launch_merge_argmin(int B, int K, const int32_t* prop_s, const long long* prop_q, const long long* prop_x,
+                         int32_t* best_s, long long* best_q, long long* best_x, F32Tally* f32, cudaStream_t st);
+void launch_order_flips(int B, const int32_t* order, const long long* best_x, unsigned long long* count,
+                        cudaStream_t st);
 void launch_merge_union(int B, const int32_t* order, const int32_t* best_s, int btm,
                         int32_t* work, int32_t* root, int32_t* merged, cudaStream_t st);
 void launch_merge_relabel(int n, int B, int32_t* part, const int32_t* root, int32_t* present,
@@ -258,7 +275,9 @@ int nodal_phase_max_blocks();
 void launch_nodal_phase(const PhaseArgs& p, int grid, cudaStream_t st);
 // nodal phases of K <= kGangMax jobs (PhaseArgs array in device memory)
 // (the launch ends once fewer than exit_below jobs are unfinished)
-void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_below, int grid, cudaStream_t st);
+// (prec: every job's precision mode)
+void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_below, int grid, int prec,
+                       cudaStream_t st);
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
                                 const StreamPair& sp);
 void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,

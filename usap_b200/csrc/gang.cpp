@@ -77,9 +77,18 @@ void NodalGang::run(const PhaseArgs& pa, cudaStream_t job_stream) {
   while (!me.done) {
     if (ready_to_launch()) {
       busy_ = true;
-      const size_t k = std::min<size_t>(pending_.size(), kGangMax);
-      std::vector<Pending*> batch(pending_.begin(), pending_.begin() + static_cast<long>(k));
-      pending_.erase(pending_.begin(), pending_.begin() + static_cast<long>(k));
+      // one launch runs phases of one precision mode: the oldest's, and
+      // the others of that mode in arrival order
+      const int mode = pending_.front()->pa.a.prec;
+      std::vector<Pending*> batch;
+      for (auto it = pending_.begin(); it != pending_.end() && batch.size() < static_cast<size_t>(kGangMax);) {
+        if ((*it)->pa.a.prec == mode) {
+          batch.push_back(*it);
+          it = pending_.erase(it);
+        } else {
+          ++it;
+        }
+      }
       lk.unlock();
       std::string err;
       try {
@@ -125,7 +134,7 @@ void NodalGang::launch(const std::vector<Pending*>& batch) {
   USAP_CUDA(cudaMemcpyAsync(d_jobs_, h_jobs_, sizeof(PhaseArgs) * K, cudaMemcpyHostToDevice, st_));
   USAP_CUDA(cudaMemsetAsync(d_ctl_, 0, sizeof(GangCtl), st_));
   const int done_to_exit = std::max(1, static_cast<int>(kGangExitFrac * K + 0.5));
-  launch_nodal_gang(d_jobs_, K, d_ctl_, K - done_to_exit + 1, grid_, st_);
+  launch_nodal_gang(d_jobs_, K, d_ctl_, K - done_to_exit + 1, grid_, h_jobs_[0].a.prec, st_);
   USAP_CUDA(cudaMemcpyAsync(h_ctl_, d_ctl_, sizeof(GangCtl), cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
   launches_++;

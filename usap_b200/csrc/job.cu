@@ -143,6 +143,7 @@ Job::Job(int device) : device_(device) {
   USAP_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_ring_), 2 * sizeof(NodalCtl)));
   for (auto& e : ev_sweep_) USAP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   dalloc(&ctl_, 1);
+  dalloc(&f32d_, 2);
 }
 
 Job::~Job() {
@@ -150,6 +151,7 @@ Job::~Job() {
   free_state();
   free_graph();
   dfree(ctl_);
+  dfree(f32d_);
   if (st_) cudaStreamSynchronize(st_);
   if (h_ctl_) cudaFreeHost(h_ctl_);
   if (h_ring_) cudaFreeHost(h_ring_);
@@ -188,13 +190,13 @@ void Job::free_state() {
   batch_hub_cap_ = 0;
   dfree(M_); dfree(Mt_); dfree(CS_);
   sb_.release(st_);
-  dfree(prop_s_); dfree(prop_q_); dfree(best_s_); dfree(best_q_);
+  dfree(prop_s_); dfree(prop_q_); dfree(prop_x_); dfree(prop_f_); dfree(best_s_); dfree(best_q_); dfree(best_x_);
   dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
   dfree(union_work_); dfree(root_); dfree(present_); dfree(newlabel_); dfree(merged_dev_);
   dfree(cub_tmp_);
   cub_bytes_ = 0;
   dfree(ide_q_); dfree(ide_n_);
-  dfree(rp_s_); dfree(rp_n_); dfree(rp_q_);
+  dfree(rp_s_); dfree(rp_n_); dfree(rp_q_); dfree(rp_f_);
   bcap_ = kcap_ = dcap_ = icap_ = 0;
 }
 
@@ -330,6 +332,8 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   }
   dalloc(&g.logk, wtot + 1);
   USAP_CUDA(cudaMemcpyAsync(g.logk, logk_all->data(), sizeof(double) * (wtot + 1), cudaMemcpyHostToDevice, st_));
+  dalloc(&g.logk2, wtot + 1);
+  launch_log_pairs(g.logk, g.logk2, wtot + 1, st_);
   dalloc(&g.hi_off, n);
   USAP_CUDA(cudaMemcpyAsync(g.hi_off, hi_off.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st_));
   up_bytes += static_cast<long long>(sizeof(double) * (wtot + 1) + sizeof(int64_t) * n +
@@ -364,7 +368,7 @@ GraphResident::~GraphResident() {
   dfree(g.out_ptr); dfree(g.out_idx); dfree(g.out_w);
   dfree(g.in_ptr); dfree(g.in_idx); dfree(g.in_w);
   dfree(g.chunks); dfree(g.chunk_ptr);
-  dfree(g.kout); dfree(g.kin); dfree(g.logk);
+  dfree(g.kout); dfree(g.kin); dfree(g.logk); dfree(g.logk2);
   dfree(g.hi_off);
   dfree(hubs_dev);
   if (st) {
@@ -429,15 +433,17 @@ void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxit
     dalloc(&rp_s_, n);
     dalloc(&rp_n_, n);
     dalloc(&rp_q_, n);
+    dalloc(&rp_f_, n);
   }
   if (B > bcap_) {
-    dfree(dout_); dfree(din_); dfree(best_s_); dfree(best_q_);
+    dfree(dout_); dfree(din_); dfree(best_s_); dfree(best_q_); dfree(best_x_);
     dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
     dfree(union_work_); dfree(root_); dfree(present_); dfree(newlabel_); dfree(merged_dev_);
     dalloc(&dout_, B);
     dalloc(&din_, B);
     dalloc(&best_s_, B);
     dalloc(&best_q_, B);
+    dalloc(&best_x_, B);
     dalloc(&skeys_, B);
     dalloc(&skeys_alt_, B);
     dalloc(&sidx_, B);
@@ -460,8 +466,12 @@ void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxit
   if (static_cast<int64_t>(B) * K > static_cast<int64_t>(bcap_) * kcap_) {
     dfree(prop_s_);
     dfree(prop_q_);
+    dfree(prop_x_);
+    dfree(prop_f_);
     dalloc(&prop_s_, static_cast<size_t>(bcap_) * K);
     dalloc(&prop_q_, static_cast<size_t>(bcap_) * K);
+    dalloc(&prop_x_, static_cast<size_t>(bcap_) * K);
+    dalloc(&prop_f_, static_cast<size_t>(bcap_) * K);
     kcap_ = K;
   }
   int32_t dneed = std::min(B, dense_max);
@@ -511,8 +521,13 @@ void Job::merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage,
   a.din = din_;
   a.prop_s = prop_s_;
   a.prop_q = prop_q_;
+  a.L2 = g_.logk2;
+  a.prec = prec_;
+  a.prop_x = prec_ ? prop_x_ : nullptr;
+  a.prop_f = prec_ ? prop_f_ : nullptr;
+  a.f32 = prec_ ? f32d_ : nullptr;
   launch_merge_propose(g_, sb_.view(), a, st_);
-  launch_merge_argmin(B, K, prop_s_, prop_q_, best_s_, best_q_, st_);
+  launch_merge_argmin(B, K, prop_s_, prop_q_, a.prop_x, best_s_, best_q_, prec_ ? best_x_ : nullptr, a.f32, st_);
 }
 
 int32_t Job::merge_apply(int32_t* part, int32_t B, int32_t btm) {
@@ -565,16 +580,20 @@ NodalArgs Job::nodal_args(int32_t* part, int32_t B, int32_t beg, int32_t end, ui
   a.prop_s = nullptr;
   a.prop_q = nullptr;
   a.prop_ninf = nullptr;
+  a.prop_f = nullptr;
   a.ctl = ctl_;
   a.hi_off = g_.hi_off;
   a.hkey = g_.hkey;
   a.hwo = g_.hwo;
   a.hwi = g_.hwi;
   a.stats = stats;
+  a.prec = prec_;
+  a.L2 = g_.logk2;
   if (stats == 2) {   // replay: per-vertex proposals
     a.prop_s = rp_s_;
     a.prop_q = rp_q_;
     a.prop_ninf = rp_n_;
+    a.prop_f = rp_f_;
   }
   return a;
 }
@@ -802,6 +821,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   if (p.delta_entropy_moving_avg_window < 1) throw Error(USAP_ERR_INVALID, "moving average window must be >= 1");
   if (!(p.num_block_reduction_rate > 0.0f && p.num_block_reduction_rate < 1.0f))
     throw Error(USAP_ERR_INVALID, "num_block_reduction_rate must be in (0, 1)");
+  if (p.precision < 0 || p.precision > 2) throw Error(USAP_ERR_INVALID, "precision must be 0, 1 or 2");
   const int dense_max = p.dense_max > 0 ? p.dense_max : 4096;
   auto t_start = std::chrono::steady_clock::now();
   std::memset(res, 0, sizeof(*res));
@@ -817,6 +837,9 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   ev_used_ = 0;
   const LaunchCount lc0 = launch_count();
   long long d2h = 0;
+  prec_ = p.precision;
+  F32Tally nodal32{0, 0, 0, 0.0};   // summed over the stages' nodal phases
+  if (prec_) USAP_CUDA(cudaMemsetAsync(f32d_, 0, 2 * sizeof(F32Tally), st_));
 
   // initial blocks (host): depth-limited DFS on the transpose, or identity
   std::vector<int32_t> part0(n);
@@ -847,6 +870,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     // merge phase and its application
     merge_phase(part, B, K, stage, seed);
     int32_t merged = merge_apply(part, B, btm);
+    if (prec_) launch_order_flips(B, sidx_alt_, best_x_, &f32d_[1].flips, st_);
     d2h += sizeof(int32_t);
     if (merged < btm) res->merge_shortfall += btm - merged;
     B -= merged;
@@ -975,6 +999,13 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     res->nodal_proposals += static_cast<int64_t>(h_ctl_->proposals);
     res->nodal_moves += static_cast<int64_t>(h_ctl_->moves);
     res->near_threshold += static_cast<int64_t>(h_ctl_->near);
+    if (prec_) {
+      const F32Tally& t = h_ctl_->f32;
+      nodal32.evals += t.evals;
+      nodal32.flips += t.flips;
+      nodal32.err_max = std::max(nodal32.err_max, t.err_max);   // bits of non-negative doubles order as integers
+      nodal32.err_sum += t.err_sum;
+    }
     res->edge_visits += static_cast<int64_t>(h_ctl_->edge_visits);
     res->nodal_kernel_bytes += static_cast<double>(h_ctl_->bytes);
     // description length of the finished stage
@@ -1022,6 +1053,25 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
     USAP_CUDA(cudaMemcpyAsync(slots_[next], slots_[restore], sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st_));
     B = restore == gs.large.slot ? gs.large.B : gs.med.B;
     work = next;
+  }
+  if (prec_) {
+    F32Tally m[2];
+    USAP_CUDA(cudaMemcpyAsync(m, f32d_, sizeof(m), cudaMemcpyDeviceToHost, st_));
+    wait();
+    d2h += sizeof(m);
+    auto as_double = [](unsigned long long bits) {
+      double d;
+      std::memcpy(&d, &bits, sizeof(d));
+      return d;
+    };
+    res->fp32_nodal_evals = static_cast<int64_t>(nodal32.evals);
+    res->fp32_nodal_flips = static_cast<int64_t>(nodal32.flips);
+    res->fp32_merge_evals = static_cast<int64_t>(m[0].evals);
+    res->fp32_merge_flips = static_cast<int64_t>(m[0].flips);
+    res->fp32_order_flips = static_cast<int64_t>(m[1].flips);
+    res->fp32_flip_rate = nodal32.evals ? static_cast<double>(nodal32.flips) / static_cast<double>(nodal32.evals) : 0.0;
+    res->fp32_err_max = std::max(as_double(nodal32.err_max), as_double(m[0].err_max));
+    res->fp32_err_mean = nodal32.evals ? nodal32.err_sum / static_cast<double>(nodal32.evals) : 0.0;
   }
   res->ms_merge = ms_merge;
   res->ms_nodal = ms_nodal;
@@ -1086,18 +1136,29 @@ int64_t Job::op_entropy(const int32_t* part, int32_t B, int32_t dense_max) {
 }
 
 void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
-                         int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q) {
+                         int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q, int prec,
+                         double* prop_f, int64_t* flips) {
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
   if (K < 1) throw Error(USAP_ERR_INVALID, "K must be >= 1");
   USAP_CUDA(cudaSetDevice(device_));
   ensure_capacity(B, K, 1, 1);
+  if (prec < 0 || prec > 2) throw Error(USAP_ERR_INVALID, "precision must be 0, 1 or 2");
+  prec_ = prec;
+  if (prec_) USAP_CUDA(cudaMemsetAsync(f32d_, 0, 2 * sizeof(F32Tally), st_));
   USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
   merge_phase(slots_[0], B, K, static_cast<uint32_t>(stage), seed);
+  const size_t nk = static_cast<size_t>(B) * K;
   USAP_CUDA(cudaMemcpyAsync(best_s, best_s_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaMemcpyAsync(best_q, best_q_, sizeof(int64_t) * B, cudaMemcpyDeviceToHost, st_));
-  if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, prop_s_, sizeof(int32_t) * B * K, cudaMemcpyDeviceToHost, st_));
-  if (prop_q) USAP_CUDA(cudaMemcpyAsync(prop_q, prop_q_, sizeof(int64_t) * B * K, cudaMemcpyDeviceToHost, st_));
+  if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, prop_s_, sizeof(int32_t) * nk, cudaMemcpyDeviceToHost, st_));
+  if (prop_q)
+    USAP_CUDA(cudaMemcpyAsync(prop_q, prec_ ? prop_x_ : prop_q_, sizeof(int64_t) * nk, cudaMemcpyDeviceToHost, st_));
+  if (prec_ && prop_f) USAP_CUDA(cudaMemcpyAsync(prop_f, prop_f_, sizeof(double) * nk, cudaMemcpyDeviceToHost, st_));
+  F32Tally m{0, 0, 0, 0.0};
+  if (prec_) USAP_CUDA(cudaMemcpyAsync(&m, f32d_, sizeof(m), cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
+  if (flips) *flips = static_cast<int64_t>(m.flips);
+  prec_ = 0;
 }
 
 void Job::op_merge_apply(int32_t* part, int32_t B, const int32_t* best_s, const int64_t* best_q,
@@ -1119,10 +1180,13 @@ void Job::op_merge_apply(int32_t* part, int32_t B, const int32_t* best_s, const 
 
 void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t beg, int32_t end,
                          int32_t itr, int32_t stage, uint64_t seed, int32_t* prop_s, int64_t* prop_q,
-                         int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves) {
+                         int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves, int prec,
+                         double* prop_f, int64_t* flips) {
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
   if (beg < 0 || end > hg_->n || beg > end) throw Error(USAP_ERR_INVALID, "batch range out of bounds");
   USAP_CUDA(cudaSetDevice(device_));
+  if (prec < 0 || prec > 2) throw Error(USAP_ERR_INVALID, "precision must be 0, 1 or 2");
+  prec_ = prec;
   ensure_capacity(B, 1, dense_max, 1);
   USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
   const bool dense = B <= dense_max;
@@ -1137,11 +1201,14 @@ void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t be
   if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, rp_s_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));
   if (prop_q) USAP_CUDA(cudaMemcpyAsync(prop_q, rp_q_, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost, st_));
   if (prop_ninf) USAP_CUDA(cudaMemcpyAsync(prop_ninf, rp_n_, sizeof(int32_t) * cnt, cudaMemcpyDeviceToHost, st_));
+  if (prec_ && prop_f) USAP_CUDA(cudaMemcpyAsync(prop_f, rp_f_, sizeof(double) * cnt, cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
+  prec_ = 0;
   if (cum_q) *cum_q = static_cast<int64_t>(h_ctl_->cum_q);
   if (cum_ninf) *cum_ninf = h_ctl_->cum_ninf;
   if (moves) *moves = static_cast<int64_t>(h_ctl_->moves);
+  if (flips) *flips = static_cast<int64_t>(h_ctl_->f32.flips);
 }
 
 }  // namespace usap

@@ -171,13 +171,17 @@ class Job {
   void op_build(const int32_t* part, int32_t B, int32_t dense_max, int32_t* M, int32_t* dout,
                 int32_t* din);
   int64_t op_entropy(const int32_t* part, int32_t B, int32_t dense_max);
+  // prec: precision mode (1, 2: prop_q then gets the exact values,
+  // prop_f the FP32 ones, *flips the blocks whose FP32 choice differs)
   void op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
-                      int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q);
+                      int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q, int prec = 0,
+                      double* prop_f = nullptr, int64_t* flips = nullptr);
   void op_merge_apply(int32_t* part, int32_t B, const int32_t* best_s, const int64_t* best_q,
                       int32_t btm, int32_t* B_new, int32_t* merged);
   void op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t beg, int32_t end,
                       int32_t itr, int32_t stage, uint64_t seed, int32_t* prop_s, int64_t* prop_q,
-                      int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves);
+                      int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf, int64_t* moves, int prec = 0,
+                      double* prop_f = nullptr, int64_t* flips = nullptr);
 
   double last_h2d_ms() const { return gr_ ? gr_->h2d_ms : 0.0; }
   long long last_h2d_bytes() const { return gr_ ? gr_->h2d_bytes : 0; }
@@ -242,8 +246,15 @@ class Job {
   SortedBuilder sb_;
   int32_t* prop_s_ = nullptr;
   long long* prop_q_ = nullptr;
+  long long* prop_x_ = nullptr;   // precision modes 1, 2: exact merge dS beside the FP32 key in prop_q_
+  double* prop_f_ = nullptr;
   int32_t* best_s_ = nullptr;
   long long* best_q_ = nullptr;
+  long long* best_x_ = nullptr;
+  // precision mode of the current solve; with modes 1, 2: [0] merge
+  // proposals, [1].flips merge-order inversions
+  int prec_ = 0;
+  F32Tally* f32d_ = nullptr;
   unsigned long long *skeys_ = nullptr, *skeys_alt_ = nullptr;
   int32_t *sidx_ = nullptr, *sidx_alt_ = nullptr;
   int32_t *union_work_ = nullptr, *root_ = nullptr, *present_ = nullptr, *newlabel_ = nullptr;
@@ -256,6 +267,7 @@ class Job {
   int* ide_n_ = nullptr;
   int32_t *rp_s_ = nullptr, *rp_n_ = nullptr;   // replay proposal buffers [n]
   long long* rp_q_ = nullptr;
+  double* rp_f_ = nullptr;
   // stats
   std::vector<cudaEvent_t> ev_pool_;
   size_t ev_used_ = 0;

@@ -177,7 +177,27 @@ int key_bits(int B) {
   return bits;
 }
 
+// the log table as float pairs: hi = log k rounded to float, lo = the
+// remainder rounded to float (log 0 = -inf has lo = 0)
+__global__ void k_log_pairs(int64_t n, const double* __restrict__ L, float2* __restrict__ T) {
+  for (int64_t k = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; k < n;
+       k += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double x = L[k];
+    const float hi = __double2float_rn(x);
+    const float lo = isinf(x) ? 0.0f : __double2float_rn(__dsub_rn(x, static_cast<double>(hi)));
+    T[k] = make_float2(hi, lo);
+  }
+}
+
 }  // namespace
+
+void launch_log_pairs(const double* L, float2* T, int64_t n, cudaStream_t st) {
+  if (n <= 0) return;
+  int64_t blocks = (n + kThreads - 1) / kThreads;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_log_pairs<<<static_cast<int>(blocks), kThreads, 0, st>>>(n, L, T);
+  USAP_LAUNCHED();
+}
 
 void launch_dense_build(const GraphDev& g, const int32_t* part, int B, int ld, int* M, int* Mt,
                         cudaStream_t st) {

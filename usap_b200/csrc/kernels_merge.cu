@@ -46,7 +46,25 @@ __device__ __forceinline__ int sym_pick(const SortedView& v, int u, long long t)
   return __ldg(v.symcol + j);
 }
 
+// FP32 pair sum over the warp; every lane gets the same value
+__device__ __forceinline__ FF warp_ffsum(FF f) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    f = ff_add(f, FF{__shfl_xor_sync(0xffffffffu, f.hi, o), __shfl_xor_sync(0xffffffffu, f.lo, o)});
+  return f;
+}
+
+// P (precision mode 1 or 2): dS is also evaluated in FP32 and the merge key
+// (argmin, merge order) is the FP32 value in Q32; the exact value is kept
+// beside it
+template <int P>
 __global__ void __launch_bounds__(kThreads) k_merge_propose(SortedView v, MergeArgs a) {
+  constexpr bool F32 = P > 0;
+  __shared__ F32Tally s_f32;
+  if (F32) {
+    if (threadIdx.x == 0) s_f32 = F32Tally{0, 0, 0, 0.0};
+    __syncthreads();
+  }
   const int lane = threadIdx.x & 31;
   const long long items = static_cast<long long>(a.B) * a.K;
   const long long nwarps = static_cast<long long>(gridDim.x) * kWarps;
@@ -96,6 +114,7 @@ __global__ void __launch_bounds__(kThreads) k_merge_propose(SortedView v, MergeA
     const long long Mrr = __shfl_sync(0xffffffffu, e4, 0), Mrs = __shfl_sync(0xffffffffu, e4, 1);
     const long long Msr = __shfl_sync(0xffffffffu, e4, 2), Mss = __shfl_sync(0xffffffffu, e4, 3);
     long long acc = 0;
+    FF f{0.0f, 0.0f};
     // rows: entries present in both row r and row s (h is symmetric)
     {
       int rlo = __ldg(v.rowptr + r), rhi = __ldg(v.rowptr + r + 1);
@@ -107,7 +126,11 @@ __global__ void __launch_bounds__(kThreads) k_merge_propose(SortedView v, MergeA
         int i = __ldg(v.col + p);
         if (i == r || i == s) continue;
         int q = find_sorted(v.col, olo, ohi, i);
-        if (q >= 0) acc += q32(h_term(a.L, __ldg(v.val + p), __ldg(v.val + q)));
+        if (q >= 0) {
+          const int x = __ldg(v.val + p), y = __ldg(v.val + q);
+          acc += q32(h_term(a.L, x, y));
+          if constexpr (F32) f = ff_add(f, h_term_ff<P>(a.L2, x, y));
+        }
       }
     }
     // columns likewise, through the CSC
@@ -121,16 +144,28 @@ __global__ void __launch_bounds__(kThreads) k_merge_propose(SortedView v, MergeA
         int i = __ldg(v.row + p);
         if (i == r || i == s) continue;
         int q = find_sorted(v.row, olo, ohi, i);
-        if (q >= 0) acc += q32(h_term(a.L, __ldg(v.cval + p), __ldg(v.cval + q)));
+        if (q >= 0) {
+          const int x = __ldg(v.cval + p), y = __ldg(v.cval + q);
+          acc += q32(h_term(a.L, x, y));
+          if constexpr (F32) f = ff_add(f, h_term_ff<P>(a.L2, x, y));
+        }
       }
     }
     acc = warp_sum_ll(acc);
+    if constexpr (F32) f = warp_ffsum(f);
     if (lane == 0) {
       acc += q32(g_term(a.L, Mrr, dr_in, dr_out));
       acc += q32(g_term(a.L, Mrs, ds_in, dr_out));
       acc += q32(g_term(a.L, Msr, dr_in, ds_out));
       acc += q32(g_term(a.L, Mss, ds_in, ds_out));
       acc -= q32(g_term(a.L, Mrr + Mrs + Msr + Mss, ds_in_n, ds_out_n));
+      if constexpr (F32) {
+        f = ff_add(f, g_term_ff<P>(a.L2, Mrr, dr_in, dr_out));
+        f = ff_add(f, g_term_ff<P>(a.L2, Mrs, ds_in, dr_out));
+        f = ff_add(f, g_term_ff<P>(a.L2, Msr, dr_in, ds_out));
+        f = ff_add(f, g_term_ff<P>(a.L2, Mss, ds_in, ds_out));
+        f = ff_sub(f, g_term_ff<P>(a.L2, Mrr + Mrs + Msr + Mss, ds_in_n, ds_out_n));
+      }
       long long Ar, As, Cr, Cs;
       if (s != r) {
         Ar = dr_out - Mrr - Mrs;
@@ -146,28 +181,78 @@ __global__ void __launch_bounds__(kThreads) k_merge_propose(SortedView v, MergeA
       acc += q32(coef_term(a.L, Cr, ds_in_n, dr_in));
       acc += q32(coef_term(a.L, Cs, ds_in_n, ds_in));
       a.prop_s[item] = s;
-      a.prop_q[item] = acc;
+      if constexpr (F32) {
+        const float2* __restrict__ T = a.L2;
+        f = ff_add(f, coef_ff<P>(Ar, ld_ff(T, ds_out_n), ld_ff(T, dr_out)));
+        f = ff_add(f, coef_ff<P>(As, ld_ff(T, ds_out_n), ld_ff(T, ds_out)));
+        f = ff_add(f, coef_ff<P>(Cr, ld_ff(T, ds_in_n), ld_ff(T, dr_in)));
+        f = ff_add(f, coef_ff<P>(Cs, ld_ff(T, ds_in_n), ld_ff(T, ds_in)));
+        const double fv = ff_value(f);
+        a.prop_q[item] = q32(fv);
+        a.prop_x[item] = acc;
+        a.prop_f[item] = fv;
+        const double err = f32_err(fv, acc);
+        atomicAdd(&s_f32.evals, 1ull);
+        atomicMax(&s_f32.err_max, static_cast<unsigned long long>(__double_as_longlong(err)));
+        atomicAdd(&s_f32.err_sum, err);
+      } else {
+        a.prop_q[item] = acc;
+      }
     }
+  }
+  if (F32) {
+    __syncthreads();
+    if (threadIdx.x == 0) f32_tally_flush(&s_f32, a.f32);
   }
 }
 
-// first strict minimum over the K proposals of each block (:363-366)
+// first strict minimum over the K proposals of each block (:363-366).
+// prop_x (precision modes 1, 2): the exact values, whose first strict minimum
+// is found too; a block whose two choices differ counts as a flip, and
+// best_x gets the exact value of the chosen proposal.
 __global__ void k_merge_argmin(int B, int K, const int32_t* __restrict__ prop_s,
-                               const long long* __restrict__ prop_q, int32_t* __restrict__ best_s,
-                               long long* __restrict__ best_q) {
+                               const long long* __restrict__ prop_q, const long long* __restrict__ prop_x,
+                               int32_t* __restrict__ best_s, long long* __restrict__ best_q,
+                               long long* __restrict__ best_x, F32Tally* f32) {
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= B) return;
-  long long bq = LLONG_MAX;
-  int bs = -1;
+  long long bq = LLONG_MAX, xq = LLONG_MAX;
+  int bs = -1, bk = -1, xk = -1;
   for (int k = 0; k < K; k++) {
-    long long q = prop_q[static_cast<long long>(r) * K + k];
+    const long long i = static_cast<long long>(r) * K + k;
+    long long q = prop_q[i];
     if (q < bq) {
       bq = q;
-      bs = prop_s[static_cast<long long>(r) * K + k];
+      bs = prop_s[i];
+      bk = k;
+    }
+    if (prop_x) {
+      const long long x = prop_x[i];
+      if (x < xq) {
+        xq = x;
+        xk = k;
+      }
     }
   }
   best_s[r] = bs;
   best_q[r] = bq;
+  if (prop_x) {
+    best_x[r] = bk >= 0 ? prop_x[static_cast<long long>(r) * K + bk] : LLONG_MAX;
+    if (bk != xk && (bk < 0 || xk < 0 || prop_s[static_cast<long long>(r) * K + bk] !=
+                                             prop_s[static_cast<long long>(r) * K + xk]))
+      atomicAdd(&f32->flips, 1ull);
+  }
+}
+
+// precision modes 1, 2: adjacent pairs of the merge order (sorted by the FP32
+// key) that the exact values would put the other way round
+__global__ void k_order_flips(int B, const int32_t* __restrict__ order, const long long* __restrict__ best_x,
+                              unsigned long long* count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i + 1 >= B) return;
+  const int a = order[i], b = order[i + 1];
+  const long long xa = best_x[a], xb = best_x[b];
+  if (xa > xb || (xa == xb && a > b)) atomicAdd(count, 1ull);
 }
 
 __global__ void k_sort_keys(int B, const long long* __restrict__ best_q,
@@ -288,13 +373,22 @@ void launch_merge_propose(const GraphDev& g, SortedView v, const MergeArgs& a, c
   long long blocks = (items + kWarps - 1) / kWarps;
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (blocks < 1) blocks = 1;
-  k_merge_propose<<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
+  if (a.prec == 1) k_merge_propose<1><<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
+  else if (a.prec == 2) k_merge_propose<2><<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
+  else k_merge_propose<0><<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
   USAP_LAUNCHED();
 }
 
-void launch_merge_argmin(int B, int K, const int32_t* prop_s, const long long* prop_q, int32_t* best_s,
-                         long long* best_q, cudaStream_t st) {
-  k_merge_argmin<<<(B + 255) / 256, 256, 0, st>>>(B, K, prop_s, prop_q, best_s, best_q);
+void launch_merge_argmin(int B, int K, const int32_t* prop_s, const long long* prop_q, const long long* prop_x,
+                         int32_t* best_s, long long* best_q, long long* best_x, F32Tally* f32, cudaStream_t st) {
+  k_merge_argmin<<<(B + 255) / 256, 256, 0, st>>>(B, K, prop_s, prop_q, prop_x, best_s, best_q, best_x, f32);
+  USAP_LAUNCHED();
+}
+
+void launch_order_flips(int B, const int32_t* order, const long long* best_x, unsigned long long* count,
+                        cudaStream_t st) {
+  if (B < 2) return;
+  k_order_flips<<<(B + 255) / 256, 256, 0, st>>>(B, order, best_x, count);
   USAP_LAUNCHED();
 }
 

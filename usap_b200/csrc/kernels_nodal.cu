@@ -35,6 +35,7 @@
 // the non-coherent path is used only for data that no phase writes.
 #include <cmath>
 #include <mutex>
+#include <type_traits>
 
 #include <cooperative_groups.h>
 #include <cooperative_groups/reduce.h>
@@ -90,6 +91,13 @@ struct Grp {
     for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, G);
     return v;
   }
+  // compensated FP32 sum over the group; every lane gets the same value
+  __device__ __forceinline__ FF ffsum(FF f) const {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1)
+      f = ff_add(f, FF{__shfl_xor_sync(mask, f.hi, o, G), __shfl_xor_sync(mask, f.lo, o, G)});
+    return f;
+  }
   template <class T>
   __device__ __forceinline__ T incl_scan(T v) const {
 #pragma unroll
@@ -101,9 +109,12 @@ struct Grp {
   }
 };
 
-template <class LD>
+// P (precision mode 1 or 2): dS is also evaluated in FP32 and decisions
+// are taken on that value; the exact FP64 value is kept beside it.
+template <class LD, int P = 0>
 struct DenseOpsT {
   using Ld = LD;
+  static constexpr int kP = P;
   DenseView v;
   int B;
   __device__ __forceinline__ int get(int x, int y) const {
@@ -170,10 +181,10 @@ struct DenseOpsT {
   }
 };
 
-using DenseOps = DenseOpsT<LdNC>;
-
-struct SortedOps {
+template <int P = 0>
+struct SortedOpsT {
   using Ld = LdNC;
+  static constexpr int kP = P;
   SortedView v;
   int B;
   __device__ __forceinline__ int get(int x, int y) const {
@@ -191,6 +202,9 @@ struct SortedOps {
     return __ldg(v.symcol + j);
   }
 };
+
+using DenseOps = DenseOpsT<LdNC>;
+using SortedOps = SortedOpsT<0>;
 
 __device__ __forceinline__ unsigned hash_slot(int b, int lg) {
   return (static_cast<unsigned>(b) * 0x9E3779B1u) >> (32 - lg);
@@ -284,18 +298,33 @@ __device__ __forceinline__ int propose_target(const NodalArgs& a, const Ops& ops
 struct TermSums {
   long long acc;
   int sXR, sXS, sYR, sYS;
+  FF f;   // FP32 value of the same terms (precision modes 1, 2)
 };
 
 // log of the degrees of r and s before and after the move
 struct DegLogs {
   double r_out, s_out, r_out_n, s_out_n, r_in, s_in, r_in_n, s_in_n;
+  FF fr_out, fs_out, fr_out_n, fs_out_n, fr_in, fs_in, fr_in_n, fs_in_n;   // precision modes 1, 2
 };
 
-__device__ __forceinline__ DegLogs deg_logs(const double* __restrict__ L, long long dr_out, long long dr_in,
-                                            long long ds_out, long long ds_in, long long kout,
-                                            long long kin) {
-  return DegLogs{__ldg(L + dr_out), __ldg(L + ds_out), __ldg(L + dr_out - kout), __ldg(L + ds_out + kout),
-                 __ldg(L + dr_in),  __ldg(L + ds_in),  __ldg(L + dr_in - kin),   __ldg(L + ds_in + kin)};
+template <int P>
+__device__ __forceinline__ DegLogs deg_logs(const NodalArgs& a, long long dr_out, long long dr_in, long long ds_out,
+                                            long long ds_in, long long kout, long long kin) {
+  const double* __restrict__ L = a.L;
+  DegLogs d{__ldg(L + dr_out), __ldg(L + ds_out), __ldg(L + dr_out - kout), __ldg(L + ds_out + kout),
+            __ldg(L + dr_in),  __ldg(L + ds_in),  __ldg(L + dr_in - kin),   __ldg(L + ds_in + kin)};
+  if constexpr (P > 0) {
+    const float2* __restrict__ T = a.L2;
+    d.fr_out = ld_ff(T, dr_out);
+    d.fs_out = ld_ff(T, ds_out);
+    d.fr_out_n = ld_ff(T, dr_out - kout);
+    d.fs_out_n = ld_ff(T, ds_out + kout);
+    d.fr_in = ld_ff(T, dr_in);
+    d.fs_in = ld_ff(T, ds_in);
+    d.fr_in_n = ld_ff(T, dr_in - kin);
+    d.fs_in_n = ld_ff(T, ds_in + kin);
+  }
+  return d;
 }
 
 // g(x, d1, d2) = x * ((L[x] - L[d1]) - L[d2]) from loaded log values,
@@ -307,27 +336,45 @@ __device__ __forceinline__ double g_val(long long x, double Lx, double L1, doubl
 
 // dS terms of one aggregated neighbour block b (b not in {r, s}): v sends
 // wo to b and receives wi from b
+// the four terms of one changed pair of entries: + g(X) + g(Y) - g(X - w) - g(Y + w)
+// (row entries M[r|s, b]: g(x, d_in[b], d_out[r|s]); column entries
+// M[b, r|s]: g(x, d_in[r|s], d_out[b])); b's degree index is D
+template <int P>
+__device__ __forceinline__ void pair_terms(const NodalArgs& a, int X, int Y, int w, int D, const DegLogs& dl,
+                                           bool col, TermSums& ts) {
+  const double* __restrict__ L = a.L;
+  const double LD = __ldg(L + D);
+  const double a0 = col ? dl.r_in : dl.r_out, b0 = col ? dl.s_in : dl.s_out;
+  const double a1 = col ? dl.r_in_n : dl.r_out_n, b1 = col ? dl.s_in_n : dl.s_out_n;
+  const double LX = __ldg(L + X), LY = __ldg(L + Y), LXn = __ldg(L + X - w), LYn = __ldg(L + Y + w);
+  ts.acc += q32(g_val(X, LX, col ? a0 : LD, col ? LD : a0));
+  ts.acc += q32(g_val(Y, LY, col ? b0 : LD, col ? LD : b0));
+  ts.acc -= q32(g_val(X - w, LXn, col ? a1 : LD, col ? LD : a1));
+  ts.acc -= q32(g_val(Y + w, LYn, col ? b1 : LD, col ? LD : b1));
+  if constexpr (P > 0) {
+    const float2* __restrict__ T = a.L2;
+    const FF fD = ld_ff(T, D);
+    const FF fa0 = col ? dl.fr_in : dl.fr_out, fb0 = col ? dl.fs_in : dl.fs_out;
+    const FF fa1 = col ? dl.fr_in_n : dl.fr_out_n, fb1 = col ? dl.fs_in_n : dl.fs_out_n;
+    ts.f = ff_add(ts.f, g_ff<P>(X, ld_ff(T, X), col ? fa0 : fD, col ? fD : fa0));
+    ts.f = ff_add(ts.f, g_ff<P>(Y, ld_ff(T, Y), col ? fb0 : fD, col ? fD : fb0));
+    ts.f = ff_sub(ts.f, g_ff<P>(X - w, ld_ff(T, X - w), col ? fa1 : fD, col ? fD : fa1));
+    ts.f = ff_sub(ts.f, g_ff<P>(Y + w, ld_ff(T, Y + w), col ? fb1 : fD, col ? fD : fb1));
+  }
+}
+
 template <class Ops>
 __device__ __forceinline__ void slot_terms(const NodalArgs& a, const Ops& ops, int r, int s, int b, int wo,
                                            int wi, const DegLogs& dl, TermSums& ts) {
-  const double* __restrict__ L = a.L;
   if (wo > 0) {
     const int R = ops.get(r, b), S = ops.get(s, b);
-    const double LD = __ldg(L + Ops::Ld::ld(a.din + b));
-    ts.acc += q32(g_val(R, __ldg(L + R), LD, dl.r_out));
-    ts.acc += q32(g_val(S, __ldg(L + S), LD, dl.s_out));
-    ts.acc -= q32(g_val(R - wo, __ldg(L + R - wo), LD, dl.r_out_n));
-    ts.acc -= q32(g_val(S + wo, __ldg(L + S + wo), LD, dl.s_out_n));
+    pair_terms<Ops::kP>(a, R, S, wo, Ops::Ld::ld(a.din + b), dl, false, ts);
     ts.sXR += R;
     ts.sXS += S;
   }
   if (wi > 0) {
     const int R = ops.get(b, r), S = ops.get(b, s);
-    const double LD = __ldg(L + Ops::Ld::ld(a.dout + b));
-    ts.acc += q32(g_val(R, __ldg(L + R), dl.r_in, LD));
-    ts.acc += q32(g_val(S, __ldg(L + S), dl.s_in, LD));
-    ts.acc -= q32(g_val(R - wi, __ldg(L + R - wi), dl.r_in_n, LD));
-    ts.acc -= q32(g_val(S + wi, __ldg(L + S + wi), dl.s_in_n, LD));
+    pair_terms<Ops::kP>(a, R, S, wi, Ops::Ld::ld(a.dout + b), dl, true, ts);
     ts.sYR += R;
     ts.sYS += S;
   }
@@ -335,23 +382,16 @@ __device__ __forceinline__ void slot_terms(const NodalArgs& a, const Ops& ops, i
 
 // slot_terms from values already loaded: R = M[r,b], S = M[s,b], Di =
 // d_in[b] (if wo > 0) and Rc = M[b,r], Sc = M[b,s], Do = d_out[b] (if wi > 0)
-__device__ __forceinline__ void slot_terms_vals(const double* __restrict__ L, int R, int S, int Rc, int Sc, int Di,
-                                                int Do, int wo, int wi, const DegLogs& dl, TermSums& ts) {
+template <int P>
+__device__ __forceinline__ void slot_terms_vals(const NodalArgs& a, int R, int S, int Rc, int Sc, int Di, int Do,
+                                                int wo, int wi, const DegLogs& dl, TermSums& ts) {
   if (wo > 0) {
-    const double LD = __ldg(L + Di);
-    ts.acc += q32(g_val(R, __ldg(L + R), LD, dl.r_out));
-    ts.acc += q32(g_val(S, __ldg(L + S), LD, dl.s_out));
-    ts.acc -= q32(g_val(R - wo, __ldg(L + R - wo), LD, dl.r_out_n));
-    ts.acc -= q32(g_val(S + wo, __ldg(L + S + wo), LD, dl.s_out_n));
+    pair_terms<P>(a, R, S, wo, Di, dl, false, ts);
     ts.sXR += R;
     ts.sXS += S;
   }
   if (wi > 0) {
-    const double LD = __ldg(L + Do);
-    ts.acc += q32(g_val(Rc, __ldg(L + Rc), dl.r_in, LD));
-    ts.acc += q32(g_val(Sc, __ldg(L + Sc), dl.s_in, LD));
-    ts.acc -= q32(g_val(Rc - wi, __ldg(L + Rc - wi), dl.r_in_n, LD));
-    ts.acc -= q32(g_val(Sc + wi, __ldg(L + Sc + wi), dl.s_in_n, LD));
+    pair_terms<P>(a, Rc, Sc, wi, Do, dl, true, ts);
     ts.sYR += Rc;
     ts.sYS += Sc;
   }
@@ -361,13 +401,15 @@ __device__ __forceinline__ void slot_terms_vals(const double* __restrict__ L, in
 // lane (lanes 0-11), added to the warp-summed neighbour terms `ts`.  The
 // four new 2x2 terms are subtracted; a -inf among them sets *ninf and is
 // left out of the sum (the reference's dS is then -inf).  Every lane
-// returns the same result.
-template <int G>
-__device__ __forceinline__ long long finalize_grp(const double* __restrict__ L, const Grp<G>& g, const TermSums& ts,
+// returns the same result.  P > 0: `fpart` is this lane's part of the
+// FP32 sum of the neighbour terms; the group's FP32 dS goes to *f.
+template <int G, int P = 0>
+__device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<G>& g, const TermSums& ts,
                                                    long long Rr, long long Rs, long long Sr, long long Ss,
                                                    long long wor, long long wos, long long dr_out,
                                                    long long dr_in, long long ds_out, long long ds_in,
-                                                   long long kout, long long kin, int* ninf) {
+                                                   long long kout, long long kin, int* ninf, FF fpart, double* f) {
+  const double* __restrict__ L = a.L;
   const long long dr_out_n = dr_out - kout, ds_out_n = ds_out + kout;
   const long long dr_in_n = dr_in - kin, ds_in_n = ds_in + kin;
   // g lanes: mult * ((L[i0] - L[i1]) - L[i2]); coefficient lanes: mult * (L[i0] - L[i1])
@@ -398,18 +440,31 @@ __device__ __forceinline__ long long finalize_grp(const double* __restrict__ L, 
   long long q = inf ? 0 : q32(t);
   if (neg) q = -q;
   *ninf = g.any(inf) ? 1 : 0;
+  if constexpr (P > 0) {
+    FF t32{0.0f, 0.0f};
+    if (mult != 0 && !inf) {
+      const FF A = ld_ff(a.L2, i0), Bv = ld_ff(a.L2, i1);
+      t32 = coef ? coef_ff<P>(mult, A, Bv) : g_ff<P>(mult, A, Bv, ld_ff(a.L2, i2));
+    }
+    fpart = ff_add(fpart, neg ? ff_neg(t32) : t32);
+    *f = ff_value(g.ffsum(fpart));
+  }
   return ts.acc + g.sum(q);
 }
 
 // per-vertex outputs of a decided proposal; returns whether it is accepted
-__device__ __forceinline__ bool emit(const NodalArgs& a, int v, int r, int s, long long acc, int ninf) {
-  const bool accept = ninf || acc < 0;
+// (on the FP32 pair's value f in precision modes 1, 2, else on the exact
+// FP64 value acc)
+template <int P>
+__device__ __forceinline__ bool emit(const NodalArgs& a, int v, int r, int s, long long acc, double f, int ninf) {
+  const bool accept = ninf || (P > 0 ? f < 0.0 : acc < 0);
   a.move_to[v] = accept ? s : -1;
   a.from[v] = r;
   if (a.prop_s) {
     a.prop_s[v - a.beg] = s;
     a.prop_q[v - a.beg] = acc;
     a.prop_ninf[v - a.beg] = ninf;
+    if (P > 0 && a.prop_f) a.prop_f[v - a.beg] = f;
   }
   return accept;
 }
@@ -421,23 +476,45 @@ __device__ __forceinline__ void record_stay(const NodalArgs& a, int v, int r) {
     a.prop_s[v - a.beg] = -1;
     a.prop_q[v - a.beg] = 0;
     a.prop_ninf[v - a.beg] = 0;
+    if (a.prop_f) a.prop_f[v - a.beg] = 0.0;
   }
 }
 
 // accepted dS, moves and near-threshold proposals of one CTA, added to the
 // control block once at the end of the kernel
+// (the accepted dS summed for the convergence test is the exact FP64 value
+// in both precision modes)
 struct CtaTally {
   unsigned long long cum, moves, near;
   int ninf;
+  F32Tally f32;
 };
 
-__device__ __forceinline__ void tally(CtaTally* t, bool accept, long long acc, int ninf) {
+template <int P>
+__device__ __forceinline__ void tally(CtaTally* t, bool accept, long long acc, double f, int ninf) {
   if (accept) {
     if (ninf) atomicOr(&t->ninf, 1);
     else atomicAdd(&t->cum, static_cast<unsigned long long>(acc));
     atomicAdd(&t->moves, 1ull);
   }
   if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&t->near, 1ull);
+  if constexpr (P > 0) {
+    if (!ninf) f32_tally(&t->f32, f, acc);
+  }
+}
+
+// the same straight into the control block (one proposal per CTA)
+template <int P>
+__device__ __forceinline__ void tally_ctl(NodalCtl* c, bool accept, long long acc, double f, int ninf) {
+  if (accept) {
+    if (ninf) atomicOr(&c->cum_ninf, 1);
+    else atomicAdd(&c->cum_q, static_cast<unsigned long long>(acc));
+    atomicAdd(&c->moves, 1ull);
+  }
+  if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&c->near, 1ull);
+  if constexpr (P > 0) {
+    if (!ninf) f32_tally(&c->f32, f, acc);
+  }
 }
 
 __device__ __forceinline__ void tally_flush(const CtaTally* t, NodalCtl* ctl) {
@@ -445,6 +522,7 @@ __device__ __forceinline__ void tally_flush(const CtaTally* t, NodalCtl* ctl) {
   if (t->cum) atomicAdd(&ctl->cum_q, t->cum);
   if (t->moves) atomicAdd(&ctl->moves, t->moves);
   if (t->near) atomicAdd(&ctl->near, t->near);
+  f32_tally_flush(&t->f32, &ctl->f32);
 }
 
 // Proposal for one vertex of degree <= 4 * G by a group of G lanes (a
@@ -538,7 +616,7 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
   const long long ds_out = LD::ld(a.dout + s), ds_in = LD::ld(a.din + s);
   int e4 = 0;
   if (g.gl < 4) e4 = ops.get(g.gl < 2 ? r : s, (g.gl & 1) ? s : r);
-  const DegLogs dl = deg_logs(a.L, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
+  const DegLogs dl = deg_logs<Ops::kP>(a, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
   // compact the occupied slots so that each lane takes about one block
   int nlist = 0, noccupied = 0;
   for (int base = 0; base < cap; base += G) {
@@ -580,7 +658,8 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
       }
     }
 #pragma unroll
-    for (int k = 0; k < 2; k++) slot_terms_vals(a.L, R[k], S[k], Rc[k], Sc[k], Di[k], Do[k], wo[k], wi[k], dl, ts);
+    for (int k = 0; k < 2; k++)
+      slot_terms_vals<Ops::kP>(a, R[k], S[k], Rc[k], Sc[k], Di[k], Do[k], wo[k], wi[k], dl, ts);
   }
   ts.acc = g.sum(ts.acc);
   ts.sXR = g.sum(ts.sXR);
@@ -592,10 +671,11 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
   const long long wor = table_lookup_wo(key, two, cap, lg, r);
   const long long wos = table_lookup_wo(key, two, cap, lg, s);
   int ninf;
-  const long long acc = finalize_grp(a.L, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
-                                     vi.kout, vi.kin, &ninf);
+  double f = 0.0;
+  const long long acc = finalize_grp<G, Ops::kP>(a, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out,
+                                                 ds_in, vi.kout, vi.kin, &ninf, ts.f, &f);
   if (g.gl == 0) {
-    tally(tl, emit(a, v, r, s, acc, ninf), acc, ninf);
+    tally<Ops::kP>(tl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
     if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * noccupied + 48 + 8ull * scanned;
   }
   g.sync();
@@ -629,6 +709,7 @@ template <int NW>
 struct HubShared {
   long long acc[NW];
   int sum[5][NW];
+  float fhi[NW], flo[NW];   // FP32 partial sums (precision modes 1, 2)
   int target, scanned;
 };
 
@@ -712,7 +793,7 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
   }
   const long long dr_out = LD::ld(a.dout + r), dr_in = LD::ld(a.din + r);
   const long long ds_out = LD::ld(a.dout + s), ds_in = LD::ld(a.din + s);
-  const DegLogs dl = deg_logs(a.L, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
+  const DegLogs dl = deg_logs<Ops::kP>(a, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
   TermSums ts{0, 0, 0, 0, 0};
   int nocc = 0;
   for (int i = threadIdx.x; i < cap;) {
@@ -741,8 +822,11 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
   ts.sYR = warp_sum_i(ts.sYR);
   ts.sYS = warp_sum_i(ts.sYS);
   nocc = warp_sum_i(nocc);
+  if constexpr (Ops::kP > 0) ts.f = Grp<32>(lane).ffsum(ts.f);
   if (lane == 0) {
     sh->acc[wib] = ts.acc;
+    sh->fhi[wib] = ts.f.hi;
+    sh->flo[wib] = ts.f.lo;
     sh->sum[0][wib] = ts.sXR;
     sh->sum[1][wib] = ts.sXS;
     sh->sum[2][wib] = ts.sYR;
@@ -753,7 +837,9 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
   if (wib == 0) {
     TermSums tot{0, 0, 0, 0, 0};
     int occ = 0;
+    FF fpart{0.0f, 0.0f};
     if (lane < NW) {
+      fpart = FF{sh->fhi[lane], sh->flo[lane]};
       tot.acc = sh->acc[lane];
       tot.sXR = sh->sum[0][lane];
       tot.sXS = sh->sum[1][lane];
@@ -774,16 +860,11 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
     const long long wor = table_lookup_wo(key, two, cap, lg, r);
     const long long wos = table_lookup_wo(key, two, cap, lg, s);
     int ninf;
-    const long long acc = finalize_grp(a.L, Grp<32>(lane), tot, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in,
-                                        vi.kout, vi.kin, &ninf);
+    double f = 0.0;
+    const long long acc = finalize_grp<32, Ops::kP>(a, Grp<32>(lane), tot, Rr, Rs, Sr, Ss, wor, wos, dr_out,
+                                                    dr_in, ds_out, ds_in, vi.kout, vi.kin, &ninf, fpart, &f);
     if (lane == 0) {
-      const bool accept = emit(a, v, r, s, acc, ninf);
-      if (accept) {
-        if (ninf) atomicOr(&a.ctl->cum_ninf, 1);
-        else atomicAdd(&a.ctl->cum_q, static_cast<unsigned long long>(acc));
-        atomicAdd(&a.ctl->moves, 1ull);
-      }
-      if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&a.ctl->near, 1ull);
+      tally_ctl<Ops::kP>(a.ctl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
       if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * occ + 48 + 8ull * sh->scanned;
     }
   }
@@ -1166,12 +1247,33 @@ __device__ __forceinline__ int grid_barrier(CtlT* ctl, unsigned* target, bool pu
 // counter) and an apply pass over the batch's edge chunks, during which
 // one thread runs the batch-end bookkeeping.  Leaves when the convergence
 // test sets `done`.
+// One work unit of the persistent kernels: two vertices of degree <= 64
+// (a half-warp each; un.y = -1 when there is only one) or one vertex of
+// degree <= 128 (the whole warp, un.y = kUnitWarp).  wtab: the warp's
+// shared-memory tables.
+template <class Ops>
+__device__ __forceinline__ void unit_vertices(const NodalArgs& a, const Ops& ops, int2 un, uint32_t itr, int* wtab,
+                                              CtaTally* tl, int lane, unsigned long long* my_bytes) {
+  if (un.y == kUnitWarp) {
+    group_vertex(a, ops, un.x, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap, tl, Grp<32>(lane),
+                 my_bytes);
+  } else {
+    const int h = lane >> 4;
+    const int vv = h ? un.y : un.x;
+    if (vv >= 0)
+      group_vertex(a, ops, vv, itr, wtab + h * (kHCap / 2), wtab + kHCap + h * (kHCap / 2),
+                   wtab + 2 * kHCap + h * (kHCap / 2), wtab + 3 * kHCap + h * (kHubDegree / 2), tl, Grp<16>(lane),
+                   my_bytes);
+  }
+}
+
+template <int P>
 __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   extern __shared__ int dyn[];
   __shared__ CtaTally s_tally;
   __shared__ HubShared<kPWarps> sh;
   __shared__ int s_base, s_state;
-  using Ops = DenseOpsT<LdCG>;
+  using Ops = DenseOpsT<LdCG, P>;
   const Ops ops{p.v, p.a.B};
   NodalCtl* ctl = p.a.ctl;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1227,24 +1329,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       // work units: two vertices of degree <= 64 (a half-warp each) or one
       // of degree <= 128 (a warp)
       const int u_lo = __ldg(p.unit_ptr + bi), nun = __ldg(p.unit_ptr + bi + 1) - u_lo;
-      auto run_unit = [&](int u) {
-        const int2 un = __ldg(p.units + u_lo + u);
-        if (un.y == kUnitWarp) {
-          group_vertex(a, ops, un.x, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap, &s_tally,
-                       Grp<32>(lane), &my_bytes);
-        } else {
-          const int h = lane >> 4;
-          const int vv = h ? un.y : un.x;
-          if (vv >= 0)
-            group_vertex(a, ops, vv, itr, wtab + h * (kHCap / 2), wtab + kHCap + h * (kHCap / 2),
-                         wtab + 2 * kHCap + h * (kHCap / 2), wtab + 3 * kHCap + h * (kHubDegree / 2), &s_tally,
-                         Grp<16>(lane), &my_bytes);
-        }
-      };
       const int first = (gridDim.x - hcta) * kPWarps;   // units handed out without the counter
       if (static_cast<int>(blockIdx.x) >= hcta) {
         const int i = (blockIdx.x - hcta) * kPWarps + wib;
-        if (i < nun) run_unit(i);
+        if (i < nun) unit_vertices(a, ops, __ldg(p.units + u_lo + i), itr, wtab, &s_tally, lane, &my_bytes);
       }
       // the rest in rounds of one unit per warp, kPWarps per counter step
       for (;;) {
@@ -1253,7 +1341,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
         __syncthreads();
         const int i0 = s_base;
         if (i0 >= nun) break;
-        if (i0 + wib < nun) run_unit(i0 + wib);
+        if (i0 + wib < nun) unit_vertices(a, ops, __ldg(p.units + u_lo + i0 + wib), itr, wtab, &s_tally, lane, &my_bytes);
       }
       __syncthreads();
       if (threadIdx.x == 0) tally_flush(&s_tally, ctl);
@@ -1349,6 +1437,7 @@ __device__ __forceinline__ void gang_tables_flush(const DeltaTables& t, const Ph
 // is spent; the launch ends with the last job.  The arithmetic per job is
 // that of k_nodal_phase (same device functions, same order of the integer
 // sums' terms is irrelevant), so each job's result equals its solo solve.
+template <int P>
 __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __restrict__ jobs, int K, GangCtl* gc,
                                                              int exit_below) {
   extern __shared__ int dyn[];
@@ -1357,7 +1446,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
   __shared__ int s_bi[kGangMax], s_sw[kGangMax], s_act[kGangMax], s_nb[kGangMax];
   __shared__ long long s_hp[kGangMax + 1], s_up[kGangMax + 1], s_cp[kGangMax + 1];
   __shared__ int s_base, s_state, s_flag;
-  using Ops = DenseOpsT<LdCG>;
+  using Ops = DenseOpsT<LdCG, P>;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gw = blockIdx.x * kPWarps + wib;
   const int nw = gridDim.x * kPWarps;
@@ -1459,19 +1548,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
       const int j = find_job(s_up, K, u);
       const PhaseArgs& p = jobs[j];
       const int2 un = __ldg(p.units + __ldg(p.unit_ptr + s_bi[j]) + (u - static_cast<int>(s_up[j])));
-      const Ops ops{p.v, p.a.B};
-      const uint32_t itr = static_cast<uint32_t>(s_sw[j]);
-      if (un.y == kUnitWarp) {
-        group_vertex(p.a, ops, un.x, itr, wtab, wtab + kHCap, wtab + 2 * kHCap, wtab + 3 * kHCap, &s_tally[j],
-                     Grp<32>(lane), &unused_bytes);
-      } else {
-        const int hh = lane >> 4;
-        const int vv = hh ? un.y : un.x;
-        if (vv >= 0)
-          group_vertex(p.a, ops, vv, itr, wtab + hh * (kHCap / 2), wtab + kHCap + hh * (kHCap / 2),
-                       wtab + 2 * kHCap + hh * (kHCap / 2), wtab + 3 * kHCap + hh * (kHubDegree / 2), &s_tally[j],
-                       Grp<16>(lane), &unused_bytes);
-      }
+      unit_vertices(p.a, Ops{p.v, p.a.B}, un, static_cast<uint32_t>(s_sw[j]), wtab, &s_tally[j], lane,
+                    &unused_bytes);
     };
     const int hcta = min(H, static_cast<int>(gridDim.x));
     const int first = (gridDim.x - hcta) * kPWarps;
@@ -1592,22 +1670,31 @@ void nodal_configure(int device) {
   if (device < 0 || device >= 64) return;
   std::call_once(once[device], [device] {
     const int smem = static_cast<int>(sizeof(int) * 3 * kHubSmemSlots);
-    USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<DenseOps>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<SortedOps>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    USAP_CUDA(cudaFuncSetAttribute(k_nodal_phase, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(kPSmemBytes)));
-    USAP_CUDA(cudaFuncSetAttribute(k_nodal_gang, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(kPSmemBytes)));
-    int coop = 0, sms = 0, per_sm = 0;
+    const int psmem = static_cast<int>(kPSmemBytes);
+    int coop = 0, sms = 0;
     USAP_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
     USAP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_nodal_phase, kPThreads, kPSmemBytes));
-    g_phase_grid[device] = coop ? per_sm * sms : 0;
-    int per_sm_g = 0;
-    USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_g, k_nodal_gang, kPThreads, kPSmemBytes));
-    g_gang_grid[device] = coop ? per_sm_g * sms : 0;
+    // one grid for every precision mode: the fewest co-resident CTAs
+    int per_phase = 1 << 30, per_gang = 1 << 30;
+    auto configure = [&](auto tag) {
+      constexpr int P = decltype(tag)::value;
+      USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<DenseOpsT<LdNC, P>>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<SortedOpsT<P>>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      USAP_CUDA(cudaFuncSetAttribute(k_nodal_phase<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
+      USAP_CUDA(cudaFuncSetAttribute(k_nodal_gang<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
+      int a = 0, b = 0;
+      USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_nodal_phase<P>, kPThreads, kPSmemBytes));
+      USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_nodal_gang<P>, kPThreads, kPSmemBytes));
+      per_phase = std::min(per_phase, a);
+      per_gang = std::min(per_gang, b);
+    };
+    configure(std::integral_constant<int, 0>{});
+    configure(std::integral_constant<int, 1>{});
+    configure(std::integral_constant<int, 2>{});
+    g_phase_grid[device] = coop ? per_phase * sms : 0;
+    g_gang_grid[device] = coop ? per_gang * sms : 0;
   });
 }
 
@@ -1625,33 +1712,51 @@ int nodal_gang_grid(int device) {
 
 int nodal_phase_max_blocks() { return 2 * kPHubSlots / 4; }
 
-void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_below, int grid, cudaStream_t st) {
+// the cooperative kernels of precision mode `prec` (0, 1, 2)
+static const void* gang_kernel(int prec) {
+  if (prec == 1) return reinterpret_cast<const void*>(k_nodal_gang<1>);
+  if (prec == 2) return reinterpret_cast<const void*>(k_nodal_gang<2>);
+  return reinterpret_cast<const void*>(k_nodal_gang<0>);
+}
+
+static const void* phase_kernel(int prec) {
+  if (prec == 1) return reinterpret_cast<const void*>(k_nodal_phase<1>);
+  if (prec == 2) return reinterpret_cast<const void*>(k_nodal_phase<2>);
+  return reinterpret_cast<const void*>(k_nodal_phase<0>);
+}
+
+void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_below, int grid, int prec,
+                       cudaStream_t st) {
   const PhaseArgs* j = jobs_dev;
   int k = K;
   GangCtl* c = gc;
   int e = exit_below;
   void* kargs[] = {&j, &k, &c, &e};
-  USAP_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_nodal_gang), dim3(grid), dim3(kPThreads),
-                                        kargs, kPSmemBytes, st));
+  const void* fn = gang_kernel(prec);
+  USAP_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPThreads), kargs, kPSmemBytes, st));
   USAP_LAUNCHED();
 }
 
 void launch_nodal_phase(const PhaseArgs& p, int grid, cudaStream_t st) {
   PhaseArgs args = p;
   void* kargs[] = {&args};
-  USAP_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_nodal_phase), dim3(grid), dim3(kPThreads),
-                                        kargs, kPSmemBytes, st));
+  const void* fn = phase_kernel(p.a.prec);
+  USAP_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPThreads), kargs, kPSmemBytes, st));
   USAP_LAUNCHED();
 }
 
 void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& hubs,
                                 const StreamPair& sp) {
-  launch_propose(a, DenseOps{v, a.B}, hubs, sp);
+  if (a.prec == 1) launch_propose(a, DenseOpsT<LdNC, 1>{v, a.B}, hubs, sp);
+  else if (a.prec == 2) launch_propose(a, DenseOpsT<LdNC, 2>{v, a.B}, hubs, sp);
+  else launch_propose(a, DenseOps{v, a.B}, hubs, sp);
 }
 
 void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList& hubs,
                                  const StreamPair& sp) {
-  launch_propose(a, SortedOps{v, a.B}, hubs, sp);
+  if (a.prec == 1) launch_propose(a, SortedOpsT<1>{v, a.B}, hubs, sp);
+  else if (a.prec == 2) launch_propose(a, SortedOpsT<2>{v, a.B}, hubs, sp);
+  else launch_propose(a, SortedOps{v, a.B}, hubs, sp);
 }
 
 void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st) {

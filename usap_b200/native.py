@@ -44,7 +44,7 @@ class Params(C.Structure):
                 ("init_mode", C.c_int32), ("dense_max", C.c_int32), ("device", C.c_int32),
                 ("stats", C.c_int32), ("trace_kinds", C.c_int32), ("sweep_graphs", C.c_int32),
                 ("persistent", C.c_int32), ("persistent_ctas", C.c_int32),
-                ("reserved", C.c_int32 * 2)]
+                ("precision", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class Result(C.Structure):
@@ -57,7 +57,11 @@ class Result(C.Structure):
                 ("ms_nodal_kernel", C.c_double), ("nodal_kernel_launches", C.c_int64),
                 ("nodal_kernel_bytes", C.c_double), ("kernel_launches", C.c_int64),
                 ("cub_calls", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
-                ("sweep_graph_launches", C.c_int64)]
+                ("sweep_graph_launches", C.c_int64),
+                ("fp32_nodal_evals", C.c_int64), ("fp32_nodal_flips", C.c_int64),
+                ("fp32_merge_evals", C.c_int64), ("fp32_merge_flips", C.c_int64),
+                ("fp32_order_flips", C.c_int64), ("fp32_flip_rate", C.c_double),
+                ("fp32_err_max", C.c_double), ("fp32_err_mean", C.c_double)]
 
 
 class Scores(C.Structure):
@@ -110,7 +114,8 @@ EXPORTS = ("usap_version", "usap_last_error", "usap_params_default", "usap_parti
            "usap_evaluate", "usap_ctx_create", "usap_ctx_destroy", "usap_ctx_load",
            "usap_ctx_num_nodes", "usap_ctx_partition", "usap_ctx_set_trace", "usap_op_scc",
            "usap_op_build", "usap_op_entropy", "usap_op_merge_phase", "usap_op_merge_apply",
-           "usap_op_nodal_batch", "usap_batch_partition", "usap_entropy_static",
+           "usap_op_nodal_batch", "usap_op_merge_phase_prec", "usap_op_nodal_batch_prec",
+           "usap_batch_partition", "usap_entropy_static",
            "usap_server_config_default", "usap_server_create", "usap_server_destroy",
            "usap_server_submit", "usap_server_poll", "usap_server_wait", "usap_server_get_stats")
 
@@ -148,6 +153,12 @@ def lib() -> C.CDLL:
     L.usap_op_nodal_batch.argtypes = [C.c_void_p, i32p, C.c_int32, C.c_int32, C.c_int32,
                                       C.c_int32, C.c_int32, C.c_int32, C.c_uint64, i32p, i64p,
                                       i32p, i64p, i32p, i64p]
+    f64p = C.POINTER(C.c_double)
+    L.usap_op_merge_phase_prec.argtypes = [C.c_void_p, i32p, C.c_int32, C.c_int32, C.c_int32,
+                                           C.c_uint64, C.c_int32, i32p, i64p, i32p, i64p, f64p, i64p]
+    L.usap_op_nodal_batch_prec.argtypes = [C.c_void_p, i32p, C.c_int32, C.c_int32, C.c_int32,
+                                           C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, i32p,
+                                           i64p, f64p, i32p, i64p, i32p, i64p, i64p]
     L.usap_batch_partition.argtypes = [C.POINTER(Graph), C.c_int32, C.POINTER(Params),
                                        C.POINTER(BatchJob), C.c_int32, C.c_int32, C.c_int32,
                                        C.POINTER(BatchStats)]
@@ -183,6 +194,10 @@ def p32(a: Optional[np.ndarray]):
 
 def p64(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(i64p)
+
+
+def pf64(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
 
 
 def default_params(**overrides) -> Params:

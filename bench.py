@@ -255,6 +255,42 @@ def served_sample(local_rank: int, jobs: int = 240, rate: float = 50.0, pool: in
             "peak_admitted_mib": st["peak_admitted_bytes"] / 2**20}
 
 
+def precision_sample(ctx, G, local_rank: int, seeds=(0, 1, 2, 3, 4)) -> dict:
+    """Solves of the bench graph in precision modes 0 (FP64), 1 (float-pair
+    FP32) and 2 (plain FP32) for a few seeds: time, B, S, NMI and the FP32
+    modes' flipped decisions and error against the FP64 values."""
+    from usap_b200 import api, native as nat
+    out = {"seeds": list(seeds)}
+    for mode in (0, 1, 2):
+        runs = []
+        for seed in seeds:
+            p = nat.default_params(num_batch_nodal_update=10, seed=seed, precision=mode, device=local_rank)
+            part, r = ctx.partition(p)
+            run = {"ms": r["ms_total"], "B": r["B"], "S": r["S"], "nmi": api.evaluate(G.truth, part)["nmi"],
+                   "sweeps": r["sweeps"]}
+            if mode:
+                run.update({"nodal_evals": r["fp32_nodal_evals"], "nodal_flips": r["fp32_nodal_flips"],
+                            "flip_rate": r["fp32_flip_rate"], "merge_flips": r["fp32_merge_flips"],
+                            "order_flips": r["fp32_order_flips"], "err_max": r["fp32_err_max"],
+                            "err_mean": r["fp32_err_mean"]})
+            runs.append(run)
+        out[f"mode{mode}"] = runs
+    base = out["mode0"]
+    for mode in (1, 2):
+        runs = out[f"mode{mode}"]
+        out[f"mode{mode}_summary"] = {
+            "same_result_as_fp64": sum(1 for a, b in zip(runs, base) if a["S"] == b["S"] and a["B"] == b["B"]),
+            "max_flip_rate": max(r["flip_rate"] for r in runs),
+            "max_err": max(r["err_max"] for r in runs),
+            "median_S_rel_vs_fp64_median": statistics.median(r["S"] for r in runs)
+            / statistics.median(b["S"] for b in base) - 1.0,
+            "median_nmi": statistics.median(r["nmi"] for r in runs),
+            "median_nmi_fp64": statistics.median(b["nmi"] for b in base),
+            "median_ms": statistics.median(r["ms"] for r in runs),
+            "median_ms_fp64": statistics.median(b["ms"] for b in base)}
+    return out
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -391,6 +427,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     except Exception as e:   # reported, not fatal
         ident = {"error": str(e)}
 
+    # --- precision modes: FP32 dS (1: float pairs, 2: plain floats) against FP64,
+    # on the same graph for seeds 0-4; a flipped decision sends a chain
+    # elsewhere, so the modes are compared through the spread over seeds
+    precision = None
+    try:
+        precision = precision_sample(ctx, G, local_rank)
+    except Exception as e:   # reported, not fatal
+        precision = {"error": str(e)}
+
     # --- roofline of the nodal-phase kernel (instrumented, untimed solve)
     _, rs = ctx.partition(solver_params(seed=0, stats=1), want_assign=False)
     peak, peak_kind = hbm_peak()
@@ -455,6 +500,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "batched": batched,
         "served": served,
         "identity_init": ident,
+        "precision": precision,
         "clocks": clk,
         "mcmc_edge_visits_per_s": visits_per_s,
         "B": res["B"], "S": res["S"], "nmi": nmi, "sweeps": res["sweeps"], "stages": res["stages"],

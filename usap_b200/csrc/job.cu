@@ -183,11 +183,19 @@ void Job::free_graph() {
   g_ = GraphDev{};
 }
 
-void Job::free_state() {
+void Job::free_vertex_state() {
   for (auto& s : slots_) dfree(s);
-  dfree(move_to_); dfree(from_); dfree(dout_); dfree(din_); dfree(batch_hub_); dfree(unit_ptr_); dfree(units_);
+  dfree(move_to_); dfree(from_);
+  dfree(rp_s_); dfree(rp_n_); dfree(rp_q_); dfree(rp_f_);
+  ncap_ = 0;
+}
+
+void Job::free_state() {
+  free_vertex_state();
+  dfree(dout_); dfree(din_); dfree(batch_hub_); dfree(unit_ptr_); dfree(units_);
   batch_hub_bs_ = 0;
   batch_hub_cap_ = 0;
+  units_cap_ = 0;
   dfree(M_); dfree(Mt_); dfree(CS_);
   sb_.release(st_);
   dfree(prop_s_); dfree(prop_q_); dfree(prop_x_); dfree(prop_f_); dfree(best_s_); dfree(best_q_); dfree(best_x_);
@@ -196,7 +204,6 @@ void Job::free_state() {
   dfree(cub_tmp_);
   cub_bytes_ = 0;
   dfree(ide_q_); dfree(ide_n_);
-  dfree(rp_s_); dfree(rp_n_); dfree(rp_q_); dfree(rp_f_);
   bcap_ = kcap_ = dcap_ = icap_ = 0;
 }
 
@@ -384,20 +391,26 @@ void Job::load(const usap_graph& in) {
 
 void Job::attach(std::shared_ptr<GraphResident> gr) {
   USAP_CUDA(cudaSetDevice(device_));
-  if (gr_ != gr) {
-    // the hub scratch and per-vertex state depend on the graph
+  const bool other = gr_ != gr;
+  if (other) {
+    // buffers stay allocated across graphs (allocating while other solves
+    // run on the device is slow); only those that no longer fit are
+    // replaced, and the caches built for the previous graph are dropped
     USAP_CUDA(cudaStreamSynchronize(st_));
-    free_state();
-    dfree(hkey_); dfree(hwo_); dfree(hwi_);
+    if (gr->hg.n > ncap_) free_vertex_state();
+    batch_hub_bs_ = 0;
   }
   gr_ = std::move(gr);
   hg_ = &gr_->hg;
   g_ = gr_->g;
-  if (!hkey_) {
-    dalloc(&hkey_, g_.hi_slots);
-    dalloc(&hwo_, g_.hi_slots);
-    dalloc(&hwi_, g_.hi_slots);
+  if (!hkey_ || g_.hi_slots > hcap_) {
+    dfree(hkey_); dfree(hwo_); dfree(hwi_);
+    hcap_ = std::max<int64_t>(g_.hi_slots, 1);
+    dalloc(&hkey_, hcap_);
+    dalloc(&hwo_, hcap_);
+    dalloc(&hwi_, hcap_);
   }
+  if (other && move_to_) USAP_CUDA(cudaMemsetAsync(move_to_, 0xff, sizeof(int32_t) * hg_->n, st_));
   g_.hkey = hkey_;
   g_.hwo = hwo_;
   g_.hwi = hwi_;
@@ -434,7 +447,10 @@ void Job::ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxit
     dalloc(&rp_n_, n);
     dalloc(&rp_q_, n);
     dalloc(&rp_f_, n);
+    ncap_ = n;
   }
+  // the sorted views hold a slot per edge: grow them for a larger graph
+  if (bcap_ > 0) sb_.reserve(hg_->e, bcap_, st_);
   if (B > bcap_) {
     dfree(dout_); dfree(din_); dfree(best_s_); dfree(best_q_); dfree(best_x_);
     dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
@@ -677,10 +693,14 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
       dalloc(&unit_ptr_, nb + 1);
       batch_hub_cap_ = nb + 1;
     }
-    dfree(units_);
-    int32_t* ud = nullptr;
-    dalloc(&ud, std::max<size_t>(un.size(), 2));
-    units_ = reinterpret_cast<int2*>(ud);
+    if (units_cap_ < std::max<size_t>(un.size(), 2)) {
+      dfree(units_);
+      units_cap_ = std::max<size_t>(un.size(), 2);
+      int32_t* ua = nullptr;
+      dalloc(&ua, units_cap_);
+      units_ = reinterpret_cast<int2*>(ua);
+    }
+    int32_t* ud = reinterpret_cast<int32_t*>(units_);
     USAP_CUDA(cudaMemcpyAsync(batch_hub_, bh.data(), sizeof(int32_t) * bh.size(), cudaMemcpyHostToDevice, st_));
     USAP_CUDA(cudaMemcpyAsync(unit_ptr_, up.data(), sizeof(int32_t) * up.size(), cudaMemcpyHostToDevice, st_));
     if (!un.empty())

@@ -189,6 +189,7 @@ class Job {
  private:
   void free_graph();
   void free_state();
+  void free_vertex_state();   // buffers sized by the number of vertices
   void ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxitr);
   // block structures for a nodal phase / batch
   void prepare_nodal_blocks(const int32_t* part, int32_t B, bool dense);
@@ -231,6 +232,9 @@ class Job {
   int32_t *hkey_ = nullptr, *hwo_ = nullptr, *hwi_ = nullptr;
   // state
   int32_t bcap_ = 0, kcap_ = 0, dcap_ = 0, icap_ = 0;
+  int32_t ncap_ = 0;          // vertices the per-vertex buffers hold
+  int64_t hcap_ = 0;          // hub scratch slots
+  size_t units_cap_ = 0;      // ints of units_
   int32_t bs_ = 1;   // nodal batch size of the current solve
   int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t* move_to_ = nullptr;

@@ -233,6 +233,9 @@ void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, 
 
 // --- SortedBuilder --------------------------------------------------------------
 void SortedBuilder::reserve(int64_t e, int bmax, cudaStream_t st) {
+  if (keys_ && e <= e_ && bmax <= bmax_) return;   // the buffers already fit
+  e = std::max(e, e_);
+  bmax = std::max(bmax, bmax_);
   release(st);
   e_ = e;
   bmax_ = bmax;

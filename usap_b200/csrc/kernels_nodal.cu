@@ -990,10 +990,16 @@ struct DeltaTables {
   int tag = 0;    // job number << 24 when the tables serve several jobs
 };
 
+// Adds d under key k; false when no slot was found within kProbeMax probes
+// (the caller then adds straight to global memory), so a nearly full table
+// costs a bounded number of probes per insert.
+constexpr int kProbeMax = 32;
+
 __device__ __forceinline__ bool table_add(int* key, int* val, int lg, int k, int d) {
   const int cap = 1 << lg;
   unsigned h = hash_slot(k, lg);
-  for (int probe = 0; probe < cap; probe++) {
+  const int probes = cap < kProbeMax ? cap : kProbeMax;
+  for (int probe = 0; probe < probes; probe++) {
     const int prev = atomicCAS(key + h, -1, k);
     if (prev == -1 || prev == k) {
       atomicAdd(val + h, d);
@@ -1427,6 +1433,23 @@ __device__ __forceinline__ void gang_tables_flush(const DeltaTables& t, const Ph
   __syncthreads();
 }
 
+// out[0] = 0, out[j + 1] = v_0 + ... + v_j over the gang's jobs, where
+// thread j holds v_j (0 for j >= K); CTA-collective, K <= kGangMax = 64
+__device__ __forceinline__ void job_prefix(long long v, long long* tmp, long long* out) {
+  if (threadIdx.x < kGangMax) tmp[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int l = threadIdx.x;
+    const long long a = warp_incl_scan_ll(tmp[l], l);
+    const long long ta = __shfl_sync(0xffffffffu, a, 31);
+    const long long b = warp_incl_scan_ll(tmp[l + 32], l) + ta;
+    out[l + 1] = a;
+    out[l + 33] = b;
+    if (l == 0) out[0] = 0;
+  }
+  __syncthreads();
+}
+
 // The nodal phases of K jobs (each at some stage of its own solve, dense
 // tile, B <= 4096) in one cooperative launch.  Every round advances each
 // unfinished job by one batch: jobs that start a sweep get their entropy
@@ -1444,8 +1467,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
   __shared__ CtaTally s_tally[kGangMax];
   __shared__ HubShared<kPWarps> sh;
   __shared__ int s_bi[kGangMax], s_sw[kGangMax], s_act[kGangMax], s_nb[kGangMax];
-  __shared__ long long s_hp[kGangMax + 1], s_up[kGangMax + 1], s_cp[kGangMax + 1];
-  __shared__ int s_base, s_state, s_flag;
+  __shared__ long long s_hp[kGangMax + 1], s_up[kGangMax + 1], s_cp[kGangMax + 1], s_tmp[kGangMax];
+  __shared__ int s_base, s_state;
   using Ops = DenseOpsT<LdCG, P>;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gw = blockIdx.x * kPWarps + wib;
@@ -1472,29 +1495,22 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
 
   for (;;) {
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int any = 0, start = 0, count = 0;
-      for (int j = 0; j < K; j++) {
-        any |= s_act[j];
-        start |= s_act[j] && s_bi[j] == 0;
-        count += s_act[j];
-      }
-      s_flag = any | (start << 1) | (count << 2);
-    }
-    __syncthreads();
-    const int flag = s_flag;
+    const bool mine = threadIdx.x < K && s_act[threadIdx.x];
+    const int count = __syncthreads_count(mine);
+    const int start = __syncthreads_or(mine && s_bi[threadIdx.x] == 0);
+    const int flag = (count > 0 ? 1 : 0) | (start ? 2 : 0) | (count << 2);
     if (!(flag & 1)) break;
     if ((flag >> 2) < exit_below) break;   // enough jobs are done: the rest resume in the next launch
     if (flag & 2) {
       // data term of S for the jobs that start a sweep
-      if (threadIdx.x == 0) {
-        s_cp[0] = 0;
-        for (int j = 0; j < K; j++) {
-          const long long B = jobs[j].a.B;
-          s_cp[j + 1] = s_cp[j] + (s_act[j] && s_bi[j] == 0 ? B * B : 0);
+      {
+        long long cells = 0;
+        if (mine && s_bi[threadIdx.x] == 0) {
+          const long long B = jobs[threadIdx.x].a.B;
+          cells = B * B;
         }
+        job_prefix(cells, s_tmp, s_cp);
       }
-      __syncthreads();
       const long long total = s_cp[K];
       long long acc = 0;
       int cj = -1;
@@ -1524,17 +1540,17 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
     }
     // proposals of every unfinished job's current batch
     if (threadIdx.x < K) s_tally[threadIdx.x] = CtaTally{0, 0, 0, 0};
-    if (threadIdx.x == 0) {
-      s_hp[0] = s_up[0] = 0;
-      for (int j = 0; j < K; j++) {
-        const PhaseArgs& p = jobs[j];
-        const int b = s_bi[j];
-        const bool on = s_act[j];
-        s_hp[j + 1] = s_hp[j] + (on ? __ldg(p.batch_hub + b + 1) - __ldg(p.batch_hub + b) : 0);
-        s_up[j + 1] = s_up[j] + (on ? __ldg(p.unit_ptr + b + 1) - __ldg(p.unit_ptr + b) : 0);
+    {
+      long long nh = 0, nu = 0;
+      if (mine) {
+        const PhaseArgs& p = jobs[threadIdx.x];
+        const int b = s_bi[threadIdx.x];
+        nh = __ldg(p.batch_hub + b + 1) - __ldg(p.batch_hub + b);
+        nu = __ldg(p.unit_ptr + b + 1) - __ldg(p.unit_ptr + b);
       }
+      job_prefix(nh, s_tmp, s_hp);
+      job_prefix(nu, s_tmp, s_up);
     }
-    __syncthreads();
     const int H = static_cast<int>(s_hp[K]);
     const int U = static_cast<int>(s_up[K]);
     for (int h = blockIdx.x; h < H; h += gridDim.x) {
@@ -1580,20 +1596,16 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
       }
       if (threadIdx.x == 0) gc->vnext = 0;
     }
-    if (threadIdx.x == 0) {
-      s_cp[0] = 0;
-      for (int j = 0; j < K; j++) {
-        const PhaseArgs& p = jobs[j];
-        long long c = 0;
-        if (s_act[j]) {
-          const int beg = s_bi[j] * p.bs, end = min(p.n, beg + p.bs);
-          c = __ldg(p.chunk_ptr + end) - __ldg(p.chunk_ptr + beg);
-        }
-        s_cp[j + 1] = s_cp[j] + c;
-      }
-    }
     tables_clear(dt);
-    __syncthreads();
+    {
+      long long c = 0;
+      if (mine) {
+        const PhaseArgs& p = jobs[threadIdx.x];
+        const int beg = s_bi[threadIdx.x] * p.bs, end = min(p.n, beg + p.bs);
+        c = __ldg(p.chunk_ptr + end) - __ldg(p.chunk_ptr + beg);
+      }
+      job_prefix(c, s_tmp, s_cp);
+    }
     const long long C = s_cp[K];
     for (long long q = gw; q < C; q += nw) {
       const int j = find_job(s_cp, K, q);

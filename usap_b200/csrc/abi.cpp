@@ -230,6 +230,19 @@ usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, cons
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
       return res[jobs[a].graph]->hg.e > res[jobs[b].graph]->hg.e;
     });
+    // the first W solves (the largest graphs) would otherwise grow the memory
+    // pool while other solves' kernels run, which is slow: reserve it now
+    {
+      int64_t want = 0;
+      const int64_t dmax = base.dense_max > 0 ? base.dense_max : 4096;
+      for (int32_t k = 0; k < std::min<int32_t>(W, njobs); k++) {
+        const usap::HostGraph& hg = res[jobs[order[k]].graph]->hg;
+        // initial blocks: one per vertex, or about N/7 from the SCC pass
+        const int64_t b0 = base.init_mode == 1 ? hg.n : std::max<int64_t>(1, hg.n / 4);
+        want += usap::solve_footprint_bytes(hg.n, hg.e, std::min<int64_t>(dmax, b0), !hg.unit);
+      }
+      usap::pool_reserve(device, want);
+    }
     std::atomic<int32_t> next{0};
     std::atomic<long long> launches{0};
     std::vector<std::thread> th;

@@ -6,6 +6,7 @@
 // destroys a job) are served from the pool instead of the driver.
 // The FP64 log table log(k) is computed once per process on the host (glibc
 // log, the values both the GPU path and the oracle read) and grown on demand.
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <mutex>
@@ -30,6 +31,21 @@ void pool_configure(int device) {
     uint64_t keep = ~0ull;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   });
+}
+
+void pool_reserve(int device, int64_t bytes) {
+  if (bytes <= 0) return;
+  pool_configure(device);
+  size_t free_b = 0, total_b = 0;
+  USAP_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  bytes = std::min<int64_t>(bytes, static_cast<int64_t>(0.5 * static_cast<double>(free_b)));
+  cudaStream_t st = nullptr;
+  USAP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  void* p = nullptr;
+  if (cudaMallocAsync(&p, static_cast<size_t>(bytes), st) == cudaSuccess) cudaFreeAsync(p, st);
+  cudaGetLastError();   // a reservation that does not fit is not an error
+  USAP_CUDA(cudaStreamSynchronize(st));
+  USAP_CUDA(cudaStreamDestroy(st));
 }
 
 void* dev_alloc(size_t bytes, cudaStream_t st) {

@@ -71,6 +71,9 @@ constexpr int kHubSmemSlots = 16384;
 
 // process-wide device memory pool and host tables (devmem.cu)
 void pool_configure(int device);
+// grows the device's memory pool to hold `bytes` (allocated and freed once,
+// then kept by the pool), so that later allocations are served from it
+void pool_reserve(int device, int64_t bytes);
 void* dev_alloc(size_t bytes, cudaStream_t st);
 void dev_free(void* p, cudaStream_t st);
 std::shared_ptr<const std::vector<double>> log_table(int64_t max_k);

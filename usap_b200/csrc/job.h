@@ -13,6 +13,9 @@
 
 namespace usap {
 
+// upper estimate of the device memory one solve holds (server.cpp)
+int64_t solve_footprint_bytes(int64_t n, int64_t e, int64_t dense_max, bool weighted);
+
 struct HostGraph {
   int32_t n = 0;
   int64_t e = 0;

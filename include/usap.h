@@ -166,6 +166,14 @@ usap_status usap_partition(const usap_graph* g, const usap_params* p, int32_t* o
  * printed.  Labels are 0-based; truth label -1 marks unknown vertices. */
 usap_status usap_evaluate(const int32_t* truth, const int32_t* given, int64_t n,
                           usap_scores* out);
+/* The same scores from DEVICE arrays (n labels each, on `device`): the
+ * contingency table, pair counts and information sums are computed on the
+ * GPU, the block matching of `accuracy` on the host.  Bit-identical to
+ * usap_evaluate: both form the scores from exact integer pair counts and
+ * information terms summed in fixed point (2^-50).  USAP_ERR_LIMIT above
+ * 2^26 table cells (truth blocks x given blocks). */
+usap_status usap_evaluate_device(const int32_t* truth, const int32_t* given, int64_t n,
+                                 int32_t device, usap_scores* out);
 
 /* --- resident contexts: the graph stays in HBM across solves ------------- */
 usap_status usap_ctx_create(int32_t device, usap_ctx** out);
@@ -173,6 +181,10 @@ usap_status usap_ctx_destroy(usap_ctx* ctx);
 /* Graph_P constructor / load_graph_from_tsv (graph_parallel.hpp:251-317) */
 usap_status usap_ctx_load(usap_ctx* ctx, const usap_graph* g);
 usap_status usap_ctx_num_nodes(usap_ctx* ctx, int32_t* n, int64_t* e);
+/* Scores of the context's last partition result against truth (host array
+ * of n labels), evaluated on the device where that result lies (the
+ * partition itself is not copied back). */
+usap_status usap_ctx_evaluate(usap_ctx* ctx, const int32_t* truth, usap_scores* out);
 /* partition() on the loaded graph; out_assign may be NULL */
 usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out_assign,
                                usap_result* out);

@@ -58,6 +58,14 @@ class Context:
         nat.check(nat.lib().usap_ctx_partition(self._h, C.byref(p), nat.p32(out), C.byref(res)))
         return out, nat.result_dict(res)
 
+    def evaluate(self, truth) -> dict:
+        """Scores of the last partition() result against ``truth``, computed on
+        the device where the result lies (usap_ctx_evaluate)."""
+        t = np.ascontiguousarray(truth, np.int32)
+        s = nat.Scores()
+        nat.check(nat.lib().usap_ctx_evaluate(self._h, nat.p32(t), C.byref(s)))
+        return nat.scores_dict(s)
+
     def set_trace(self, fn: Optional[Callable[[dict], None]]) -> None:
         if fn is None:
             self._trace_fn = nat.TRACE_FN()
@@ -270,6 +278,15 @@ def evaluate(truth, given) -> dict:
         raise ValueError("truth and given must have the same length")
     s = nat.Scores()
     nat.check(nat.lib().usap_evaluate(nat.p32(t), nat.p32(g), int(t.size), C.byref(s)))
+    return nat.scores_dict(s)
+
+
+def evaluate_device(truth_ptr: int, given_ptr: int, n: int, device: int = 0) -> dict:
+    """usap_evaluate_device: the same scores from device arrays (raw int32
+    pointers on ``device``, e.g. a torch CUDA tensor's ``data_ptr()``)."""
+    s = nat.Scores()
+    nat.check(nat.lib().usap_evaluate_device(C.c_void_p(truth_ptr), C.c_void_p(given_ptr), int(n), int(device),
+                                             C.byref(s)))
     return nat.scores_dict(s)
 
 

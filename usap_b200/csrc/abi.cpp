@@ -175,6 +175,26 @@ usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out
   });
 }
 
+usap_status usap_ctx_evaluate(usap_ctx* ctx, const int32_t* truth, usap_scores* out) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (!truth || !out) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    ctx->job->evaluate_last(truth, out);
+  });
+}
+
+usap_status usap_evaluate_device(const int32_t* truth, const int32_t* given, int64_t n, int32_t device,
+                                 usap_scores* out) {
+  return guarded([&] {
+    if (!truth || !given || !out) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+      throw usap::Error(USAP_ERR_NO_DEVICE, "no CUDA device available");
+    if (device < 0 || device >= count) throw usap::Error(USAP_ERR_INVALID, "device index out of range");
+    usap::evaluate_device(truth, given, n, device, out);
+  });
+}
+
 usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user) {
   return guarded([&] {
     check_ctx(ctx);

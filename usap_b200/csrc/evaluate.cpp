@@ -1,5 +1,7 @@
 // Partition scores (bf::evaluate, include/evaluate.hpp:18-266), returned
-// instead of printed, in FP64 with exact integer pair counts.
+// instead of printed, computed from exact integer pair counts and
+// fixed-point information sums (eval_common.h), which the device version
+// (kernels_eval.cu) reproduces bit for bit.
 //
 // bf::evaluate permutes the contingency table's columns by a Kuhn-Munkres
 // matching before scoring; the pair-counting and information scores do not
@@ -11,12 +13,14 @@
 // negates unsigned costs, evaluate.hpp:62-67, which makes its own figure
 // unreliable; a correct Hungarian matching is used here).  The exact ARI
 // is reported beside it.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <limits>
 #include <unordered_map>
 #include <vector>
 
+#include "eval_common.h"
 #include "job.h"
 
 namespace usap {
@@ -75,11 +79,58 @@ int64_t hungarian_max(const std::vector<int64_t>& w, int n) {
 
 }  // namespace
 
+void scores_from_sums(const EvalSums& e, usap_scores* s) {
+  std::memset(s, 0, sizeof(*s));
+  const int64_t N = e.N;
+  const double dN = static_cast<double>(N);
+  const double pairs = dN * static_cast<double>(N - 1) / 2.0;
+  const double same = static_cast<double>(e.same), s1 = static_cast<double>(e.s1), s2 = static_cast<double>(e.s2);
+  const double diff = (dN * dN + static_cast<double>(e.sq) - static_cast<double>(e.sc) - static_cast<double>(e.sr)) / 2.0;
+  s->rand_index = (same + diff) / pairs;
+  {
+    unsigned __int128 num = static_cast<unsigned __int128>(static_cast<uint64_t>(e.s1)) * static_cast<uint64_t>(e.s2);
+    uint64_t pr = static_cast<uint64_t>(N) * static_cast<uint64_t>(N - 1) / 2;
+    double expected = static_cast<double>(static_cast<uint64_t>(num / pr));
+    s->adjusted_rand_index = (same - expected) / (0.5 * (s1 + s2) - expected);
+    double ex = s1 * s2 / pairs;
+    s->adjusted_rand_index_exact = (same - ex) / (0.5 * (s1 + s2) - ex);
+  }
+  s->pairwise_recall = same / s1;
+  s->pairwise_precision = same / s2;
+  const double H1 = -static_cast<double>(e.h_truth_q) / kQ50;
+  const double H2 = -static_cast<double>(e.h_given_q) / kQ50;
+  const double H21 = -static_cast<double>(e.h_gt_q) / kQ50;
+  const double H12 = -static_cast<double>(e.h_tg_q) / kQ50;
+  const double MI = static_cast<double>(e.mi_q) / kQ50;
+  s->h_truth = H1;
+  s->h_given = H2;
+  s->h_given_truth = H21;
+  s->h_truth_given = H12;
+  s->mi = MI;
+  s->nmi = (H1 + H2) > 0 ? 2.0 * MI / (H1 + H2) : 1.0;
+  s->nmi_sqrt = (H1 > 0 && H2 > 0) ? MI / std::sqrt(H1 * H2) : 1.0;
+  s->missed_info = H1 > 0 ? H12 / H1 : 0.0;
+  s->erroneous_info = H2 > 0 ? H21 / H2 : 0.0;
+  s->n = N;
+  s->b_truth = e.nb_truth;
+  s->b_given = e.nb_given;
+}
+
+double matching_accuracy(const int64_t* table, int b1, int b2, int64_t N) {
+  const int m = b1 > b2 ? b1 : b2;
+  if (m > 2048) return std::nan("");
+  std::vector<int64_t> w(static_cast<size_t>(m) * m, 0);
+  for (int i = 0; i < b1; i++)
+    for (int j = 0; j < b2; j++) w[static_cast<size_t>(i) * m + j] = table[static_cast<size_t>(i) * b2 + j];
+  return static_cast<double>(hungarian_max(w, m)) / static_cast<double>(N);
+}
+
 void evaluate_host(const int32_t* truth, const int32_t* given, int64_t n, usap_scores* s) {
   std::memset(s, 0, sizeof(*s));
   int32_t b1 = 0, b2 = 0;
   for (int64_t i = 0; i < n; i++) {
     if (given[i] < 0) throw Error(USAP_ERR_INVALID, "given labels must be >= 0");
+    if (truth[i] < -1) throw Error(USAP_ERR_INVALID, "truth labels must be >= -1");
     if (truth[i] + 1 > b1) b1 = truth[i] + 1;
     if (given[i] + 1 > b2) b2 = given[i] + 1;
   }
@@ -95,76 +146,40 @@ void evaluate_host(const int32_t* truth, const int32_t* given, int64_t n, usap_s
     N++;
   }
   if (N < 2) throw Error(USAP_ERR_INVALID, "need at least two vertices with known truth");
-  const double pairs = static_cast<double>(N) * static_cast<double>(N - 1) / 2.0;
-  double sq = 0, same = 0, sr = 0, sc = 0, s1 = 0, s2 = 0;
+  const std::shared_ptr<const std::vector<double>> Lp = log_table(N);
+  const std::vector<double>& L = *Lp;
+  const double dN = static_cast<double>(N), LN = L[N];
+  EvalSums e{};
+  e.N = N;
   for (const auto& kv : cells) {
-    double c = static_cast<double>(kv.second);
-    sq += c * c;
-    same += c * (c - 1) / 2;
+    const int64_t c = kv.second, i = kv.first / b2, j = kv.first % b2;
+    e.sq += c * c;
+    e.same += c * (c - 1) / 2;
+    e.h_gt_q += ev_term(c, dN, L[c], L[rows[i]]);
+    e.h_tg_q += ev_term(c, dN, L[c], L[cols[j]]);
+    e.mi_q += ev_mi_term(c, dN, L[c], LN, L[rows[i]], L[cols[j]]);
   }
-  int32_t nb1 = 0, nb2 = 0;
-  for (int64_t r : rows) {
-    sr += static_cast<double>(r) * r;
-    s1 += static_cast<double>(r) * (r - 1) / 2;
-    nb1 += r > 0;
-  }
-  for (int64_t c : cols) {
-    sc += static_cast<double>(c) * c;
-    s2 += static_cast<double>(c) * (c - 1) / 2;
-    nb2 += c > 0;
-  }
-  const double diff = (static_cast<double>(N) * N + sq - sc - sr) / 2.0;
-  s->rand_index = (same + diff) / pairs;
-  {
-    unsigned __int128 num = static_cast<unsigned __int128>(static_cast<uint64_t>(s1)) * static_cast<uint64_t>(s2);
-    uint64_t pr = static_cast<uint64_t>(N) * static_cast<uint64_t>(N - 1) / 2;
-    double expected = static_cast<double>(static_cast<uint64_t>(num / pr));
-    s->adjusted_rand_index = (same - expected) / (0.5 * (s1 + s2) - expected);
-    double ex = s1 * s2 / pairs;
-    s->adjusted_rand_index_exact = (same - ex) / (0.5 * (s1 + s2) - ex);
-  }
-  s->pairwise_recall = same / s1;
-  s->pairwise_precision = same / s2;
-  const double dN = static_cast<double>(N);
-  double H1 = 0, H2 = 0, H21 = 0, H12 = 0, MI = 0;
   for (int64_t r : rows)
     if (r) {
-      double p = r / dN;
-      H1 -= p * std::log(p);
+      e.sr += r * r;
+      e.s1 += r * (r - 1) / 2;
+      e.nb_truth++;
+      e.h_truth_q += ev_term(r, dN, L[r], LN);
     }
   for (int64_t c : cols)
     if (c) {
-      double p = c / dN;
-      H2 -= p * std::log(p);
+      e.sc += c * c;
+      e.s2 += c * (c - 1) / 2;
+      e.nb_given++;
+      e.h_given_q += ev_term(c, dN, L[c], LN);
     }
-  for (const auto& kv : cells) {
-    int64_t i = kv.first / b2, j = kv.first % b2;
-    double pj = kv.second / dN, p1 = rows[i] / dN, p2 = cols[j] / dN;
-    H21 -= pj * std::log(pj / p1);
-    H12 -= pj * std::log(pj / p2);
-    MI += pj * std::log(pj / (p1 * p2));
-  }
-  s->h_truth = H1;
-  s->h_given = H2;
-  s->h_given_truth = H21;
-  s->h_truth_given = H12;
-  s->mi = MI;
-  s->nmi = (H1 + H2) > 0 ? 2.0 * MI / (H1 + H2) : 1.0;
-  s->nmi_sqrt = (H1 > 0 && H2 > 0) ? MI / std::sqrt(H1 * H2) : 1.0;
-  s->missed_info = H1 > 0 ? H12 / H1 : 0.0;
-  s->erroneous_info = H2 > 0 ? H21 / H2 : 0.0;
-  s->n = N;
-  s->b_truth = nb1;
-  s->b_given = nb2;
+  scores_from_sums(e, s);
   // accuracy: best one-to-one matching of truth blocks to given blocks
   const int m = b1 > b2 ? b1 : b2;
   if (m <= 2048) {
-    std::vector<int64_t> w(static_cast<size_t>(m) * m, 0);
-    for (const auto& kv : cells) {
-      int64_t i = kv.first / b2, j = kv.first % b2;
-      w[static_cast<size_t>(i) * m + j] = kv.second;
-    }
-    s->accuracy = static_cast<double>(hungarian_max(w, m)) / dN;
+    std::vector<int64_t> t(static_cast<size_t>(b1) * b2, 0);
+    for (const auto& kv : cells) t[static_cast<size_t>(kv.first)] = kv.second;
+    s->accuracy = matching_accuracy(t.data(), b1, b2, N);
   } else {
     s->accuracy = std::nan("");
   }

@@ -1055,6 +1055,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
       res->ms_d2h = std::chrono::duration<double, std::milli>(td1 - td0).count();
       if (out_assign) d2h += static_cast<long long>(sizeof(int32_t)) * n;
       res->B = gs.med.B;
+      last_part_ = slots_[gs.med.slot];
       res->S_q = gs.med.S_q;
       res->S = gs.med.S;
       break;
@@ -1100,6 +1101,24 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   res->h2d_bytes = static_cast<long long>(sizeof(int32_t)) * n;   // initial partition
   res->d2h_bytes = d2h;
   res->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+}
+
+// scores of the last solve's partition, evaluated where it lies in HBM
+void Job::evaluate_last(const int32_t* truth, usap_scores* out) {
+  if (!loaded() || !last_part_) throw Error(USAP_ERR_STATE, "no solve to evaluate");
+  USAP_CUDA(cudaSetDevice(device_));
+  const int32_t n = hg_->n;
+  int32_t* t = nullptr;
+  dalloc(&t, n);
+  USAP_CUDA(cudaMemcpyAsync(t, truth, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st_));
+  USAP_CUDA(cudaStreamSynchronize(st_));
+  try {
+    evaluate_device(t, last_part_, n, device_, out);
+  } catch (...) {
+    dfree(t);
+    throw;
+  }
+  dfree(t);
 }
 
 // --- phase-level operations -------------------------------------------------------

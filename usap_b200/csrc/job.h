@@ -42,6 +42,8 @@ int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part);
 
 // host evaluation (evaluate.hpp:18-266 scores + NMI + Hungarian accuracy)
 void evaluate_host(const int32_t* truth, const int32_t* given, int64_t n, usap_scores* out);
+// the same scores from device arrays on `device` (kernels_eval.cu)
+void evaluate_device(const int32_t* truth, const int32_t* given, int64_t n, int device, usap_scores* out);
 
 // _prepare_for_partition_next (graph_parallel.hpp:1322-1365) on slot ids
 struct GoldenPoint {
@@ -164,6 +166,9 @@ class Job {
     trace_user_ = user;
   }
   void partition(const usap_params& p, int32_t* out_assign, usap_result* res);
+  // bf::evaluate scores of the last partition() result against truth (host
+  // array of n labels), computed on the device where the result lies
+  void evaluate_last(const int32_t* truth, usap_scores* out);
   // drops the graph (its device memory is freed when no job holds it);
   // the solver state stays allocated for the next graph
   void detach() { free_graph(); }
@@ -242,6 +247,7 @@ class Job {
   int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t* move_to_ = nullptr;
   int32_t* from_ = nullptr;
+  const int32_t* last_part_ = nullptr;   // slot holding the last solve's result
   int32_t* batch_hub_ = nullptr;     // first hub of each batch of size bs_
   int32_t* unit_ptr_ = nullptr;      // first work unit of each batch
   int2* units_ = nullptr;            // work units of the persistent kernel

@@ -28,56 +28,63 @@ void scc_prepare(HostGraph& g) {
 }
 
 int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part) {
-  const int32_t n = g.n;
+  const int32_t* tptr = g.transpose_is_in ? g.in_ptr.data() : g.tptr.data();
+  const int32_t* tidx = g.transpose_is_in ? g.in_idx.data() : g.tidx.data();
+  return scc_arrays(g.n, g.e, g.out_ptr.data(), g.out_idx.data(), tptr, tidx, dfs_depth, part);
+}
+
+int32_t scc_arrays(int32_t n, int64_t e, const int32_t* optr, const int32_t* oidx, const int32_t* tptr,
+                   const int32_t* tidx, int32_t dfs_depth, int32_t* part) {
+  // both passes use preallocated stacks: a vertex turns grey once and pushes
+  // each out-neighbour at most once then, so the first pass pushes at most
+  // E + N entries; the second is bounded by E + 1 per root
   std::vector<uint8_t> color(n, 0);
-  std::vector<int32_t> finish;
-  finish.reserve(n);
-  std::vector<int32_t> st;
-  st.reserve(1024);
+  std::vector<int32_t> finish(n);
+  std::vector<int32_t> stack(static_cast<size_t>(e) + n + 1);
+  uint8_t* col = color.data();
+  int32_t* st = stack.data();
+  int32_t nf = 0;
   for (int32_t v0 = 0; v0 < n; v0++) {
-    if (color[v0]) continue;
-    st.push_back(v0);
-    while (!st.empty()) {
-      int32_t v = st.back();
-      if (color[v]) {
-        st.pop_back();
-        if (color[v] == 1) {
-          finish.push_back(v);
-          color[v] = 2;
+    if (col[v0]) continue;
+    int64_t top = 0;
+    st[top++] = v0;
+    while (top) {
+      const int32_t v = st[top - 1];
+      const uint8_t c = col[v];
+      if (c) {
+        --top;
+        if (c == 1) {
+          finish[nf++] = v;
+          col[v] = 2;
         }
       } else {
-        color[v] = 1;
-        for (int32_t p = g.out_ptr[v]; p < g.out_ptr[v + 1]; p++) {
-          int32_t t = g.out_idx[p];
-          if (!color[t]) st.push_back(t);
+        col[v] = 1;
+        for (const int32_t *it = oidx + optr[v], *end = oidx + optr[v + 1]; it != end; ++it) {
+          const int32_t t = *it;
+          if (!col[t]) st[top++] = t;
         }
       }
     }
   }
-  const int32_t* tptr = g.transpose_is_in ? g.in_ptr.data() : g.tptr.data();
-  const int32_t* tidx = g.transpose_is_in ? g.in_idx.data() : g.tidx.data();
   std::vector<uint8_t> visited(n, 0);
+  uint8_t* vis = visited.data();
   for (int32_t v = 0; v < n; v++) part[v] = -1;
   int32_t b = 0;
-  std::vector<int32_t> st2;
-  st2.reserve(256);
-  while (!finish.empty()) {
-    int32_t v = finish.back();
-    finish.pop_back();
-    if (visited[v]) continue;
+  while (nf > 0) {
+    const int32_t v = finish[--nf];
+    if (vis[v]) continue;
     int32_t i = 0;
-    st2.clear();
-    st2.push_back(v);
-    while (!st2.empty() && i < dfs_depth) {
-      int32_t ni = st2.back();
-      st2.pop_back();
-      if (!visited[ni]) {
-        visited[ni] = 1;
+    int64_t top = 0;
+    st[top++] = v;
+    while (top && i < dfs_depth) {
+      const int32_t ni = st[--top];
+      if (!vis[ni]) {
+        vis[ni] = 1;
         part[ni] = b;
         i++;
-        for (int32_t p = tptr[ni]; p < tptr[ni + 1]; p++) {
-          int32_t t = tidx[p];
-          if (!visited[t]) st2.push_back(t);
+        for (const int32_t *it = tidx + tptr[ni], *end = tidx + tptr[ni + 1]; it != end; ++it) {
+          const int32_t t = *it;
+          if (!vis[t]) st[top++] = t;
         }
       }
     }

@@ -286,6 +286,15 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   const std::shared_ptr<const std::vector<double>> logk_all = log_table(wtot);
 
   auto gr = std::make_shared<GraphResident>(device);
+  // the first solve's initial blocks, on a host thread while the graph
+  // uploads (the CSR buffers keep their addresses when h moves into gr)
+  {
+    gr->scc_part.resize(n);
+    const int32_t* tp = h.transpose_is_in ? h.in_ptr.data() : h.tptr.data();
+    const int32_t* ti = h.transpose_is_in ? h.in_idx.data() : h.tidx.data();
+    gr->scc_b = std::async(std::launch::async, scc_arrays, n, h.e, h.out_ptr.data(), h.out_idx.data(), tp, ti,
+                           kDefaultDfsDepth, gr->scc_part.data());
+  }
   cudaStream_t st_ = gr->st;
   cudaEvent_t e0, e1;
   USAP_CUDA(cudaEventCreate(&e0));
@@ -363,12 +372,21 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   return gr;
 }
 
+bool GraphResident::take_initial_blocks(int32_t* B, std::vector<int32_t>* part) {
+  std::lock_guard<std::mutex> lk(scc_mu);
+  if (!scc_b.valid()) return false;
+  *B = scc_b.get();
+  part->swap(scc_part);
+  return true;
+}
+
 GraphResident::GraphResident(int dev) : device(dev) {
   pool_configure(dev);
   USAP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
 }
 
 GraphResident::~GraphResident() {
+  if (scc_b.valid()) scc_b.wait();   // the host thread reads hg
   cudaSetDevice(device);
   cudaStream_t st_ = st;
   dfree(g.src); dfree(g.dst); dfree(g.w);
@@ -867,7 +885,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   if (p.init_mode == 1) {
     for (int32_t v = 0; v < n; v++) part0[v] = v;
     B = n;
-  } else {
+  } else if (p.dfs_depth != kDefaultDfsDepth || !gr_->take_initial_blocks(&B, &part0)) {
     B = scc_host(*hg_, p.dfs_depth, part0.data());
   }
   ensure_capacity(B, K, dense_max, std::max(maxitr, 1));

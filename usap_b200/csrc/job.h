@@ -2,6 +2,7 @@
 #pragma once
 
 #include <chrono>
+#include <future>
 #include <condition_variable>
 #include <mutex>
 #include <string>
@@ -38,6 +39,8 @@ struct HostGraph {
 void scc_prepare(HostGraph& g);
 // out- and in-lists (and weighted degrees) from h.src/dst/w in file order
 void build_csr(HostGraph& h);
+int32_t scc_arrays(int32_t n, int64_t e, const int32_t* optr, const int32_t* oidx, const int32_t* tptr,
+                   const int32_t* tidx, int32_t dfs_depth, int32_t* part);
 int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part);
 
 // host evaluation (evaluate.hpp:18-266 scores + NMI + Hungarian accuracy)
@@ -76,13 +79,23 @@ inline double desc_length(double model, long long data_q) {
 // A graph loaded into HBM (CSR, edge list, log table, hub list); read-only
 // once loaded and shared by every job that solves it.  Its device arrays
 // are allocated and released on its own stream.
+// the reference's default DFS depth (graph_parallel.hpp:51)
+constexpr int32_t kDefaultDfsDepth = 20;
+
 struct GraphResident {
   explicit GraphResident(int device);
   ~GraphResident();
   GraphResident(const GraphResident&) = delete;
   GraphResident& operator=(const GraphResident&) = delete;
+  // the initial blocks for the default DFS depth, computed on a host thread
+  // while the graph uploads; the first solve takes them (later solves
+  // compute their own).  True with B and part filled when they were there.
+  bool take_initial_blocks(int32_t* B, std::vector<int32_t>* part);
   int device;
   cudaStream_t st = nullptr;
+  std::mutex scc_mu;
+  std::future<int32_t> scc_b;          // B of scc_part, once the host thread is done
+  std::vector<int32_t> scc_part;
   HostGraph hg;
   GraphDev g;                      // hkey/hwo/hwi belong to the jobs
   std::vector<int32_t> hub_ids;    // vertices of degree > kHubDegree, ascending

@@ -181,6 +181,15 @@ usap_status usap_ctx_destroy(usap_ctx* ctx);
 /* Graph_P constructor / load_graph_from_tsv (graph_parallel.hpp:251-317) */
 usap_status usap_ctx_load(usap_ctx* ctx, const usap_graph* g);
 usap_status usap_ctx_num_nodes(usap_ctx* ctx, int32_t* n, int64_t* e);
+/* load_graph_from_tsv (graph_parallel.hpp:251-317) from the bytes of the
+ * .tsv file (`len` bytes, host memory): the text is parsed on the device,
+ * one line per edge, fields read as the reference reads them (stoul, stof
+ * truncated to an integer weight; a line with no second tab takes its
+ * source id as its weight, as the reference's npos arithmetic does).
+ * n = 0: N = the largest source id, as in the reference.  A malformed line
+ * (a field without digits, id 0, weight not positive, a value above
+ * 2^31 - 1) is USAP_ERR_INVALID naming the line. */
+usap_status usap_ctx_load_tsv(usap_ctx* ctx, const char* text, int64_t len, int32_t n);
 /* Scores of the context's last partition result against truth (host array
  * of n labels), evaluated on the device where that result lies (the
  * partition itself is not copied back). */

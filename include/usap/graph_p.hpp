@@ -10,9 +10,10 @@
 //   std::vector<size_t> truePartitions                               :81
 //   void load_graph_from_tsv(const std::string& FileName)            :55, :251-317
 //
-// The constructor reads FileName.tsv (from<TAB>to<TAB>weight, 1-based) and
-// FileName_truePartition.tsv (node<TAB>block) exactly as the reference
-// does, including N = largest source id and the three summary lines on
+// The constructor reads FileName.tsv (from<TAB>to<TAB>weight, 1-based; its
+// bytes are parsed on the GPU by usap_ctx_load_tsv with the reference's
+// field rules) and FileName_truePartition.tsv (node<TAB>block) as the
+// reference does, including N = largest source id and the three summary lines on
 // stdout; an unreadable file prints "Unable to open file!" and exits, as
 // the reference does (graph_parallel.hpp:254-257, :294-297).  partition()
 // runs on the GPU through include/usap.h; num_threads is accepted and
@@ -23,6 +24,7 @@
 #include <cstdlib>
 #include <fstream>
 #include <iostream>
+#include <iterator>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -64,34 +66,21 @@ class Graph_P {
   Graph_P& operator=(const Graph_P&) = delete;
 
   void load_graph_from_tsv(const std::string& FileName) {
-    std::ifstream file(FileName + ".tsv");
+    std::ifstream file(FileName + ".tsv", std::ios::binary);
     if (!file.is_open()) {
       std::cerr << "Unable to open file!\n";
       std::exit(EXIT_FAILURE);
     }
-    N_ = 0;
-    src_.clear();
-    dst_.clear();
-    w_.clear();
+    const std::string text((std::istreambuf_iterator<char>(file)), std::istreambuf_iterator<char>());
+    file.close();
+    if (!ctx_) check(usap_ctx_create(device, &ctx_));
+    check(usap_ctx_load_tsv(ctx_, text.data(), static_cast<int64_t>(text.size()), 0));
+    int32_t n = 0;
+    int64_t e = 0;
+    check(usap_ctx_num_nodes(ctx_, &n, &e));
+    N_ = static_cast<size_t>(n);
+    E_ = static_cast<size_t>(e);
     std::string line;
-    bool unit = true;
-    while (std::getline(file, line)) {
-      size_t start = 0, tab = line.find('\t');
-      size_t from = std::stoul(line.substr(start, tab - start));
-      start = tab + 1;
-      tab = line.find('\t', start);
-      size_t to = std::stoul(line.substr(start, tab - start));
-      start = tab + 1;
-      tab = line.find('\t', start);
-      W weight = static_cast<W>(std::stof(line.substr(start, tab - start)));
-      src_.push_back(static_cast<int32_t>(from));
-      dst_.push_back(static_cast<int32_t>(to));
-      w_.push_back(static_cast<int32_t>(weight));
-      if (weight != 1) unit = false;
-      if (from > N_) N_ = from;
-    }
-    E_ = src_.size();
-    if (unit) w_.clear();
     std::ifstream true_file(FileName + "_truePartition.tsv");
     if (!true_file.is_open()) {
       std::cerr << "Unable to open file!\n";
@@ -110,15 +99,6 @@ class Graph_P {
     std::cout << "Number of nodes: " << N_ << std::endl;
     std::cout << "Number of edges: " << E_ << std::endl;
     std::cout << "NUmber of blocks:" << b << std::endl;
-    if (!ctx_) check(usap_ctx_create(device, &ctx_));
-    usap_graph g;
-    g.n = static_cast<int32_t>(N_);
-    g.e = static_cast<int64_t>(E_);
-    g.src = src_.data();
-    g.dst = dst_.data();
-    g.weight = w_.empty() ? nullptr : w_.data();
-    g.one_based = 1;
-    check(usap_ctx_load(ctx_, &g));
   }
 
   const size_t& num_nodes() const { return N_; }
@@ -158,7 +138,6 @@ class Graph_P {
     if (s != USAP_OK) throw std::runtime_error(std::string("usap: ") + usap_last_error());
   }
   size_t N_ = 0, E_ = 0;
-  std::vector<int32_t> src_, dst_, w_;
   std::vector<size_t> partitions_;
   usap_ctx* ctx_ = nullptr;
   usap_result result_{};

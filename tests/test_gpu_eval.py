@@ -83,6 +83,6 @@ def test_device_scores_reject_bad_labels(api):
     with pytest.raises(nat.UsapError):
         api.evaluate_device(t.data_ptr(), g.data_ptr(), 10)
     ctx = api.Context(0)
-    with pytest.raises(nat.UsapError):      # nothing solved yet
-        ctx.evaluate(truth)
+    with pytest.raises(nat.UsapError):      # nothing loaded or solved yet
+        ctx.evaluate(np.zeros(0, np.int32))
     ctx.close()

@@ -58,10 +58,22 @@ class Context:
         nat.check(nat.lib().usap_ctx_partition(self._h, C.byref(p), nat.p32(out), C.byref(res)))
         return out, nat.result_dict(res)
 
+    def load_tsv(self, text: bytes, n: int = 0) -> None:
+        """load_graph_from_tsv from the bytes of a reference-format .tsv file,
+        parsed on the device (usap_ctx_load_tsv); n = 0: N is the largest
+        source id."""
+        nat.check(nat.lib().usap_ctx_load_tsv(self._h, text, len(text), int(n)))
+        nn = C.c_int32()
+        ee = C.c_int64()
+        nat.check(nat.lib().usap_ctx_num_nodes(self._h, C.byref(nn), C.byref(ee)))
+        self.n, self.e = int(nn.value), int(ee.value)
+
     def evaluate(self, truth) -> dict:
         """Scores of the last partition() result against ``truth``, computed on
         the device where the result lies (usap_ctx_evaluate)."""
         t = np.ascontiguousarray(truth, np.int32)
+        if t.size != self.n:
+            raise ValueError(f"truth has {t.size} labels, the graph {self.n} vertices")
         s = nat.Scores()
         nat.check(nat.lib().usap_ctx_evaluate(self._h, nat.p32(t), C.byref(s)))
         return nat.scores_dict(s)

@@ -156,6 +156,24 @@ usap_status usap_ctx_load(usap_ctx* ctx, const usap_graph* g) {
   });
 }
 
+usap_status usap_ctx_load_tsv(usap_ctx* ctx, const char* text, int64_t len, int32_t n) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (!text && len > 0) throw usap::Error(USAP_ERR_INVALID, "null text");
+    if (n < 0) throw usap::Error(USAP_ERR_INVALID, "n must be >= 0");
+    usap::TsvEdges t = usap::parse_tsv_device(ctx->job->device(), text ? text : "", len);
+    if (t.src.empty()) throw usap::Error(USAP_ERR_INVALID, "graph needs at least one edge");
+    usap_graph g{};
+    g.n = n > 0 ? n : t.max_src;   // N = the largest source id (graph_parallel.hpp:276)
+    g.e = static_cast<int64_t>(t.src.size());
+    g.src = t.src.data();
+    g.dst = t.dst.data();
+    g.weight = t.w.empty() ? nullptr : t.w.data();
+    g.one_based = 0;
+    ctx->job->load(g);
+  });
+}
+
 usap_status usap_ctx_num_nodes(usap_ctx* ctx, int32_t* n, int64_t* e) {
   return guarded([&] {
     check_ctx(ctx);

@@ -45,6 +45,15 @@ int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part);
 
 // host evaluation (evaluate.hpp:18-266 scores + NMI + Hungarian accuracy)
 void evaluate_host(const int32_t* truth, const int32_t* given, int64_t n, usap_scores* out);
+// edges parsed on the device from the text of a reference-format .tsv
+// file (kernels_tsv.cu): 0-based ids in file order, weights empty when all
+// are 1; max_src is the reference's N
+struct TsvEdges {
+  std::vector<int32_t> src, dst, w;
+  int32_t max_src = 0, max_id = 0;
+};
+TsvEdges parse_tsv_device(int device, const char* text, int64_t len);
+
 // the same scores from device arrays on `device` (kernels_eval.cu)
 void evaluate_device(const int32_t* truth, const int32_t* given, int64_t n, int device, usap_scores* out);
 

@@ -190,6 +190,18 @@ usap_status usap_ctx_num_nodes(usap_ctx* ctx, int32_t* n, int64_t* e);
  * (a field without digits, id 0, weight not positive, a value above
  * 2^31 - 1) is USAP_ERR_INVALID naming the line. */
 usap_status usap_ctx_load_tsv(usap_ctx* ctx, const char* text, int64_t len, int32_t n);
+/* --- streaming input (no counterpart in the reference, whose README lists
+ * streaming graphs as future work, README.md:47-49) ------------------------
+ * usap_ctx_add_edges appends an edge batch to the resident graph: the edge
+ * list becomes the current one followed by these edges (file order), n
+ * grows to max(current n, g->n, largest source id + 1).
+ * usap_ctx_partition_from is partition() started from init[n] (block labels
+ * >= 0, renumbered 0..B-1 in ascending order) instead of the SCC pass
+ * (graph_parallel.hpp:338-342): pass the previous stage's result extended
+ * with labels for the new vertices to continue a partition as edges arrive. */
+usap_status usap_ctx_add_edges(usap_ctx* ctx, const usap_graph* g);
+usap_status usap_ctx_partition_from(usap_ctx* ctx, const usap_params* p, const int32_t* init,
+                                    int32_t* out_assign, usap_result* out);
 /* Scores of the context's last partition result against truth (host array
  * of n labels), evaluated on the device where that result lies (the
  * partition itself is not copied back). */

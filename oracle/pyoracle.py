@@ -151,6 +151,9 @@ def lib() -> C.CDLL:
         L.og_partition.argtypes = [C.POINTER(OgGraph), C.POINTER(OgParams), i32p,
                                    C.POINTER(OgResult), TRACE_FN, C.c_void_p]
         L.og_partition.restype = C.c_int
+        L.og_partition_from.argtypes = [C.POINTER(OgGraph), C.POINTER(OgParams), i32p, i32p,
+                                        C.POINTER(OgResult), TRACE_FN, C.c_void_p]
+        L.og_partition_from.restype = C.c_int
         L.og_hash_part.argtypes = [i32p, C.c_int32]
         L.og_hash_part.restype = C.c_uint64
         L.og_evaluate.argtypes = [i32p, i32p, C.c_int64, C.POINTER(OgScores)]
@@ -207,7 +210,9 @@ class OracleGraph:
     def blocks(self, part: np.ndarray, B: int) -> "OracleBlocks":
         return OracleBlocks(self, part, B)
 
-    def partition(self, params: Optional[dict] = None, trace: bool = False):
+    def partition(self, params: Optional[dict] = None, trace: bool = False, init=None):
+        """The whole solve; ``init`` (n labels) starts it from that partition
+        instead of the SCC pass."""
         p = OgParams()
         lib().og_params_default(C.byref(p))
         for k, v in (params or {}).items():
@@ -221,7 +226,12 @@ class OracleGraph:
             events.append({f: getattr(e, f) for f, _ in OgTraceEvent._fields_})
 
         fn = TRACE_FN(cb) if trace else TRACE_FN()
-        rc = lib().og_partition(C.byref(self.g), C.byref(p), _p32(part), C.byref(res), fn, None)
+        if init is None:
+            rc = lib().og_partition(C.byref(self.g), C.byref(p), _p32(part), C.byref(res), fn, None)
+        else:
+            ini = np.ascontiguousarray(init, dtype=np.int32)
+            rc = lib().og_partition_from(C.byref(self.g), C.byref(p), _p32(ini), _p32(part), C.byref(res), fn,
+                                         None)
         if rc != 0:
             raise RuntimeError(f"og_partition failed ({rc})")
         out = {f: getattr(res, f) for f, _ in OgResult._fields_}

@@ -866,8 +866,43 @@ int og_golden_step(og_golden* gs, int32_t B, double S, int64_t S_q, int32_t cur_
   return 0;
 }
 
+/* labels renumbered 0..B-1 in ascending order of their values; returns B,
+   or -1 for a negative label */
+int32_t og_compact_labels(const int32_t* init, int32_t n, int32_t* part) {
+  int32_t mx = -1;
+  for (int32_t v = 0; v < n; v++) {
+    if (init[v] < 0) return -1;
+    if (init[v] > mx) mx = init[v];
+  }
+  int32_t* map = malloc(sizeof(int32_t) * ((size_t)mx + 1));
+  for (int32_t i = 0; i <= mx; i++) map[i] = -1;
+  for (int32_t v = 0; v < n; v++) map[init[v]] = 0;
+  int32_t B = 0;
+  for (int32_t i = 0; i <= mx; i++)
+    if (map[i] == 0) map[i] = B++;
+  for (int32_t v = 0; v < n; v++) part[v] = map[init[v]];
+  free(map);
+  return B;
+}
+
+static int og_partition_impl(const og_graph* g, const og_params* p, const int32_t* init, int32_t* part_out,
+                             og_result* res, og_trace_fn trace, void* user);
+
 int og_partition(const og_graph* g, const og_params* p, int32_t* part_out,
                  og_result* res, og_trace_fn trace, void* user) {
+  return og_partition_impl(g, p, NULL, part_out, res, trace, user);
+}
+
+/* the solve from a given initial partition instead of the SCC pass (the
+   CUDA path's usap_ctx_partition_from; streaming input) */
+int og_partition_from(const og_graph* g, const og_params* p, const int32_t* init, int32_t* part_out,
+                      og_result* res, og_trace_fn trace, void* user) {
+  if (!init) return -1;
+  return og_partition_impl(g, p, init, part_out, res, trace, user);
+}
+
+static int og_partition_impl(const og_graph* g, const og_params* p, const int32_t* init, int32_t* part_out,
+                             og_result* res, og_trace_fn trace, void* user) {
   int32_t n = g->n;
   memset(res, 0, sizeof(*res));
   if (n <= 0 || g->e <= 0) return -1;
@@ -879,7 +914,13 @@ int og_partition(const og_graph* g, const og_params* p, int32_t* part_out,
   int32_t work = 0;
   int32_t* part = slots[work];
   int32_t B;
-  if (p->init_mode == 1) {
+  if (init) {
+    B = og_compact_labels(init, n, part);
+    if (B < 0) {
+      for (int i = 0; i < 4; i++) free(slots[i]);
+      return -1;
+    }
+  } else if (p->init_mode == 1) {
     for (int32_t v = 0; v < n; v++) part[v] = v;
     B = n;
   } else {

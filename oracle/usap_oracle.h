@@ -165,6 +165,11 @@ int og_golden_step(og_golden* gs, int32_t B, double S, int64_t S_q, int32_t cur_
 void og_params_default(og_params* p);
 int og_partition(const og_graph* g, const og_params* p, int32_t* part_out,
                  og_result* res, og_trace_fn trace, void* user);
+/* the same from a given initial partition (labels >= 0, renumbered 0..B-1
+ * in ascending order) instead of the SCC pass */
+int og_partition_from(const og_graph* g, const og_params* p, const int32_t* init, int32_t* part_out,
+                      og_result* res, og_trace_fn trace, void* user);
+int32_t og_compact_labels(const int32_t* init, int32_t n, int32_t* part);
 
 /* --- checksums used by traces (order independent where noted) ----------- */
 uint64_t og_hash_part(const int32_t* part, int32_t n);

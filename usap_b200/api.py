@@ -58,6 +58,28 @@ class Context:
         nat.check(nat.lib().usap_ctx_partition(self._h, C.byref(p), nat.p32(out), C.byref(res)))
         return out, nat.result_dict(res)
 
+    def add_edges(self, src, dst, weight=None, n: int = 0, one_based: bool = False) -> None:
+        """Streaming input: append an edge batch to the resident graph
+        (usap_ctx_add_edges); n grows to cover the new vertices."""
+        g, keep = nat.make_graph(src, dst, weight, n, one_based)
+        nat.check(nat.lib().usap_ctx_add_edges(self._h, C.byref(g)))
+        nn = C.c_int32()
+        ee = C.c_int64()
+        nat.check(nat.lib().usap_ctx_num_nodes(self._h, C.byref(nn), C.byref(ee)))
+        self.n, self.e = int(nn.value), int(ee.value)
+
+    def partition_from(self, init, params: Optional[nat.Params] = None, want_assign: bool = True):
+        """partition() started from ``init`` (one block label >= 0 per vertex)
+        instead of the SCC pass (usap_ctx_partition_from)."""
+        ini = np.ascontiguousarray(init, np.int32)
+        if ini.size != self.n:
+            raise ValueError(f"init has {ini.size} labels, the graph {self.n} vertices")
+        p = params if params is not None else nat.default_params()
+        out = np.empty(self.n, np.int32) if want_assign else None
+        res = nat.Result()
+        nat.check(nat.lib().usap_ctx_partition_from(self._h, C.byref(p), nat.p32(ini), nat.p32(out), C.byref(res)))
+        return out, nat.result_dict(res)
+
     def load_tsv(self, text: bytes, n: int = 0) -> None:
         """load_graph_from_tsv from the bytes of a reference-format .tsv file,
         parsed on the device (usap_ctx_load_tsv); n = 0: N is the largest

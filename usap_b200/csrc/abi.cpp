@@ -193,6 +193,25 @@ usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out
   });
 }
 
+usap_status usap_ctx_partition_from(usap_ctx* ctx, const usap_params* p, const int32_t* init,
+                                    int32_t* out_assign, usap_result* out) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (!init || !out) throw usap::Error(USAP_ERR_INVALID, "null argument");
+    usap_params def;
+    usap_params_default(&def);
+    ctx->job->partition(p ? *p : def, out_assign, out, init);
+  });
+}
+
+usap_status usap_ctx_add_edges(usap_ctx* ctx, const usap_graph* g) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (!g) throw usap::Error(USAP_ERR_INVALID, "null graph");
+    ctx->job->add_edges(*g);
+  });
+}
+
 usap_status usap_ctx_evaluate(usap_ctx* ctx, const int32_t* truth, usap_scores* out) {
   return guarded([&] {
     check_ctx(ctx);

@@ -850,7 +850,7 @@ void Job::emit_trace(int kind, int stage, int itr, int beg, int32_t B, const int
 }
 
 // --- the whole solve ------------------------------------------------------------
-void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res) {
+void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res, const int32_t* init) {
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
   USAP_CUDA(cudaSetDevice(device_));
   if (p.num_agg_proposals_per_block < 1) throw Error(USAP_ERR_INVALID, "num_agg_proposals_per_block must be >= 1");
@@ -882,7 +882,9 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   // initial blocks (host): depth-limited DFS on the transpose, or identity
   std::vector<int32_t> part0(n);
   int32_t B;
-  if (p.init_mode == 1) {
+  if (init) {
+    B = compact_labels(init, n, part0.data());
+  } else if (p.init_mode == 1) {
     for (int32_t v = 0; v < n; v++) part0[v] = v;
     B = n;
   } else if (p.dfs_depth != kDefaultDfsDepth || !gr_->take_initial_blocks(&B, &part0)) {
@@ -1119,6 +1121,64 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res)
   res->h2d_bytes = static_cast<long long>(sizeof(int32_t)) * n;   // initial partition
   res->d2h_bytes = d2h;
   res->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+}
+
+// labels renumbered 0..B-1 in ascending order of their values (the
+// oracle's og_compact_labels); returns B
+int32_t compact_labels(const int32_t* init, int32_t n, int32_t* part) {
+  int32_t mx = -1;
+  for (int32_t v = 0; v < n; v++) {
+    if (init[v] < 0) throw Error(USAP_ERR_INVALID, "initial block labels must be >= 0");
+    mx = std::max(mx, init[v]);
+  }
+  if (static_cast<int64_t>(mx) <= 4ll * n + 1024) {
+    std::vector<int32_t> map(static_cast<size_t>(mx) + 1, -1);
+    for (int32_t v = 0; v < n; v++) map[init[v]] = 0;
+    int32_t B = 0;
+    for (auto& m : map)
+      if (m == 0) m = B++;
+    for (int32_t v = 0; v < n; v++) part[v] = map[init[v]];
+    return B;
+  }
+  std::vector<int32_t> u(init, init + n);
+  std::sort(u.begin(), u.end());
+  u.erase(std::unique(u.begin(), u.end()), u.end());
+  for (int32_t v = 0; v < n; v++)
+    part[v] = static_cast<int32_t>(std::lower_bound(u.begin(), u.end(), init[v]) - u.begin());
+  return static_cast<int32_t>(u.size());
+}
+
+void Job::add_edges(const usap_graph& d) {
+  if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
+  if (!d.src || !d.dst || d.e <= 0) throw Error(USAP_ERR_INVALID, "no edges to add");
+  const HostGraph& h = *hg_;
+  const int32_t base = d.one_based ? 1 : 0;
+  int64_t n = std::max<int64_t>(h.n, d.n);
+  for (int64_t i = 0; i < d.e; i++) n = std::max<int64_t>(n, static_cast<int64_t>(d.src[i]) - base + 1);
+  const int64_t e = h.e + d.e;
+  std::vector<int32_t> src(e), dst(e), w;
+  std::copy(h.src.begin(), h.src.end(), src.begin());
+  std::copy(h.dst.begin(), h.dst.end(), dst.begin());
+  for (int64_t i = 0; i < d.e; i++) {
+    src[h.e + i] = d.src[i] - base;
+    dst[h.e + i] = d.dst[i] - base;
+  }
+  bool unit = h.unit && !d.weight;
+  if (d.weight)
+    for (int64_t i = 0; i < d.e; i++) unit = unit && d.weight[i] == 1;
+  if (!unit) {
+    w.assign(e, 1);
+    if (!h.unit) std::copy(h.w.begin(), h.w.end(), w.begin());
+    if (d.weight) std::copy(d.weight, d.weight + d.e, w.begin() + h.e);
+  }
+  usap_graph g{};
+  g.n = static_cast<int32_t>(n);
+  g.e = e;
+  g.src = src.data();
+  g.dst = dst.data();
+  g.weight = unit ? nullptr : w.data();
+  g.one_based = 0;
+  load(g);
 }
 
 // scores of the last solve's partition, evaluated where it lies in HBM

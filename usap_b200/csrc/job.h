@@ -45,6 +45,9 @@ int32_t scc_host(const HostGraph& g, int32_t dfs_depth, int32_t* part);
 
 // host evaluation (evaluate.hpp:18-266 scores + NMI + Hungarian accuracy)
 void evaluate_host(const int32_t* truth, const int32_t* given, int64_t n, usap_scores* out);
+// labels renumbered 0..B-1 in ascending order of their values; returns B
+int32_t compact_labels(const int32_t* init, int32_t n, int32_t* part);
+
 // edges parsed on the device from the text of a reference-format .tsv
 // file (kernels_tsv.cu): 0-based ids in file order, weights empty when all
 // are 1; max_src is the reference's N
@@ -187,7 +190,12 @@ class Job {
     trace_ = fn;
     trace_user_ = user;
   }
-  void partition(const usap_params& p, int32_t* out_assign, usap_result* res);
+  // init (n labels >= 0, renumbered 0..B-1 in ascending order) replaces
+  // the SCC pass as the initial partition when given
+  void partition(const usap_params& p, int32_t* out_assign, usap_result* res, const int32_t* init = nullptr);
+  // streaming input: the resident graph becomes its edges followed by
+  // these, with n grown to cover them
+  void add_edges(const usap_graph& delta);
   // bf::evaluate scores of the last partition() result against truth (host
   // array of n labels), computed on the device where the result lies
   void evaluate_last(const int32_t* truth, usap_scores* out);

@@ -112,7 +112,8 @@ class ServerStats(C.Structure):
 # every exported symbol of include/usap.h
 EXPORTS = ("usap_version", "usap_last_error", "usap_params_default", "usap_partition",
            "usap_evaluate", "usap_evaluate_device", "usap_ctx_evaluate", "usap_ctx_create",
-           "usap_ctx_destroy", "usap_ctx_load", "usap_ctx_load_tsv",
+           "usap_ctx_destroy", "usap_ctx_load", "usap_ctx_load_tsv", "usap_ctx_add_edges",
+           "usap_ctx_partition_from",
            "usap_ctx_num_nodes", "usap_ctx_partition", "usap_ctx_set_trace", "usap_op_scc",
            "usap_op_build", "usap_op_entropy", "usap_op_merge_phase", "usap_op_merge_apply",
            "usap_op_nodal_batch", "usap_op_merge_phase_prec", "usap_op_nodal_batch_prec",
@@ -141,6 +142,8 @@ def lib() -> C.CDLL:
     L.usap_evaluate_device.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.POINTER(Scores)]
     L.usap_ctx_evaluate.argtypes = [C.c_void_p, i32p, C.POINTER(Scores)]
     L.usap_ctx_load_tsv.argtypes = [C.c_void_p, C.c_char_p, C.c_int64, C.c_int32]
+    L.usap_ctx_add_edges.argtypes = [C.c_void_p, C.POINTER(Graph)]
+    L.usap_ctx_partition_from.argtypes = [C.c_void_p, C.POINTER(Params), i32p, i32p, C.POINTER(Result)]
     L.usap_ctx_create.argtypes = [C.c_int32, C.POINTER(C.c_void_p)]
     L.usap_ctx_destroy.argtypes = [C.c_void_p]
     L.usap_ctx_load.argtypes = [C.c_void_p, C.POINTER(Graph)]

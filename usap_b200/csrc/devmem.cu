@@ -12,6 +12,7 @@
 #include <mutex>
 #include <vector>
 
+#include "../../include/usap.h"
 #include "engine.h"
 
 namespace usap {
@@ -56,6 +57,41 @@ void* dev_alloc(size_t bytes, cudaStream_t st) {
 
 void dev_free(void* p, cudaStream_t st) {
   if (p) cudaFreeAsync(p, st);
+}
+
+DeviceLogTable::~DeviceLogTable() {
+  if (L) cudaFree(L);
+  if (L2) cudaFree(L2);
+}
+
+namespace {
+std::mutex g_dlog_mu[kMaxDevices];
+std::shared_ptr<const DeviceLogTable> g_dlog[kMaxDevices];
+}  // namespace
+
+std::shared_ptr<const DeviceLogTable> device_log_table(int device, int64_t max_k, int64_t* uploaded) {
+  if (uploaded) *uploaded = 0;
+  if (device < 0 || device >= kMaxDevices) throw Error(USAP_ERR_INVALID, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_dlog_mu[device]);
+  std::shared_ptr<const DeviceLogTable>& cur = g_dlog[device];
+  if (cur && cur->size > max_k) return cur;
+  // grow geometrically so that a stream of slightly larger graphs uploads rarely
+  const int64_t size = std::max<int64_t>(max_k + 1, cur ? 2 * cur->size : max_k + 1);
+  const std::shared_ptr<const std::vector<double>> host = log_table(size - 1);
+  auto t = std::make_shared<DeviceLogTable>();
+  USAP_CUDA(cudaSetDevice(device));
+  USAP_CUDA(cudaMalloc(reinterpret_cast<void**>(&t->L), sizeof(double) * size));
+  USAP_CUDA(cudaMalloc(reinterpret_cast<void**>(&t->L2), sizeof(float2) * size));
+  t->size = size;
+  cudaStream_t st = nullptr;
+  USAP_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  USAP_CUDA(cudaMemcpyAsync(t->L, host->data(), sizeof(double) * size, cudaMemcpyHostToDevice, st));
+  launch_log_pairs(t->L, t->L2, size, st);
+  USAP_CUDA(cudaStreamSynchronize(st));   // ready for every stream before anyone gets it
+  USAP_CUDA(cudaStreamDestroy(st));
+  if (uploaded) *uploaded = static_cast<int64_t>(sizeof(double) * size);
+  cur = t;
+  return cur;
 }
 
 std::shared_ptr<const std::vector<double>> log_table(int64_t max_k) {

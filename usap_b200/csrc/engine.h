@@ -78,6 +78,20 @@ void* dev_alloc(size_t bytes, cudaStream_t st);
 void dev_free(void* p, cudaStream_t st);
 std::shared_ptr<const std::vector<double>> log_table(int64_t max_k);
 
+// The same table on a device, as FP64 values and as float pairs (the FP32
+// precision modes), for k < size.  One per device for the process: graphs
+// share it, and it is replaced by a larger one when a graph needs more
+// entries (holders keep the table they were given alive).
+struct DeviceLogTable {
+  double* L = nullptr;
+  float2* L2 = nullptr;
+  int64_t size = 0;
+  ~DeviceLogTable();
+};
+// the device's table with at least max_k + 1 entries; *uploaded = bytes
+// copied to the device by this call (0 when the current table was enough)
+std::shared_ptr<const DeviceLogTable> device_log_table(int device, int64_t max_k, int64_t* uploaded);
+
 // Dense block matrix view: M[x*ld + y], transposed copy Mt[y*ld + x], and
 // per-row chunk sums CS[u*cld + c] of M[u,i]+M[i,u] over blocks
 // i in [128c, 128c+128).

@@ -283,7 +283,6 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
       }
     }
   }
-  const std::shared_ptr<const std::vector<double>> logk_all = log_table(wtot);
 
   auto gr = std::make_shared<GraphResident>(device);
   // the first solve's initial blocks, on a host thread while the graph
@@ -346,13 +345,13 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
                               cudaMemcpyHostToDevice, st_));
     up_bytes += static_cast<long long>(sizeof(int64_t) * h.chunk_ptr.size());
   }
-  dalloc(&g.logk, wtot + 1);
-  USAP_CUDA(cudaMemcpyAsync(g.logk, logk_all->data(), sizeof(double) * (wtot + 1), cudaMemcpyHostToDevice, st_));
-  dalloc(&g.logk2, wtot + 1);
-  launch_log_pairs(g.logk, g.logk2, wtot + 1, st_);
+  int64_t log_bytes = 0;
+  gr->logs = device_log_table(device, wtot, &log_bytes);
+  g.logk = gr->logs->L;
+  g.logk2 = gr->logs->L2;
   dalloc(&g.hi_off, n);
   USAP_CUDA(cudaMemcpyAsync(g.hi_off, hi_off.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, st_));
-  up_bytes += static_cast<long long>(sizeof(double) * (wtot + 1) + sizeof(int64_t) * n +
+  up_bytes += static_cast<long long>(log_bytes + sizeof(int64_t) * n +
                                      sizeof(int32_t) * hubs.size());
   g.hi_slots = hi_slots;
   dalloc(&gr->hubs_dev, hubs.size());
@@ -393,7 +392,7 @@ GraphResident::~GraphResident() {
   dfree(g.out_ptr); dfree(g.out_idx); dfree(g.out_w);
   dfree(g.in_ptr); dfree(g.in_idx); dfree(g.in_w);
   dfree(g.chunks); dfree(g.chunk_ptr);
-  dfree(g.kout); dfree(g.kin); dfree(g.logk); dfree(g.logk2);
+  dfree(g.kout); dfree(g.kin);   // the log tables belong to the device (logs)
   dfree(g.hi_off);
   dfree(hubs_dev);
   if (st) {

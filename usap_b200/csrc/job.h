@@ -108,6 +108,7 @@ struct GraphResident {
   std::mutex scc_mu;
   std::future<int32_t> scc_b;          // B of scc_part, once the host thread is done
   std::vector<int32_t> scc_part;
+  std::shared_ptr<const DeviceLogTable> logs;   // log k for k <= the total edge weight
   HostGraph hg;
   GraphDev g;                      // hkey/hwo/hwi belong to the jobs
   std::vector<int32_t> hub_ids;    // vertices of degree > kHubDegree, ascending

@@ -267,7 +267,9 @@ usap_status usap_op_nodal_batch(usap_ctx* ctx, int32_t* part, int32_t B, int32_t
                                 int32_t* prop_ninf, int64_t* cum_q, int32_t* cum_ninf,
                                 int64_t* moves);
 /* The same two operations in a given precision mode (usap_params.precision;
- * no counterpart in the reference, whose dS is single precision throughout).
+ * no counterpart in the reference, whose dS is single precision throughout),
+ * on the path a solve takes at this B: the merge phase reads the dense tile
+ * when B <= 4096 (the plain usap_op_merge_phase always uses sorted views).
  * In modes 1 and 2, dS is evaluated in FP32 beside the exact FP64 value and
  * decisions are taken on the FP32 value: prop_q gets the exact FP64 values
  * (Q32) and prop_f the FP32 ones (the float pair's value hi + lo, which is

@@ -111,6 +111,23 @@ def test_merge_phase_exact(case):
             assert np.array_equal(best_s, obs) and np.array_equal(best_q, obq)
 
 
+def test_merge_phase_dense_exact(case):
+    """the merge phase on the dense tile (what a solve runs for B <= 4096)"""
+    name, ctx, og, states = case
+    K = 10
+    for sname, (B, part) in states.items():
+        for stage, seed in ((0, 0), (3, 12345678901)):
+            best_s, best_q, ps, pq, _, _ = ctx.op_merge_phase(part, B, K, stage, seed, dense=True)
+            blk = og.blocks(part, B)
+            obs, obq = blk.merge_phase(K, stage, seed)
+            for r in range(B):
+                for k in range(K):
+                    s = blk.merge_propose(r, k, stage, seed)
+                    assert ps[r, k] == s, (name, sname, r, k)
+                    assert pq[r, k] == blk.merge_dq(r, s), (name, sname, r, k)
+            assert np.array_equal(best_s, obs) and np.array_equal(best_q, obq)
+
+
 def _merge_apply_cases(B, rng):
     """best targets and dS with ties, self targets, 2-cycles and longer cycles"""
     out = []

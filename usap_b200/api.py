@@ -132,15 +132,18 @@ class Context:
         nat.check(nat.lib().usap_op_entropy(self._h, nat.p32(part), B, dense_max, C.byref(S)))
         return int(S.value)
 
-    def op_merge_phase(self, part, B: int, K: int, stage: int, seed: int, precision: int = 0):
-        """block_merge task; in precision mode 1 or 2 also returns the FP32 dS
-        of every proposal and the number of blocks whose choice flipped."""
+    def op_merge_phase(self, part, B: int, K: int, stage: int, seed: int, precision: int = 0,
+                       dense: bool = False):
+        """block_merge task on sorted views; with ``dense`` or a precision mode
+        (usap_op_merge_phase_prec) on the path a solve takes, the dense tile
+        for B <= 4096, and then also the FP32 dS of every proposal and the
+        number of blocks whose choice flipped."""
         part = np.ascontiguousarray(part, np.int32)
         best_s = np.empty(B, np.int32)
         best_q = np.empty(B, np.int64)
         ps = np.empty(B * K, np.int32)
         pq = np.empty(B * K, np.int64)
-        if not precision:
+        if not precision and not dense:
             nat.check(nat.lib().usap_op_merge_phase(self._h, nat.p32(part), B, K, stage, seed,
                                                     nat.p32(best_s), nat.p64(best_q), nat.p32(ps),
                                                     nat.p64(pq)))

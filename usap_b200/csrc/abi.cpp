@@ -436,7 +436,9 @@ usap_status usap_op_merge_phase_prec(usap_ctx* ctx, const int32_t* part, int32_t
     check_ctx(ctx);
     check_part(ctx, part, B);
     if (!best_s || !best_q) throw usap::Error(USAP_ERR_INVALID, "null output");
-    ctx->job->op_merge_phase(part, B, K, stage, seed, best_s, best_q, prop_s, prop_q, precision, prop_f, flips);
+    // the path a solve takes at this B: the dense tile up to 4096 blocks
+    ctx->job->op_merge_phase(part, B, K, stage, seed, best_s, best_q, prop_s, prop_q, precision, prop_f, flips,
+                             4096);
   });
 }
 

@@ -273,6 +273,8 @@ void launch_entropy_sorted(const GraphDev& g, SortedView v, const int* nnz_dev, 
                            unsigned long long* acc, cudaStream_t st);
 
 void launch_merge_propose(const GraphDev& g, SortedView v, const MergeArgs& a, cudaStream_t st);
+// the same on the dense tile (B <= dense_max; M, Mt and the chunk sums current)
+void launch_merge_propose_dense(DenseView v, const MergeArgs& a, cudaStream_t st);
 // prop_x / best_x / f32: precision modes 1, 2 only (else null)
 void launch_merge_argmin(int B, int K, const int32_t* prop_s, const long long* prop_q, const long long* prop_x,
                          int32_t* best_s, long long* best_q, long long* best_x, F32Tally* f32, cudaStream_t st);

@@ -541,9 +541,14 @@ void Job::prepare_nodal_blocks(const int32_t* part, int32_t B, bool dense) {
   }
 }
 
-void Job::merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage, uint64_t seed) {
-  launch_degrees(g_, part, B, dout_, din_, st_);
-  sb_.build(g_, part, B, true, true, st_);
+void Job::merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage, uint64_t seed, bool dense) {
+  // dense: the tile (and its chunk sums) the nodal phase uses, else sorted views
+  if (dense) {
+    prepare_nodal_blocks(part, B, true);
+  } else {
+    launch_degrees(g_, part, B, dout_, din_, st_);
+    sb_.build(g_, part, B, true, true, st_);
+  }
   MergeArgs a;
   a.L = g_.logk;
   a.B = B;
@@ -559,7 +564,8 @@ void Job::merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage,
   a.prop_x = prec_ ? prop_x_ : nullptr;
   a.prop_f = prec_ ? prop_f_ : nullptr;
   a.f32 = prec_ ? f32d_ : nullptr;
-  launch_merge_propose(g_, sb_.view(), a, st_);
+  if (dense) launch_merge_propose_dense(dense_view(), a, st_);
+  else launch_merge_propose(g_, sb_.view(), a, st_);
   launch_merge_argmin(B, K, prop_s_, prop_q_, a.prop_x, best_s_, best_q_, prec_ ? best_x_ : nullptr, a.f32, st_);
 }
 
@@ -907,7 +913,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
     int32_t* part = slots_[work];
     auto tm0 = std::chrono::steady_clock::now();
     // merge phase and its application
-    merge_phase(part, B, K, stage, seed);
+    merge_phase(part, B, K, stage, seed, B <= dense_max);
     int32_t merged = merge_apply(part, B, btm);
     if (prec_) launch_order_flips(B, sidx_alt_, best_x_, &f32d_[1].flips, st_);
     d2h += sizeof(int32_t);
@@ -1154,6 +1160,7 @@ void Job::add_edges(const usap_graph& d) {
   const int32_t base = d.one_based ? 1 : 0;
   int64_t n = std::max<int64_t>(h.n, d.n);
   for (int64_t i = 0; i < d.e; i++) n = std::max<int64_t>(n, static_cast<int64_t>(d.src[i]) - base + 1);
+  if (n > INT32_MAX) throw Error(USAP_ERR_LIMIT, "more than 2^31 - 1 vertices");
   const int64_t e = h.e + d.e;
   std::vector<int32_t> src(e), dst(e), w;
   std::copy(h.src.begin(), h.src.end(), src.begin());
@@ -1253,16 +1260,16 @@ int64_t Job::op_entropy(const int32_t* part, int32_t B, int32_t dense_max) {
 
 void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
                          int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q, int prec,
-                         double* prop_f, int64_t* flips) {
+                         double* prop_f, int64_t* flips, int32_t dense_max) {
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
   if (K < 1) throw Error(USAP_ERR_INVALID, "K must be >= 1");
   USAP_CUDA(cudaSetDevice(device_));
-  ensure_capacity(B, K, 1, 1);
+  ensure_capacity(B, K, dense_max, 1);
   if (prec < 0 || prec > 2) throw Error(USAP_ERR_INVALID, "precision must be 0, 1 or 2");
   prec_ = prec;
   if (prec_) USAP_CUDA(cudaMemsetAsync(f32d_, 0, 2 * sizeof(F32Tally), st_));
   USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
-  merge_phase(slots_[0], B, K, static_cast<uint32_t>(stage), seed);
+  merge_phase(slots_[0], B, K, static_cast<uint32_t>(stage), seed, B <= dense_max);
   const size_t nk = static_cast<size_t>(B) * K;
   USAP_CUDA(cudaMemcpyAsync(best_s, best_s_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaMemcpyAsync(best_q, best_q_, sizeof(int64_t) * B, cudaMemcpyDeviceToHost, st_));

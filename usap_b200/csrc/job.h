@@ -214,7 +214,7 @@ class Job {
   // prop_f the FP32 ones, *flips the blocks whose FP32 choice differs)
   void op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stage, uint64_t seed,
                       int32_t* best_s, int64_t* best_q, int32_t* prop_s, int64_t* prop_q, int prec = 0,
-                      double* prop_f = nullptr, int64_t* flips = nullptr);
+                      double* prop_f = nullptr, int64_t* flips = nullptr, int32_t dense_max = 1);
   void op_merge_apply(int32_t* part, int32_t B, const int32_t* best_s, const int64_t* best_q,
                       int32_t btm, int32_t* B_new, int32_t* merged);
   void op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t beg, int32_t end,
@@ -232,7 +232,7 @@ class Job {
   void ensure_capacity(int32_t B, int32_t K, int32_t dense_max, int32_t maxitr);
   // block structures for a nodal phase / batch
   void prepare_nodal_blocks(const int32_t* part, int32_t B, bool dense);
-  void merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage, uint64_t seed);
+  void merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage, uint64_t seed, bool dense);
   int32_t merge_apply(int32_t* part, int32_t B, int32_t btm);
   void entropy_launch(const int32_t* part, int32_t B, bool dense);
   void nodal_batch(int32_t* part, int32_t B, bool dense, int32_t beg, int32_t end, uint32_t stage,

@@ -886,6 +886,151 @@ __global__ void __launch_bounds__(kHubThreads) k_nodal_propose_hub(NodalArgs a, 
   if (a.stats && threadIdx.x == 0 && my_bytes) atomicAdd(&a.ctl->bytes, my_bytes);
 }
 
+// --- block-merge proposals on the dense tile ------------------------------------
+// The block_merge task (graph_parallel.hpp:349-368, _propose_new_partition_block
+// :761-988) for B <= dense_max, reading the tile the nodal phase keeps (M, its
+// transpose, the chunk sums) instead of sorted sparse views.  Draws, candidate
+// order and the Q32 terms are those of the sparse kernel (kernels_merge.cu):
+// the symmetric row M[u,:]+M[:,u] is walked in block-id order through the
+// chunk sums, and the rows and columns of r and s are scanned whole, every
+// column where both are non-zero giving one h term.
+
+// sum of M[u,i] + M[i,u] over i < r (warp-collective, every lane returns it)
+__device__ __forceinline__ long long sym_prefix(const DenseView& v, int u, int r, int lane) {
+  const int c = r / kChunk;
+  long long acc = 0;
+  const int* cs = v.CS + static_cast<long long>(u) * v.cld;
+  for (int q = lane; q < c; q += 32) acc += __ldg(cs + q);
+  const int* mrow = v.M + static_cast<long long>(u) * v.ld;
+  const int* trow = v.Mt + static_cast<long long>(u) * v.ld;
+  for (int i = c * kChunk + lane; i < r; i += 32) acc += __ldg(mrow + i) + __ldg(trow + i);
+  return warp_sum_ll(acc);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_merge_propose_dense(DenseView v, MergeArgs a) {
+  constexpr bool F32 = P > 0;
+  __shared__ F32Tally s_f32;
+  if (F32) {
+    if (threadIdx.x == 0) s_f32 = F32Tally{0, 0, 0, 0.0};
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const DenseOps ops{v, a.B};
+  const Grp<32> g(lane);
+  const long long items = static_cast<long long>(a.B) * a.K;
+  const long long nwarps = static_cast<long long>(gridDim.x) * kWarps;
+  for (long long item = static_cast<long long>(blockIdx.x) * kWarps + (threadIdx.x >> 5); item < items;
+       item += nwarps) {
+    const int r = static_cast<int>(item / a.K), k = static_cast<int>(item - static_cast<long long>(r) * a.K);
+    const int B = a.B;
+    const Draws x = philox(static_cast<uint32_t>(r), static_cast<uint32_t>(k), a.stage, kTagMerge, a.seed);
+    const long long dr_out = __ldg(a.dout + r), dr_in = __ldg(a.din + r);
+    const long long ka = dr_out + dr_in;
+    int s;
+    int scanned = 0;
+    if (ka == 0) {
+      s = static_cast<int>(draw_below(x.x2, B));
+    } else {
+      const int u = ops.sym_sample(r, static_cast<long long>(draw_below(x.x0, ka)), g, &scanned);
+      const long long dau = static_cast<long long>(__ldg(a.dout + u)) + __ldg(a.din + u);
+      if (accept_uniform(x.x1, dau, B)) {
+        s = skip_r(static_cast<int>(draw_below(x.x2, B)), r, B);
+      } else {
+        // the multinomial over row u with r left out
+        const long long c_ur = static_cast<long long>(ops.get(u, r)) + ops.get(r, u);
+        const long long before = sym_prefix(v, u, r, lane);
+        const long long wsum = dau - c_ur;
+        if (wsum == 0) {
+          s = skip_r(static_cast<int>(draw_below(x.x2, B)), r, B);
+        } else {
+          long long t2 = draw_below(x.x2, wsum);
+          if (c_ur > 0 && t2 >= before) t2 += c_ur;
+          s = ops.sym_sample(u, t2, g, &scanned);
+        }
+      }
+    }
+    // --- dS of merging r into s ---
+    const long long ds_out = __ldg(a.dout + s), ds_in = __ldg(a.din + s);
+    const long long ds_out_n = ds_out + dr_out, ds_in_n = ds_in + dr_in;
+    int e4 = 0;
+    if (lane < 4) e4 = ops.get(lane < 2 ? r : s, (lane & 1) ? s : r);
+    const long long Mrr = __shfl_sync(0xffffffffu, e4, 0), Mrs = __shfl_sync(0xffffffffu, e4, 1);
+    const long long Msr = __shfl_sync(0xffffffffu, e4, 2), Mss = __shfl_sync(0xffffffffu, e4, 3);
+    long long acc = 0;
+    FF f{0.0f, 0.0f};
+    // rows r and s (M) and columns r and s (rows of Mt): columns i not in
+    // {r, s} where both entries are non-zero
+    const int* mr = v.M + static_cast<long long>(r) * v.ld;
+    const int* ms = v.M + static_cast<long long>(s) * v.ld;
+    const int* tr = v.Mt + static_cast<long long>(r) * v.ld;
+    const int* ts = v.Mt + static_cast<long long>(s) * v.ld;
+    for (int i = lane; i < B; i += 32) {
+      if (i == r || i == s) continue;
+      const int xr = __ldg(mr + i), xs = __ldg(ms + i);
+      if (xr > 0 && xs > 0) {
+        acc += q32(h_term(a.L, xr, xs));
+        if constexpr (F32) f = ff_add(f, h_term_ff<P>(a.L2, xr, xs));
+      }
+      const int yr = __ldg(tr + i), ys = __ldg(ts + i);
+      if (yr > 0 && ys > 0) {
+        acc += q32(h_term(a.L, yr, ys));
+        if constexpr (F32) f = ff_add(f, h_term_ff<P>(a.L2, yr, ys));
+      }
+    }
+    acc = warp_sum_ll(acc);
+    if constexpr (F32) f = g.ffsum(f);
+    if (lane == 0) {
+      acc += q32(g_term(a.L, Mrr, dr_in, dr_out));
+      acc += q32(g_term(a.L, Mrs, ds_in, dr_out));
+      acc += q32(g_term(a.L, Msr, dr_in, ds_out));
+      acc += q32(g_term(a.L, Mss, ds_in, ds_out));
+      acc -= q32(g_term(a.L, Mrr + Mrs + Msr + Mss, ds_in_n, ds_out_n));
+      long long Ar, As, Cr, Cs;
+      if (s != r) {
+        Ar = dr_out - Mrr - Mrs;
+        As = ds_out - Msr - Mss;
+        Cr = dr_in - Mrr - Msr;
+        Cs = ds_in - Mrs - Mss;
+      } else {
+        Ar = As = dr_out - Mrr;
+        Cr = Cs = dr_in - Mrr;
+      }
+      acc += q32(coef_term(a.L, Ar, ds_out_n, dr_out));
+      acc += q32(coef_term(a.L, As, ds_out_n, ds_out));
+      acc += q32(coef_term(a.L, Cr, ds_in_n, dr_in));
+      acc += q32(coef_term(a.L, Cs, ds_in_n, ds_in));
+      a.prop_s[item] = s;
+      if constexpr (F32) {
+        const float2* __restrict__ T = a.L2;
+        f = ff_add(f, g_term_ff<P>(T, Mrr, dr_in, dr_out));
+        f = ff_add(f, g_term_ff<P>(T, Mrs, ds_in, dr_out));
+        f = ff_add(f, g_term_ff<P>(T, Msr, dr_in, ds_out));
+        f = ff_add(f, g_term_ff<P>(T, Mss, ds_in, ds_out));
+        f = ff_sub(f, g_term_ff<P>(T, Mrr + Mrs + Msr + Mss, ds_in_n, ds_out_n));
+        f = ff_add(f, coef_ff<P>(Ar, ld_ff(T, ds_out_n), ld_ff(T, dr_out)));
+        f = ff_add(f, coef_ff<P>(As, ld_ff(T, ds_out_n), ld_ff(T, ds_out)));
+        f = ff_add(f, coef_ff<P>(Cr, ld_ff(T, ds_in_n), ld_ff(T, dr_in)));
+        f = ff_add(f, coef_ff<P>(Cs, ld_ff(T, ds_in_n), ld_ff(T, ds_in)));
+        const double fv = ff_value(f);
+        a.prop_q[item] = q32(fv);
+        a.prop_x[item] = acc;
+        a.prop_f[item] = fv;
+        const double err = f32_err(fv, acc);
+        atomicAdd(&s_f32.evals, 1ull);
+        atomicMax(&s_f32.err_max, static_cast<unsigned long long>(__double_as_longlong(err)));
+        atomicAdd(&s_f32.err_sum, err);
+      } else {
+        a.prop_q[item] = acc;
+      }
+    }
+  }
+  if (F32) {
+    __syncthreads();
+    if (threadIdx.x == 0) f32_tally_flush(&s_f32, a.f32);
+  }
+}
+
 // chunk sums CS[u][c] = sum over the chunk's blocks i of M[u,i] + M[i,u]
 __global__ void __launch_bounds__(kThreads) k_chunk_sums(int B, int ld, const int* __restrict__ M,
                                                         const int* __restrict__ Mt, int cld,
@@ -1769,6 +1914,17 @@ void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList
   if (a.prec == 1) launch_propose(a, SortedOpsT<1>{v, a.B}, hubs, sp);
   else if (a.prec == 2) launch_propose(a, SortedOpsT<2>{v, a.B}, hubs, sp);
   else launch_propose(a, SortedOps{v, a.B}, hubs, sp);
+}
+
+void launch_merge_propose_dense(DenseView v, const MergeArgs& a, cudaStream_t st) {
+  long long items = static_cast<long long>(a.B) * a.K;
+  long long blocks = (items + kWarps - 1) / kWarps;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks < 1) blocks = 1;
+  if (a.prec == 1) k_merge_propose_dense<1><<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
+  else if (a.prec == 2) k_merge_propose_dense<2><<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
+  else k_merge_propose_dense<0><<<static_cast<int>(blocks), kThreads, 0, st>>>(v, a);
+  USAP_LAUNCHED();
 }
 
 void launch_chunk_sums(int B, DenseView v, int* CS, cudaStream_t st) {

@@ -162,7 +162,8 @@ __global__ void k_tsv_parse(const char* __restrict__ text, int64_t len, const in
 
 TsvEdges parse_tsv_device(int device, const char* text, int64_t len) {
   if (!text || len < 0) throw Error(USAP_ERR_INVALID, "null text");
-  if (len > (int64_t(1) << 40)) throw Error(USAP_ERR_LIMIT, "text too large");
+  // line counts and offsets are int32: at most 2^31 - 1 bytes of text
+  if (len > static_cast<int64_t>(INT_MAX)) throw Error(USAP_ERR_LIMIT, "tsv text above 2^31 - 1 bytes");
   USAP_CUDA(cudaSetDevice(device));
   pool_configure(device);
   cudaStream_t st = nullptr;
@@ -185,9 +186,7 @@ TsvEdges parse_tsv_device(int device, const char* text, int64_t len) {
   if (len == 0) return out;
   char* d_text = static_cast<char*>(alloc(static_cast<size_t>(len)));
   USAP_CUDA(cudaMemcpyAsync(d_text, text, static_cast<size_t>(len), cudaMemcpyHostToDevice, st));
-  const int64_t blocks64 = (len + kChunk - 1) / kChunk;
-  if (blocks64 > INT_MAX / 2) throw Error(USAP_ERR_LIMIT, "text too large");
-  const int blocks = static_cast<int>(blocks64);
+  const int blocks = static_cast<int>((len + kChunk - 1) / kChunk);
   int* counts = static_cast<int*>(alloc(sizeof(int) * (blocks + 1)));
   int* offsets = static_cast<int*>(alloc(sizeof(int) * (blocks + 1)));
   k_tsv_count<<<blocks, kThreads, 0, st>>>(d_text, len, counts);

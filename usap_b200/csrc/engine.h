@@ -68,6 +68,9 @@ LaunchCount& launch_count();
 // memory (3 ints per slot), larger ones use the vertex's global region.
 constexpr int kHubDegree = 128;
 constexpr int kHubSmemSlots = 16384;
+// the persistent kernels' hub table (shared memory): hubs whose table is
+// larger get a region of global memory, so those kernels take any B
+constexpr int kPhaseHubSlots = 8192;
 
 // process-wide device memory pool and host tables (devmem.cu)
 void pool_configure(int device);

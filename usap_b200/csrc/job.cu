@@ -277,7 +277,7 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
     if (deg > kHubDegree) {
       hubs.push_back(v);
       int cap = 1 << hash_lg(deg);
-      if (cap > kHubSmemSlots) {
+      if (cap > kPhaseHubSlots) {   // beyond the smaller shared-memory table of the two kernels
         hi_off[v] = hi_slots;
         hi_slots += cap;
       }
@@ -913,7 +913,9 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
     int32_t* part = slots_[work];
     auto tm0 = std::chrono::steady_clock::now();
     // merge phase and its application
-    merge_phase(part, B, K, stage, seed, B <= dense_max);
+    // the dense merge scans whole rows (K B^2 reads): below 4096 blocks it
+    // beats rebuilding the sorted views, above it does not
+    merge_phase(part, B, K, stage, seed, B <= std::min(dense_max, kDenseMergeMax));
     int32_t merged = merge_apply(part, B, btm);
     if (prec_) launch_order_flips(B, sidx_alt_, best_x_, &f32d_[1].flips, st_);
     d2h += sizeof(int32_t);
@@ -934,7 +936,8 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
     const double model_d = model_S(n, hg_->e, B);
     trace_prev_moves_ = 0;
     const bool phase_ok = dense && !use_graphs && maxitr > 0 && B <= nodal_phase_max_blocks() && !trace_on(2);
-    const bool in_gang = gang_ != nullptr && phase_ok && !stats;
+    // the gang's delta-table keys pack (job, cell) into 31 bits: B <= 4096
+    const bool in_gang = gang_ != nullptr && phase_ok && !stats && B <= 4096;
     const int pgrid = phase_ok && (p.persistent || in_gang) ? nodal_phase_grid(device_) : 0;
     const int pctas = p.persistent_ctas > 0 ? std::min(pgrid, static_cast<int>(p.persistent_ctas)) : pgrid;
     if (pgrid > 0) {
@@ -1269,7 +1272,7 @@ void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stag
   prec_ = prec;
   if (prec_) USAP_CUDA(cudaMemsetAsync(f32d_, 0, 2 * sizeof(F32Tally), st_));
   USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
-  merge_phase(slots_[0], B, K, static_cast<uint32_t>(stage), seed, B <= dense_max);
+  merge_phase(slots_[0], B, K, static_cast<uint32_t>(stage), seed, B <= std::min(dense_max, kDenseMergeMax));
   const size_t nk = static_cast<size_t>(B) * K;
   USAP_CUDA(cudaMemcpyAsync(best_s, best_s_, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaMemcpyAsync(best_q, best_q_, sizeof(int64_t) * B, cudaMemcpyDeviceToHost, st_));

@@ -91,6 +91,9 @@ inline double desc_length(double model, long long data_q) {
 // A graph loaded into HBM (CSR, edge list, log table, hub list); read-only
 // once loaded and shared by every job that solves it.  Its device arrays
 // are allocated and released on its own stream.
+// largest B whose merge phase reads the dense tile (row scans, K B^2 reads)
+constexpr int32_t kDenseMergeMax = 4096;
+
 // the reference's default DFS depth (graph_parallel.hpp:51)
 constexpr int32_t kDefaultDfsDepth = 20;
 

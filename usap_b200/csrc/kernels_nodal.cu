@@ -1325,7 +1325,8 @@ constexpr int kPThreads = 768;    // one CTA per SM (80 registers a thread)
 constexpr int kPWarps = kPThreads / 32;
 constexpr int kUnitWarp = -2;     // work unit of one vertex with 64 < degree <= 128
 constexpr int kPHubLg = 13;
-constexpr int kPHubSlots = 1 << kPHubLg;  // hub table slots: 2 * min(deg, B) rounded up, B <= 4096
+constexpr int kPHubSlots = 1 << kPHubLg;  // hub table slots in shared memory; larger hub tables are global
+static_assert(kPHubSlots == kPhaseHubSlots, "hub regions are assigned for tables beyond this size");
 constexpr unsigned long long kBarrierTimeoutNs = 200ull * 1000ull * 1000ull;
 // dynamic shared memory: per-warp tables and lists, then the hub table
 constexpr size_t kPWarpInts = 3 * kHCap + kHubDegree;
@@ -1867,7 +1868,8 @@ int nodal_gang_grid(int device) {
   return g_gang_grid[device];
 }
 
-int nodal_phase_max_blocks() { return 2 * kPHubSlots / 4; }
+// the apply pass keys a tile cell as x * ld + y in 31 bits
+int nodal_phase_max_blocks() { return 32768; }
 
 // the cooperative kernels of precision mode `prec` (0, 1, 2)
 static const void* gang_kernel(int prec) {

@@ -1056,15 +1056,19 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
     }
     res->edge_visits += static_cast<int64_t>(h_ctl_->edge_visits);
     res->nodal_kernel_bytes += static_cast<double>(h_ctl_->bytes);
-    // description length of the finished stage
-    if (!dense) sb_.build(g_, part, B, false, true, st_);
-    entropy_launch(part, B, dense);
-    USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
-    wait();
-    const long long data_fin = -static_cast<long long>(h_ctl_->entropy_acc);
+    // description length of the finished stage: the cooperative kernels
+    // computed its data term at the end of the phase
+    long long data_fin = -static_cast<long long>(h_ctl_->entropy_acc);
+    if (pgrid <= 0) {
+      if (!dense) sb_.build(g_, part, B, false, true, st_);
+      entropy_launch(part, B, dense);
+      USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));
+      wait();
+      data_fin = -static_cast<long long>(h_ctl_->entropy_acc);
+      d2h += sizeof(NodalCtl);
+    }
     const double S_fin = desc_length(model_d, data_fin);
     const long long S_fin_q = add_sat(q32_host(model_d), data_fin);
-    d2h += sizeof(NodalCtl);
     auto tn1 = std::chrono::steady_clock::now();
     ms_nodal += std::chrono::duration<double, std::milli>(tn1 - tm1).count();
     if (trace_on(3)) emit_trace(3, stage, 0, 0, B, part, dense, S_fin_q, 0, 0, 0, 0);

@@ -1439,6 +1439,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   const int64_t cells = static_cast<int64_t>(B) * B;
   unsigned target = 0;
   unsigned long long my_bytes = 0;
+  bool converged = false;
   for (int sw = 0; sw < p.maxitr; sw++) {
     // data term of S for this sweep (the entropy kernel's sum)
     {
@@ -1524,11 +1525,27 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       }
       tables_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
       const int st = grid_barrier(ctl, &target, done, &s_state);
-      if (st != 0) {   // converged (or a barrier failed)
-        if (p.a.stats && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
-        return;
+      if (st < 0) return;   // a barrier failed
+      if (st > 0) {         // converged
+        converged = true;
+        break;
       }
     }
+    if (converged) break;
+  }
+  // the data term of the final state (the stage's description length),
+  // read by the host with the control block; entropy_acc was cleared at
+  // the last sweep start
+  {
+    long long acc = 0;
+    for (int64_t c = static_cast<int64_t>(blockIdx.x) * kPThreads + threadIdx.x; c < cells;
+         c += static_cast<int64_t>(gridDim.x) * kPThreads) {
+      const int i = static_cast<int>(c / B), j = static_cast<int>(c - static_cast<int64_t>(i) * B);
+      const int m = __ldcg(p.v.M + static_cast<int64_t>(i) * p.v.ld + j);
+      if (m) acc += q32(g_term(p.a.L, m, __ldcg(p.din + j), __ldcg(p.dout + i)));
+    }
+    acc = warp_sum_ll(acc);
+    if (lane == 0 && acc) atomicAdd(&ctl->entropy_acc, static_cast<unsigned long long>(acc));
   }
   if (p.a.stats && my_bytes) atomicAdd(&ctl->bytes, my_bytes);
 }
@@ -1613,6 +1630,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
   __shared__ CtaTally s_tally[kGangMax];
   __shared__ HubShared<kPWarps> sh;
   __shared__ int s_bi[kGangMax], s_sw[kGangMax], s_act[kGangMax], s_nb[kGangMax];
+  __shared__ int s_fin[kGangMax];   // finished in the last round: its final data term is due
   __shared__ long long s_hp[kGangMax + 1], s_up[kGangMax + 1], s_cp[kGangMax + 1], s_tmp[kGangMax];
   __shared__ int s_base, s_state;
   using Ops = DenseOpsT<LdCG, P>;
@@ -1636,6 +1654,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
     s_sw[threadIdx.x] = gb > 0 ? started - 1 : started;
     s_act[threadIdx.x] = !done && s_sw[threadIdx.x] < p.maxitr ? 1 : 0;
     s_nb[threadIdx.x] = (p.n + p.bs - 1) / p.bs;
+    s_fin[threadIdx.x] = 0;
   }
   __syncthreads();
 
@@ -1643,15 +1662,16 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
     __syncthreads();
     const bool mine = threadIdx.x < K && s_act[threadIdx.x];
     const int count = __syncthreads_count(mine);
-    const int start = __syncthreads_or(mine && s_bi[threadIdx.x] == 0);
-    const int flag = (count > 0 ? 1 : 0) | (start ? 2 : 0) | (count << 2);
-    if (!(flag & 1)) break;
-    if ((flag >> 2) < exit_below) break;   // enough jobs are done: the rest resume in the next launch
-    if (flag & 2) {
-      // data term of S for the jobs that start a sweep
+    const int fin = __syncthreads_or(threadIdx.x < K && s_fin[threadIdx.x]);
+    // no job left, or enough are done: the rest resume in the next launch
+    const bool leaving = count == 0 || count < exit_below;
+    const int start = leaving ? 0 : __syncthreads_or(mine && s_bi[threadIdx.x] == 0);
+    if (start || fin) {
+      // data term of S: at the sweep start of the jobs that begin one, and
+      // of the final state of those that finished (read by the host)
       {
         long long cells = 0;
-        if (mine && s_bi[threadIdx.x] == 0) {
+        if ((start && mine && s_bi[threadIdx.x] == 0) || (threadIdx.x < K && s_fin[threadIdx.x])) {
           const long long B = jobs[threadIdx.x].a.B;
           cells = B * B;
         }
@@ -1676,14 +1696,19 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
         if (m) acc += q32(g_term(p.a.L, m, __ldcg(p.din + jj), __ldcg(p.dout + i)));
       }
       if (cj >= 0 && acc) atomicAdd(&jobs[cj].a.ctl->entropy_acc, static_cast<unsigned long long>(acc));
-      if (grid_barrier(gc, &target, false, &s_state) < 0) return;
-      if (blockIdx.x == 0 && threadIdx.x < K && s_act[threadIdx.x] && s_bi[threadIdx.x] == 0) {
-        const PhaseArgs& p = jobs[threadIdx.x];
-        ctl_sweep_start(p.a.ctl, p.W, p.ide_q, p.ide_n);
-        p.a.ctl->entropy_acc = 0;
+      __syncthreads();
+      if (threadIdx.x < K) s_fin[threadIdx.x] = 0;
+      if (start) {
+        if (grid_barrier(gc, &target, false, &s_state) < 0) return;
+        if (blockIdx.x == 0 && threadIdx.x < K && s_act[threadIdx.x] && s_bi[threadIdx.x] == 0) {
+          const PhaseArgs& p = jobs[threadIdx.x];
+          ctl_sweep_start(p.a.ctl, p.W, p.ide_q, p.ide_n);
+          p.a.ctl->entropy_acc = 0;
+        }
+        if (grid_barrier(gc, &target, false, &s_state) < 0) return;
       }
-      if (grid_barrier(gc, &target, false, &s_state) < 0) return;
     }
+    if (leaving) break;
     // proposals of every unfinished job's current batch
     if (threadIdx.x < K) s_tally[threadIdx.x] = CtaTally{0, 0, 0, 0};
     {
@@ -1774,7 +1799,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
         s_bi[j] = 0;
         s_sw[j]++;
       }
-      if (done || s_sw[j] >= p.maxitr) s_act[j] = 0;
+      if (done || s_sw[j] >= p.maxitr) {
+        s_act[j] = 0;
+        s_fin[j] = 1;
+      }
     }
   }
   // where each job stands: finished, or the batch to resume at

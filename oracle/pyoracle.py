@@ -1,8 +1,8 @@
 """ctypes wrapper of the C oracle (oracle/usap_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and
-the CPU-baseline leg of ``bench.py`` as the checker.  The product path never
-loads it.
+the CPU-baseline leg of ``bench.py``, as the reference the CUDA path is
+compared against.  The product path never loads it.
 """
 from __future__ import annotations
 

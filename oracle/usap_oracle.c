@@ -1,5 +1,5 @@
 /* Oracle: plain-C restatement of uSAP's SBP path (see usap_oracle.h).
- * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path, never shipped.
+ * TEST INFRASTRUCTURE ONLY: what the CUDA path is compared against, never shipped.
  * Every function cites the reference lines it restates
  * (include/graph_parallel.hpp unless noted).  Compile with
  * -ffp-contract=off: terms must round exactly as written.

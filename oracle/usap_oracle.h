@@ -1,8 +1,8 @@
 /* Oracle: a plain-C, single-threaded restatement of uSAP's stochastic block
  * partitioning path (include/graph_parallel.hpp of chih-chun-chang/uSAP).
  *
- * TEST INFRASTRUCTURE ONLY.  It is the checker that the CUDA path is
- * compared against; it is never part of the product path.  Only tests/,
+ * TEST INFRASTRUCTURE ONLY.  It is what the CUDA path is compared
+ * against; it is never part of the product path.  Only tests/,
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it.
  *
  * It follows the reference's control flow and arithmetic rules, with the

@@ -122,6 +122,9 @@ typedef struct usap_result {
   double fp32_flip_rate;     /* fp32_nodal_flips / fp32_nodal_evals */
   double fp32_err_max;       /* largest |dS_fp32 - dS_fp64| over nodal and merge evaluations */
   double fp32_err_mean;      /* mean |dS_fp32 - dS_fp64| over nodal evaluations */
+  int64_t apply_scans;       /* nodal batches of the cooperative kernel whose moves were applied by
+                                scanning all of the batch's edges (a CTA accepted more moves than its
+                                shared-memory list holds) instead of each CTA's own list */
 } usap_result;
 
 typedef struct usap_scores {

@@ -261,6 +261,32 @@ def test_persistent_cta_cap_same_result(api):
     ctx.close()
 
 
+def test_persistent_move_list_overflow(api, oracle):
+    """Each CTA of the cooperative kernel applies the moves it accepted from
+    a list in shared memory; when one CTA's list overflows, every CTA scans
+    all of the batch's edges instead.  One CTA and whole-graph batches make
+    the early sweeps overflow and the late ones fit: the solve must equal
+    the per-batch launches (which never list) and the oracle."""
+    from usap_b200 import native as nat
+    G = gen.generate(gen.config_c1(within=0.8, alpha=10.0, seed=0))
+    params = {"num_batch_nodal_update": 1, "seed": 3}
+    ctx = api.Context(0)
+    ctx.load(G.src, G.dst, None, G.n)
+    part_b, res_b = ctx.partition(nat.default_params(persistent=0, **params))
+    scans = {}
+    for ctas in (1, 4, 0):
+        part, res = ctx.partition(nat.default_params(persistent_ctas=ctas, **params))
+        assert np.array_equal(part, part_b) and res["S_q"] == res_b["S_q"], ctas
+        assert res["batches"] == res_b["batches"], ctas
+        scans[ctas] = res["apply_scans"]
+    ctx.close()
+    assert 0 < scans[1] < res_b["batches"], scans
+    assert scans[0] == 0, scans
+    og = oracle.OracleGraph(G.n, G.src, G.dst)
+    part_o, res_o, _ = og.partition(params)
+    assert np.array_equal(part_b, part_o) and res_b["S_q"] == res_o["S_q"]
+
+
 @pytest.mark.parametrize("within,alpha,seed", [(0.8, 10.0, 0), (0.5, 1.0, 1), (0.8, 1.0, 2),
                                                (0.5, 10.0, 3)])
 def test_c1_solve_exact(api, oracle, within, alpha, seed):

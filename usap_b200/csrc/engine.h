@@ -165,11 +165,12 @@ struct NodalCtl {
   unsigned int apply_done;         // CTAs of the apply kernel that have finished
   // persistent kernel: grid barrier (arrivals, generation, timeout flag)
   // and the counter that hands out a batch's vertices
-  unsigned long long bar;   // arrivals (low 32 bits) + convergence flag (bit 32)
+  unsigned long long bar;   // arrivals (low 32 bits), convergence (bits 32-47) and move-list overflow (bits 48-63) arrivals
   int bar_err;
   unsigned int vnext;
   int gang_batch;           // gang launches: next batch of the current sweep (0: a new sweep starts)
   F32Tally f32;             // precision mode 1: FP32 decisions against the FP64 values
+  unsigned long long apply_scans;   // persistent kernel: batches applied by scanning all chunks (a CTA's move list overflowed)
 };
 
 struct GraphDev {

@@ -1047,6 +1047,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
     res->nodal_proposals += static_cast<int64_t>(h_ctl_->proposals);
     res->nodal_moves += static_cast<int64_t>(h_ctl_->moves);
     res->near_threshold += static_cast<int64_t>(h_ctl_->near);
+    res->apply_scans += static_cast<int64_t>(h_ctl_->apply_scans);
     if (prec_) {
       const F32Tally& t = h_ctl_->f32;
       nodal32.evals += t.evals;

@@ -488,6 +488,11 @@ struct CtaTally {
   unsigned long long cum, moves, near;
   int ninf;
   F32Tally f32;
+  // persistent kernel: the edge chunks {v, chunk} of the CTA's accepted
+  // moves, so that its apply pass visits only those (null elsewhere); nown
+  // counts past own_cap when the list overflows
+  int2* own;
+  int nown, own_cap;
 };
 
 template <int P>
@@ -675,7 +680,14 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
   const long long acc = finalize_grp<G, Ops::kP>(a, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out,
                                                  ds_in, vi.kout, vi.kin, &ninf, ts.f, &f);
   if (g.gl == 0) {
-    tally<Ops::kP>(tl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
+    const bool moved = emit<Ops::kP>(a, v, r, s, acc, f, ninf);
+    tally<Ops::kP>(tl, moved, acc, f, ninf);
+    if (moved && tl->own) {
+      const int nch = deg > 32 ? (deg + 31) >> 5 : 1;   // the vertex's chunks (one even without edges)
+      const int i0 = atomicAdd(&tl->nown, nch);
+      for (int c = 0; c < nch; c++)
+        if (i0 + c < tl->own_cap) tl->own[i0 + c] = make_int2(v, c);
+    }
     if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * noccupied + 48 + 8ull * scanned;
   }
   g.sync();
@@ -1123,16 +1135,29 @@ struct LdPlain {
   __device__ __forceinline__ static T ld(const T* p) { return *p; }
 };
 
-// Shared-memory accumulation of one CTA's tile deltas during an apply pass.
-// `mkey/mval` hold M[a][b] += d under the key a * ld + b; at the flush each
-// entry updates M and Mt and feeds the chunk sums of rows a and b, which are
-// accumulated in `ckey/cval` (key row * cld + chunk) and flushed last.  All
-// sums are exact integers, so the order of the updates does not matter.  A
-// table that is full passes the update straight to global memory.
+// Accumulation of one CTA's tile deltas during an apply pass, in one of
+// three modes.  All sums are exact integers, so the order of the updates
+// does not matter.
+//  kDeltaHashed: open-addressed tables in shared memory; `mkey/mval` hold
+//    M[a][b] += d under the key a * ld + b; at the flush each entry updates
+//    M and Mt and feeds the chunk sums of rows a and b, which are
+//    accumulated in `ckey/cval` (key row * cld + chunk) and flushed last.  A
+//    table that is full passes the update straight to global memory.
+//  kDeltaDense (B * B <= the table region): a dense B x B array of deltas in
+//    `mkey` (row stride dB = B) and the chunk-sum deltas in `ckey` (row *
+//    cld + chunk); no probing, and a flush that scans B * B cells.  For
+//    small B, where every CTA's updates fall on a few hundred cells and
+//    global atomics would queue on them.
+//  kDeltaGlobal: every update straight to M, Mt and the chunk sums; for
+//    large B the updates spread over many cells and the per-CTA tables cost
+//    more (clear, probes, flush) than they save.
+constexpr int kDeltaHashed = 0, kDeltaGlobal = 1, kDeltaDense = 2;
 struct DeltaTables {
   int *mkey, *mval, *ckey, *cval;
   int mlg, clg;   // capacities 1 << mlg, 1 << clg
   int tag = 0;    // job number << 24 when the tables serve several jobs
+  int mode = kDeltaHashed;
+  int dB = 0;     // kDeltaDense: B
 };
 
 // Adds d under key k; false when no slot was found within kProbeMax probes
@@ -1161,6 +1186,19 @@ __device__ __forceinline__ void cs_add(const DeltaTables& t, int* CS, int key, i
 
 __device__ __forceinline__ void tile_add(const DeltaTables& t, int* M, int* Mt, int* CS, int ld, int cld, int x,
                                          int y, int d) {
+  if (t.mode == kDeltaDense) {
+    atomicAdd(t.mkey + x * t.dB + y, d);
+    atomicAdd(t.ckey + x * cld + y / kChunk, d);
+    atomicAdd(t.ckey + y * cld + x / kChunk, d);
+    return;
+  }
+  if (t.mode == kDeltaGlobal) {
+    atomicAdd(M + static_cast<long long>(x) * ld + y, d);
+    atomicAdd(Mt + static_cast<long long>(y) * ld + x, d);
+    atomicAdd(CS + x * cld + y / kChunk, d);
+    atomicAdd(CS + y * cld + x / kChunk, d);
+    return;
+  }
   if (table_add(t.mkey, t.mval, t.mlg, t.tag | (x * ld + y), d)) return;
   atomicAdd(M + static_cast<long long>(x) * ld + y, d);
   atomicAdd(Mt + static_cast<long long>(y) * ld + x, d);
@@ -1206,6 +1244,35 @@ __device__ __forceinline__ void tables_flush(const DeltaTables& t, int* M, int* 
     if (d) atomicAdd(CS + k, d);
   }
   __syncthreads();
+}
+
+// kDeltaDense: zero the B x B deltas and the B * cld chunk-sum deltas
+__device__ __forceinline__ void dense_clear(const DeltaTables& t, int cld) {
+  const int nm = t.dB * t.dB, nc = t.dB * cld;
+  for (int i = threadIdx.x; i < nm; i += blockDim.x) t.mkey[i] = 0;
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) t.ckey[i] = 0;
+}
+
+// kDeltaDense: writes the non-zero deltas to M, Mt and the chunk sums (whose
+// layout row * cld + chunk the dense array shares) and zeroes them
+// (CTA-collective)
+__device__ __forceinline__ void dense_flush(const DeltaTables& t, int* M, int* Mt, int* CS, int ld, int cld) {
+  __syncthreads();
+  const int B = t.dB, nm = B * B, nc = B * cld;
+  for (int i = threadIdx.x; i < nm; i += blockDim.x) {
+    const int d = t.mkey[i];
+    if (d == 0) continue;
+    t.mkey[i] = 0;
+    const int x = i / B, y = i - x * B;
+    atomicAdd(M + static_cast<long long>(x) * ld + y, d);
+    atomicAdd(Mt + static_cast<long long>(y) * ld + x, d);
+  }
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+    const int d = t.ckey[i];
+    if (d == 0) continue;
+    t.ckey[i] = 0;
+    atomicAdd(CS + i, d);
+  }
 }
 
 // Applies and commits the moves of one 32-edge chunk of a batch vertex
@@ -1326,6 +1393,7 @@ constexpr int kPWarps = kPThreads / 32;
 constexpr int kUnitWarp = -2;     // work unit of one vertex with 64 < degree <= 128
 constexpr int kPHubLg = 13;
 constexpr int kPHubSlots = 1 << kPHubLg;  // hub table slots in shared memory; larger hub tables are global
+constexpr int kDeltaGlobalMinB = 256;     // from this B the phase kernel's apply writes straight to global memory
 static_assert(kPHubSlots == kPhaseHubSlots, "hub regions are assigned for tables beyond this size");
 constexpr unsigned long long kBarrierTimeoutNs = 200ull * 1000ull * 1000ull;
 // dynamic shared memory: per-warp tables and lists, then the hub table
@@ -1348,30 +1416,34 @@ __device__ __forceinline__ void red_release_add64(unsigned long long* p, unsigne
   asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-constexpr unsigned long long kBarDone = 1ull << 32;
+constexpr unsigned long long kBarDone = 1ull << 32;   // bits 32..47: done arrivals
+constexpr unsigned long long kBarOvf = 1ull << 48;    // bits 48..63: overflow arrivals (mod 2^16)
 
 // Grid-wide barrier of the persistent kernel (all CTAs are co-resident:
 // cooperative launch).  ctl->bar counts arrivals over the whole launch in
 // its low 32 bits; barrier number k is passed once it reaches
 // k * gridDim.x (`target`, advanced here).  After __syncthreads, thread 0
 // adds its arrival with release semantics (publishing the CTA's writes)
-// and waits with acquire loads.  The arrival may also carry kBarDone, which
-// every CTA then sees in the same load.  A wait gives up after
-// kBarrierTimeoutNs and sets bar_err.  Returns -1 on error (every CTA then
-// leaves at its next barrier), else 1 if kBarDone is set, else 0.
+// and waits with acquire loads.  The arrival may also carry kBarDone or
+// kBarOvf, which every CTA then sees in the same load; *s_ovf (if given)
+// receives the overflow count.  A wait gives up after kBarrierTimeoutNs and
+// sets bar_err.  Returns -1 on error (every CTA then leaves at its next
+// barrier), else 1 if kBarDone is set, else 0.
 template <class CtlT>
-__device__ __forceinline__ int grid_barrier(CtlT* ctl, unsigned* target, bool publish_done, int* s_state) {
+__device__ __forceinline__ int grid_barrier(CtlT* ctl, unsigned* target, bool publish_done, int* s_state,
+                                            bool publish_ovf = false, unsigned* s_ovf = nullptr) {
   *target += gridDim.x;
   __syncthreads();
   if (threadIdx.x == 0) {
-    red_release_add64(&ctl->bar, publish_done ? 1ull + kBarDone : 1ull);
+    red_release_add64(&ctl->bar, (publish_done ? 1ull + kBarDone : 1ull) + (publish_ovf ? kBarOvf : 0ull));
     const unsigned long long t0 = global_ns();
     unsigned spins = 0;
     int st;
     for (;;) {
       const unsigned long long v = ld_acquire64(&ctl->bar);
       if (static_cast<unsigned>(v) >= *target) {
-        st = (v & ~0xffffffffull) ? 1 : 0;
+        st = ((v >> 32) & 0xffffull) ? 1 : 0;
+        if (s_ovf) *s_ovf = static_cast<unsigned>(v >> 48);
         break;
       }
       if ((++spins & 63u) == 0) {
@@ -1396,9 +1468,25 @@ __device__ __forceinline__ int grid_barrier(CtlT* ctl, unsigned* target, bool pu
 // each an entropy pass, the sweep-start bookkeeping, and for every batch a
 // proposal pass (hubs first, one per CTA; then warp-per-vertex, first one
 // vertex per warp of the CTAs without a hub, the rest handed out by a
-// counter) and an apply pass over the batch's edge chunks, during which
-// one thread runs the batch-end bookkeeping.  Leaves when the convergence
+// counter) and an apply pass, during which one thread runs the batch-end
+// bookkeeping.  Each CTA applies the moves it accepted itself: the chunks
+// of its moved work-unit vertices (listed in shared memory during the
+// proposals) and of its moved hubs.  If any CTA's list overflowed (it
+// announces that with its barrier arrival, so every CTA learns it from the
+// same barrier load), every CTA instead scans all of the batch's edge
+// chunks, skipping vertices that did not move.  Tile deltas accumulate per
+// CTA as DeltaTables' mode for this B says.  Leaves when the convergence
 // test sets `done`.
+constexpr int kOwnCap = 1024;   // chunk entries of a CTA's own-move list
+
+// algorithmic bytes of an applied chunk: per edge of a moved vertex its
+// neighbour's id and block (8) and the two updated entries of M (16)
+__device__ __forceinline__ unsigned long long apply_bytes(const NodalArgs& a, int2 ch) {
+  if (__ldcg(a.move_to + ch.x) < 0) return 0;
+  const int deg = (__ldg(a.out_ptr + ch.x + 1) - __ldg(a.out_ptr + ch.x)) +
+                  (__ldg(a.in_ptr + ch.x + 1) - __ldg(a.in_ptr + ch.x));
+  return 24ull * static_cast<unsigned long long>(max(0, min(32, deg - 32 * ch.y)));
+}
 // One work unit of the persistent kernels: two vertices of degree <= 64
 // (a half-warp each; un.y = -1 when there is only one) or one vertex of
 // degree <= 128 (the whole warp, un.y = kUnitWarp).  wtab: the warp's
@@ -1425,6 +1513,8 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   __shared__ CtaTally s_tally;
   __shared__ HubShared<kPWarps> sh;
   __shared__ int s_base, s_state;
+  __shared__ unsigned s_ovf;
+  __shared__ int2 s_own[kOwnCap];
   using Ops = DenseOpsT<LdCG, P>;
   const Ops ops{p.v, p.a.B};
   NodalCtl* ctl = p.a.ctl;
@@ -1433,9 +1523,13 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   const int nw = gridDim.x * kPWarps;
   int* wtab = dyn + wib * kPWarpInts;
   int* htab = dyn + kPWarps * kPWarpInts;   // hub table during proposals, delta tables during apply
+  // dense deltas in the first 2 * kPHubSlots ints, chunk-sum deltas (B <= 128: B entries) after them
+  const int mode = p.a.B >= kDeltaGlobalMinB ? kDeltaGlobal
+                   : (p.a.B * p.a.B <= 2 * kPHubSlots ? kDeltaDense : kDeltaHashed);
   const DeltaTables dt{htab, htab + kPHubSlots, htab + 2 * kPHubSlots, htab + 2 * kPHubSlots + kPHubSlots / 2,
-                       kPHubLg, kPHubLg - 1};
+                       kPHubLg, kPHubLg - 1, 0, mode, p.a.B};
   const int B = p.a.B;
+  unsigned ovf_seen = 0;   // overflow count at the previous proposal barrier
   const int64_t cells = static_cast<int64_t>(B) * B;
   unsigned target = 0;
   unsigned long long my_bytes = 0;
@@ -1473,7 +1567,11 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       a.end = a.beg + p.bs < p.n ? a.beg + p.bs : p.n;
       const int count = a.end - a.beg;
       // proposals
-      if (threadIdx.x == 0) s_tally = CtaTally{0, 0, 0, 0};
+      if (threadIdx.x == 0) {
+        s_tally = CtaTally{0, 0, 0, 0};
+        s_tally.own = s_own;
+        s_tally.own_cap = kOwnCap;
+      }
       __syncthreads();
       const int hub_lo = __ldg(p.batch_hub + bi), hub_hi = __ldg(p.batch_hub + bi + 1);
       const int hcta = min(hub_hi - hub_lo, static_cast<int>(gridDim.x));
@@ -1498,7 +1596,15 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       }
       __syncthreads();
       if (threadIdx.x == 0) tally_flush(&s_tally, ctl);
-      if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+      const int nown = s_tally.nown;
+      if (grid_barrier(ctl, &target, false, &s_state, nown > kOwnCap, &s_ovf) < 0) return;
+      // every CTA reads the same count here: the next overflow arrivals come
+      // after the next proposal pass, which no CTA starts before all passed
+      // the apply barrier below
+      const bool scan_all = s_ovf != ovf_seen;
+      ovf_seen = s_ovf;
+      if (dt.mode == kDeltaDense) dense_clear(dt, p.v.cld);
+      else if (dt.mode == kDeltaHashed) tables_clear(dt);
       // apply + commit; one thread closes the batch meanwhile
       bool done = false;
       if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1507,23 +1613,35 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
         const CtlArgs ca{1, p.W, p.thr, p.model_d, p.ide_q, p.ide_n, count, edges};
         done = ctl_batch_end(ctl, ca);
         ctl->vnext = 0;
+        if (scan_all) ctl->apply_scans++;
       }
-      tables_clear(dt);
       __syncthreads();
-      const int64_t c0 = __ldg(p.chunk_ptr + a.beg), c1 = __ldg(p.chunk_ptr + a.end);
-      for (int64_t q = c0 + gw; q < c1; q += nw) {
-        const int2 ch = __ldg(p.g.chunks + q);
-        apply_chunk<LdCG, LdCG>(ch, p.g, p.part, a.move_to, a.from, a.beg, a.end, dt, p.v.ld, p.M, p.Mt,
-                                p.v.cld, p.CS, p.dout, p.din, lane);
-        // algorithmic bytes of a moved vertex's edge: its neighbour's id and
-        // block (8) and the two updated entries of M (16)
-        if (p.a.stats && lane == 0 && __ldcg(a.move_to + ch.x) >= 0) {
-          const int deg = (__ldg(p.a.out_ptr + ch.x + 1) - __ldg(p.a.out_ptr + ch.x)) +
-                          (__ldg(p.a.in_ptr + ch.x + 1) - __ldg(p.a.in_ptr + ch.x));
-          my_bytes += 24ull * static_cast<unsigned long long>(max(0, min(32, deg - 32 * ch.y)));
+      {
+        // own moves (chunk k of the CTA's list), or every chunk of the batch
+        const int64_t cb = scan_all ? __ldg(p.chunk_ptr + a.beg) : 0;
+        const int64_t k1 = scan_all ? __ldg(p.chunk_ptr + a.end) : nown;
+        const int step = scan_all ? nw : kPWarps;
+        for (int64_t k = (scan_all ? cb + gw : wib); k < k1; k += step) {
+          const int2 ch = scan_all ? __ldg(p.g.chunks + k) : s_own[k];
+          apply_chunk<LdCG, LdCG>(ch, p.g, p.part, a.move_to, a.from, a.beg, a.end, dt, p.v.ld, p.M, p.Mt,
+                                  p.v.cld, p.CS, p.dout, p.din, lane);
+          if (p.a.stats && lane == 0) my_bytes += apply_bytes(p.a, ch);
         }
       }
-      tables_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
+      // the CTA's moved hubs, whose chunks are not listed
+      for (int h = hub_lo + blockIdx.x; !scan_all && h < hub_hi; h += gridDim.x) {
+        const int v = __ldg(p.hubs + h);
+        if (__ldcg(a.move_to + v) < 0) continue;   // CTA-uniform
+        const int64_t q1 = __ldg(p.chunk_ptr + v + 1);
+        for (int64_t q = __ldg(p.chunk_ptr + v) + wib; q < q1; q += kPWarps) {
+          const int2 ch = __ldg(p.g.chunks + q);
+          apply_chunk<LdCG, LdCG>(ch, p.g, p.part, a.move_to, a.from, a.beg, a.end, dt, p.v.ld, p.M, p.Mt,
+                                  p.v.cld, p.CS, p.dout, p.din, lane);
+          if (p.a.stats && lane == 0) my_bytes += apply_bytes(p.a, ch);
+        }
+      }
+      if (dt.mode == kDeltaDense) dense_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
+      else if (dt.mode == kDeltaHashed) tables_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
       const int st = grid_barrier(ctl, &target, done, &s_state);
       if (st < 0) return;   // a barrier failed
       if (st > 0) {         // converged

@@ -111,14 +111,18 @@ struct Grp {
 
 // P (precision mode 1 or 2): dS is also evaluated in FP32 and decisions
 // are taken on that value; the exact FP64 value is kept beside it.
-template <class LD, int P = 0>
+// Ld loads the partition, LdT the tile state (M, Mt, chunk sums, block
+// degrees): the persistent kernel may read the latter from a per-batch
+// copy in shared memory.
+template <class LD, int P = 0, class LDT = LD>
 struct DenseOpsT {
   using Ld = LD;
+  using LdT = LDT;
   static constexpr int kP = P;
   DenseView v;
   int B;
   __device__ __forceinline__ int get(int x, int y) const {
-    return LD::ld(v.M + static_cast<long long>(x) * v.ld + y);
+    return LDT::ld(v.M + static_cast<long long>(x) * v.ld + y);
   }
   // first block i (block-id order) whose cumulative M[u,i]+M[i,u] exceeds t:
   // a group scan over the row's chunk sums, then over the 128 entries of the
@@ -133,7 +137,7 @@ struct DenseOpsT {
     int c = nch - 1;
     for (int base = 0; base < nch; base += G) {
       const int cc = base + g.gl;
-      const int val = cc < nch ? LD::ld(cs + cc) : 0;
+      const int val = cc < nch ? LDT::ld(cs + cc) : 0;
       const int incl = g.incl_scan(val);
       const int total = g.shfl(incl, G - 1);
       if (run + total > t) {
@@ -156,8 +160,8 @@ struct DenseOpsT {
       const int i = i0 + 4 * q;
       const int prev = q ? pr[4 * q - 1] : 0;
       if (i < B) {
-        const int4 a = LD::ld(reinterpret_cast<const int4*>(mrow + i));
-        const int4 b = LD::ld(reinterpret_cast<const int4*>(trow + i));
+        const int4 a = LDT::ld(reinterpret_cast<const int4*>(mrow + i));
+        const int4 b = LDT::ld(reinterpret_cast<const int4*>(trow + i));
         pr[4 * q] = prev + a.x + b.x;
         pr[4 * q + 1] = pr[4 * q] + a.y + b.y;
         pr[4 * q + 2] = pr[4 * q + 1] + a.z + b.z;
@@ -184,6 +188,7 @@ struct DenseOpsT {
 template <int P = 0>
 struct SortedOpsT {
   using Ld = LdNC;
+  using LdT = LdNC;
   static constexpr int kP = P;
   SortedView v;
   int B;
@@ -256,7 +261,7 @@ __device__ __forceinline__ VertexInfo vertex_info(const NodalArgs& a, int v) {
 template <class Ops, int G>
 __device__ __forceinline__ int target_from(const NodalArgs& a, const Ops& ops, const Draws& x, int u,
                                            const Grp<G>& g, int* scanned) {
-  const long long dau = static_cast<long long>(Ops::Ld::ld(a.dout + u)) + Ops::Ld::ld(a.din + u);
+  const long long dau = static_cast<long long>(Ops::LdT::ld(a.dout + u)) + Ops::LdT::ld(a.din + u);
   if (accept_uniform(x.x1, dau, a.B)) return static_cast<int>(draw_below(x.x2, a.B));
   return ops.template sym_sample<G>(u, draw_below(x.x2, dau), g, scanned);
 }
@@ -368,13 +373,13 @@ __device__ __forceinline__ void slot_terms(const NodalArgs& a, const Ops& ops, i
                                            int wi, const DegLogs& dl, TermSums& ts) {
   if (wo > 0) {
     const int R = ops.get(r, b), S = ops.get(s, b);
-    pair_terms<Ops::kP>(a, R, S, wo, Ops::Ld::ld(a.din + b), dl, false, ts);
+    pair_terms<Ops::kP>(a, R, S, wo, Ops::LdT::ld(a.din + b), dl, false, ts);
     ts.sXR += R;
     ts.sXS += S;
   }
   if (wi > 0) {
     const int R = ops.get(b, r), S = ops.get(b, s);
-    pair_terms<Ops::kP>(a, R, S, wi, Ops::Ld::ld(a.dout + b), dl, true, ts);
+    pair_terms<Ops::kP>(a, R, S, wi, Ops::LdT::ld(a.dout + b), dl, true, ts);
     ts.sYR += R;
     ts.sYS += S;
   }
@@ -541,6 +546,7 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
                                              int* two, int* twi, int* list, CtaTally* tl, const Grp<G>& g,
                                              unsigned long long* my_bytes) {
   using LD = typename Ops::Ld;
+  using LDT = typename Ops::LdT;
   constexpr int KN = 4;   // neighbours per lane
   const unsigned lanes_below = (1u << g.gl) - 1u;
   const VertexInfo vi = vertex_info<Ops>(a, v);
@@ -548,7 +554,7 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
   if (deg > KN * G) return;   // proposed by a larger group or a whole CTA
   const int r = vi.r;
   const Draws x = philox(static_cast<uint32_t>(v), itr, a.stage, kTagNodal, a.seed);
-  const long long dr_out = LD::ld(a.dout + r), dr_in = LD::ld(a.din + r);
+  const long long dr_out = LDT::ld(a.dout + r), dr_in = LDT::ld(a.din + r);
   int lg = 5;
   while ((1 << lg) < 2 * deg) lg++;
   const int cap = 1 << lg;   // <= 8 * G
@@ -618,7 +624,7 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
     g.sync();
     return;
   }
-  const long long ds_out = LD::ld(a.dout + s), ds_in = LD::ld(a.din + s);
+  const long long ds_out = LDT::ld(a.dout + s), ds_in = LDT::ld(a.din + s);
   int e4 = 0;
   if (g.gl < 4) e4 = ops.get(g.gl < 2 ? r : s, (g.gl & 1) ? s : r);
   const DegLogs dl = deg_logs<Ops::kP>(a, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
@@ -653,12 +659,12 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
         if (wo[k] > 0) {
           R[k] = ops.get(r, b);
           S[k] = ops.get(s, b);
-          Di[k] = LD::ld(a.din + b);
+          Di[k] = LDT::ld(a.din + b);
         }
         if (wi[k] > 0) {
           Rc[k] = ops.get(b, r);
           Sc[k] = ops.get(b, s);
-          Do[k] = LD::ld(a.dout + b);
+          Do[k] = LDT::ld(a.dout + b);
         }
       }
     }
@@ -735,6 +741,7 @@ template <class Ops, int NT>
 __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, int v, uint32_t itr, int* stab,
                                            int scap, HubShared<NT / 32>* sh, unsigned long long* my_bytes) {
   using LD = typename Ops::Ld;
+  using LDT = typename Ops::LdT;
   constexpr int NW = NT / 32;
   constexpr int kIns = NT - 32;   // threads that fill the table
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -803,8 +810,8 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
     __syncthreads();
     return;
   }
-  const long long dr_out = LD::ld(a.dout + r), dr_in = LD::ld(a.din + r);
-  const long long ds_out = LD::ld(a.dout + s), ds_in = LD::ld(a.din + s);
+  const long long dr_out = LDT::ld(a.dout + r), dr_in = LDT::ld(a.din + r);
+  const long long ds_out = LDT::ld(a.dout + s), ds_in = LDT::ld(a.din + s);
   const DegLogs dl = deg_logs<Ops::kP>(a, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
   TermSums ts{0, 0, 0, 0, 0};
   int nocc = 0;
@@ -1394,6 +1401,15 @@ constexpr int kUnitWarp = -2;     // work unit of one vertex with 64 < degree <=
 constexpr int kPHubLg = 13;
 constexpr int kPHubSlots = 1 << kPHubLg;  // hub table slots in shared memory; larger hub tables are global
 constexpr int kDeltaGlobalMinB = 256;     // from this B the phase kernel's apply writes straight to global memory
+// the proposals of the phase kernel read the tile from shared memory up to
+// this B: M and Mt (B x ld each, ld = B rounded up to 4) after the first
+// kSnapOff slots of the hub table's first and second arrays, chunk sums and
+// degrees after those of its third
+constexpr int kSnapMaxB = 88;
+constexpr int kSnapOff = 256;   // >= a hub table's capacity for B <= kSnapMaxB (2 * B rounded up to a power of 2)
+static_assert(kSnapOff + kSnapMaxB * ((kSnapMaxB + 3) & ~3) <= kPHubSlots, "tile copy overruns its region");
+static_assert(kSnapOff + 3 * kSnapMaxB <= kPHubSlots, "degree copy overruns its region");
+static_assert(2 * kSnapMaxB <= kSnapOff && kSnapMaxB <= kChunk, "hub tables or chunk sums outgrow the layout");
 static_assert(kPHubSlots == kPhaseHubSlots, "hub regions are assigned for tables beyond this size");
 constexpr unsigned long long kBarrierTimeoutNs = 200ull * 1000ull * 1000ull;
 // dynamic shared memory: per-warp tables and lists, then the hub table
@@ -1507,7 +1523,7 @@ __device__ __forceinline__ void unit_vertices(const NodalArgs& a, const Ops& ops
   }
 }
 
-template <int P>
+template <int P, bool kSnap>
 __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   extern __shared__ int dyn[];
   __shared__ CtaTally s_tally;
@@ -1515,14 +1531,29 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   __shared__ int s_base, s_state;
   __shared__ unsigned s_ovf;
   __shared__ int2 s_own[kOwnCap];
-  using Ops = DenseOpsT<LdCG, P>;
-  const Ops ops{p.v, p.a.B};
+  using Ops = DenseOpsT<LdCG, P, std::conditional_t<kSnap, LdPlain, LdCG>>;
   NodalCtl* ctl = p.a.ctl;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gw = blockIdx.x * kPWarps + wib;
   const int nw = gridDim.x * kPWarps;
   int* wtab = dyn + wib * kPWarpInts;
   int* htab = dyn + kPWarps * kPWarpInts;   // hub table during proposals, delta tables during apply
+  // kSnap (B <= kSnapMaxB): the proposals read M, Mt, the chunk sums and the
+  // block degrees from a copy in shared memory, taken at every batch start;
+  // it shares the hub table's region (a hub's table then needs at most
+  // kSnapOff slots per array)
+  int* sM = htab + kSnapOff;
+  int* sMt = htab + kPHubSlots + kSnapOff;
+  int* sCS = htab + 2 * kPHubSlots + kSnapOff;
+  int* sdin = sCS + kSnapMaxB;
+  int* sdout = sdin + kSnapMaxB;
+  DenseView vs = p.v;
+  if (kSnap) {
+    vs.M = sM;
+    vs.Mt = sMt;
+    vs.CS = sCS;
+  }
+  const Ops ops{vs, p.a.B};
   // dense deltas in the first 2 * kPHubSlots ints, chunk-sum deltas (B <= 128: B entries) after them
   const int mode = p.a.B >= kDeltaGlobalMinB ? kDeltaGlobal
                    : (p.a.B * p.a.B <= 2 * kPHubSlots ? kDeltaDense : kDeltaHashed);
@@ -1566,6 +1597,23 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       a.beg = bi * p.bs;
       a.end = a.beg + p.bs < p.n ? a.beg + p.bs : p.n;
       const int count = a.end - a.beg;
+      if (kSnap) {
+        // the tile as the previous batch left it (rows padded to ld with
+        // zeros; cld = 1)
+        const int n4 = B * p.v.ld / 4;
+        for (int i = threadIdx.x; i < n4; i += kPThreads) {
+          reinterpret_cast<int4*>(sM)[i] = __ldcg(reinterpret_cast<const int4*>(p.v.M) + i);
+          reinterpret_cast<int4*>(sMt)[i] = __ldcg(reinterpret_cast<const int4*>(p.v.Mt) + i);
+        }
+        for (int i = threadIdx.x; i < B; i += kPThreads) {
+          sCS[i] = __ldcg(p.v.CS + i);
+          sdin[i] = __ldcg(p.din + i);
+          sdout[i] = __ldcg(p.dout + i);
+        }
+        a.din = sdin;
+        a.dout = sdout;
+        __syncthreads();
+      }
       // proposals
       if (threadIdx.x == 0) {
         s_tally = CtaTally{0, 0, 0, 0};
@@ -1986,12 +2034,14 @@ void nodal_configure(int device) {
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       USAP_CUDA(cudaFuncSetAttribute(k_nodal_propose_hub<SortedOpsT<P>>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-      USAP_CUDA(cudaFuncSetAttribute(k_nodal_phase<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
+      USAP_CUDA(cudaFuncSetAttribute(k_nodal_phase<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
+      USAP_CUDA(cudaFuncSetAttribute(k_nodal_phase<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
       USAP_CUDA(cudaFuncSetAttribute(k_nodal_gang<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, psmem));
-      int a = 0, b = 0;
-      USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_nodal_phase<P>, kPThreads, kPSmemBytes));
+      int a = 0, a2 = 0, b = 0;
+      USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_nodal_phase<P, false>, kPThreads, kPSmemBytes));
+      USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a2, k_nodal_phase<P, true>, kPThreads, kPSmemBytes));
       USAP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_nodal_gang<P>, kPThreads, kPSmemBytes));
-      per_phase = std::min(per_phase, a);
+      per_phase = std::min(per_phase, std::min(a, a2));
       per_gang = std::min(per_gang, b);
     };
     configure(std::integral_constant<int, 0>{});
@@ -2024,10 +2074,16 @@ static const void* gang_kernel(int prec) {
   return reinterpret_cast<const void*>(k_nodal_gang<0>);
 }
 
-static const void* phase_kernel(int prec) {
-  if (prec == 1) return reinterpret_cast<const void*>(k_nodal_phase<1>);
-  if (prec == 2) return reinterpret_cast<const void*>(k_nodal_phase<2>);
-  return reinterpret_cast<const void*>(k_nodal_phase<0>);
+// snap: the variant that copies the tile into shared memory (B <= kSnapMaxB)
+static const void* phase_kernel(int prec, bool snap) {
+  if (snap) {
+    if (prec == 1) return reinterpret_cast<const void*>(k_nodal_phase<1, true>);
+    if (prec == 2) return reinterpret_cast<const void*>(k_nodal_phase<2, true>);
+    return reinterpret_cast<const void*>(k_nodal_phase<0, true>);
+  }
+  if (prec == 1) return reinterpret_cast<const void*>(k_nodal_phase<1, false>);
+  if (prec == 2) return reinterpret_cast<const void*>(k_nodal_phase<2, false>);
+  return reinterpret_cast<const void*>(k_nodal_phase<0, false>);
 }
 
 void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_below, int grid, int prec,
@@ -2045,7 +2101,7 @@ void launch_nodal_gang(const PhaseArgs* jobs_dev, int K, GangCtl* gc, int exit_b
 void launch_nodal_phase(const PhaseArgs& p, int grid, cudaStream_t st) {
   PhaseArgs args = p;
   void* kargs[] = {&args};
-  const void* fn = phase_kernel(p.a.prec);
+  const void* fn = phase_kernel(p.a.prec, p.a.B <= kSnapMaxB);
   USAP_CUDA(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kPThreads), kargs, kPSmemBytes, st));
   USAP_LAUNCHED();
 }

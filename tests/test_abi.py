@@ -28,6 +28,43 @@ def test_library_exports_every_declared_symbol():
     assert sorted(nat.EXPORTS) == declared
 
 
+_MIRRORS = {"usap_graph": "Graph", "usap_params": "Params", "usap_result": "Result",
+            "usap_scores": "Scores", "usap_trace_event": "TraceEvent", "usap_batch_job": "BatchJob",
+            "usap_batch_stats": "BatchStats", "usap_server_config": "ServerConfig",
+            "usap_server_timing": "ServerTiming", "usap_server_stats": "ServerStats"}
+
+
+def test_struct_layout_matches_header(tmp_path):
+    """The Python mirrors of include/usap.h's structs have the header's
+    size and every field at the header's offset (a C probe compiled with
+    the host compiler prints them)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no host C compiler")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "usap.h"', "int main(void) {"]
+    for cname, pname in _MIRRORS.items():
+        lines.append(f'  printf("{cname} . %zu\\n", sizeof({cname}));')
+        for f, _ in getattr(nat, pname)._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    seen = 0
+    for line in filter(None, out):
+        cname, field, value = line.split()
+        st = getattr(nat, _MIRRORS[cname])
+        got = C.sizeof(st) if field == "." else getattr(st, field).offset
+        assert got == int(value), (cname, field, got, int(value))
+        seen += 1
+    assert seen == sum(1 + len(getattr(nat, p)._fields_) for p in _MIRRORS.values())
+
+
 def test_version_and_defaults():
     L = nat.lib()
     assert b"sm_100a" in L.usap_version()

@@ -493,11 +493,13 @@ struct CtaTally {
   unsigned long long cum, moves, near;
   int ninf;
   F32Tally f32;
-  // persistent kernel: the edge chunks {v, chunk} of the CTA's accepted
-  // moves, so that its apply pass visits only those (null elsewhere); nown
-  // counts past own_cap when the list overflows
+  // persistent kernels: the edge chunks {v, own_tag | chunk} of the CTA's
+  // accepted moves, so that its apply pass visits only those (null
+  // elsewhere); *nown, shared by the CTA's tallies, counts past own_cap when
+  // the list overflows; own_tag is the job index << 16 in the gang kernel
   int2* own;
-  int nown, own_cap;
+  int* nown;
+  int own_cap, own_tag;
 };
 
 template <int P>
@@ -690,9 +692,9 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
     tally<Ops::kP>(tl, moved, acc, f, ninf);
     if (moved && tl->own) {
       const int nch = deg > 32 ? (deg + 31) >> 5 : 1;   // the vertex's chunks (one even without edges)
-      const int i0 = atomicAdd(&tl->nown, nch);
+      const int i0 = atomicAdd(tl->nown, nch);
       for (int c = 0; c < nch; c++)
-        if (i0 + c < tl->own_cap) tl->own[i0 + c] = make_int2(v, c);
+        if (i0 + c < tl->own_cap) tl->own[i0 + c] = make_int2(v, tl->own_tag | c);
     }
     if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * noccupied + 48 + 8ull * scanned;
   }
@@ -1531,6 +1533,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   __shared__ int s_base, s_state;
   __shared__ unsigned s_ovf;
   __shared__ int2 s_own[kOwnCap];
+  __shared__ int s_nown;
   using Ops = DenseOpsT<LdCG, P, std::conditional_t<kSnap, LdPlain, LdCG>>;
   NodalCtl* ctl = p.a.ctl;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1618,7 +1621,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       if (threadIdx.x == 0) {
         s_tally = CtaTally{0, 0, 0, 0};
         s_tally.own = s_own;
+        s_tally.nown = &s_nown;
         s_tally.own_cap = kOwnCap;
+        s_nown = 0;
       }
       __syncthreads();
       const int hub_lo = __ldg(p.batch_hub + bi), hub_hi = __ldg(p.batch_hub + bi + 1);
@@ -1644,7 +1649,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       }
       __syncthreads();
       if (threadIdx.x == 0) tally_flush(&s_tally, ctl);
-      const int nown = s_tally.nown;
+      const int nown = s_nown;
       if (grid_barrier(ctl, &target, false, &s_state, nown > kOwnCap, &s_ovf) < 0) return;
       // every CTA reads the same count here: the next overflow arrivals come
       // after the next proposal pass, which no CTA starts before all passed
@@ -1799,6 +1804,10 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
   __shared__ int s_fin[kGangMax];   // finished in the last round: its final data term is due
   __shared__ long long s_hp[kGangMax + 1], s_up[kGangMax + 1], s_cp[kGangMax + 1], s_tmp[kGangMax];
   __shared__ int s_base, s_state;
+  __shared__ unsigned s_ovf;
+  __shared__ int2 s_own[kOwnCap];   // {v, job << 16 | chunk} of the CTA's accepted work-unit moves
+  __shared__ int s_nown;
+  unsigned ovf_seen = 0;
   using Ops = DenseOpsT<LdCG, P>;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int gw = blockIdx.x * kPWarps + wib;
@@ -1876,7 +1885,14 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
     }
     if (leaving) break;
     // proposals of every unfinished job's current batch
-    if (threadIdx.x < K) s_tally[threadIdx.x] = CtaTally{0, 0, 0, 0};
+    if (threadIdx.x < K) {
+      s_tally[threadIdx.x] = CtaTally{0, 0, 0, 0};
+      s_tally[threadIdx.x].own = s_own;
+      s_tally[threadIdx.x].nown = &s_nown;
+      s_tally[threadIdx.x].own_cap = kOwnCap;
+      s_tally[threadIdx.x].own_tag = threadIdx.x << 16;
+    }
+    if (threadIdx.x == 0) s_nown = 0;
     {
       long long nh = 0, nu = 0;
       if (mine) {
@@ -1920,8 +1936,15 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
     }
     __syncthreads();
     if (threadIdx.x < K && s_act[threadIdx.x]) tally_flush(&s_tally[threadIdx.x], jobs[threadIdx.x].a.ctl);
-    if (grid_barrier(gc, &target, false, &s_state) < 0) return;
-    // apply + commit of every job's batch; one thread per job closes it
+    const int nown = s_nown;
+    if (grid_barrier(gc, &target, false, &s_state, nown > kOwnCap, &s_ovf) < 0) return;
+    // as in k_nodal_phase: every CTA reads the same overflow count here
+    const bool scan_all = s_ovf != ovf_seen;
+    ovf_seen = s_ovf;
+    // apply + commit of every job's batch; one thread per job closes it.
+    // Each CTA applies the moves it accepted (its listed work-unit chunks
+    // and its moved hubs), or, after an overflow anywhere, every CTA takes
+    // its share of all jobs' batch chunks.
     if (blockIdx.x == 0) {
       if (threadIdx.x < K && s_act[threadIdx.x]) {
         const PhaseArgs& p = jobs[threadIdx.x];
@@ -1934,7 +1957,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
       if (threadIdx.x == 0) gc->vnext = 0;
     }
     tables_clear(dt);
-    {
+    if (scan_all) {
       long long c = 0;
       if (mine) {
         const PhaseArgs& p = jobs[threadIdx.x];
@@ -1942,17 +1965,42 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
         c = __ldg(p.chunk_ptr + end) - __ldg(p.chunk_ptr + beg);
       }
       job_prefix(c, s_tmp, s_cp);
-    }
-    const long long C = s_cp[K];
-    for (long long q = gw; q < C; q += nw) {
-      const int j = find_job(s_cp, K, q);
-      const PhaseArgs& p = jobs[j];
-      const int beg = s_bi[j] * p.bs, end = min(p.n, beg + p.bs);
-      const int2 ch = __ldg(p.g.chunks + __ldg(p.chunk_ptr + beg) + (q - s_cp[j]));
-      DeltaTables tj = dt;
-      tj.tag = j << 24;
-      apply_chunk<LdCG, LdCG>(ch, p.g, p.part, p.a.move_to, p.a.from, beg, end, tj, p.v.ld, p.M, p.Mt, p.v.cld,
-                              p.CS, p.dout, p.din, lane);
+      const long long C = s_cp[K];
+      for (long long q = gw; q < C; q += nw) {
+        const int j = find_job(s_cp, K, q);
+        const PhaseArgs& p = jobs[j];
+        const int beg = s_bi[j] * p.bs, end = min(p.n, beg + p.bs);
+        const int2 ch = __ldg(p.g.chunks + __ldg(p.chunk_ptr + beg) + (q - s_cp[j]));
+        DeltaTables tj = dt;
+        tj.tag = j << 24;
+        apply_chunk<LdCG, LdCG>(ch, p.g, p.part, p.a.move_to, p.a.from, beg, end, tj, p.v.ld, p.M, p.Mt,
+                                p.v.cld, p.CS, p.dout, p.din, lane);
+      }
+    } else {
+      __syncthreads();
+      for (int i = wib; i < nown; i += kPWarps) {
+        const int2 e = s_own[i];
+        const int j = e.y >> 16;
+        const PhaseArgs& p = jobs[j];
+        const int beg = s_bi[j] * p.bs, end = min(p.n, beg + p.bs);
+        DeltaTables tj = dt;
+        tj.tag = j << 24;
+        apply_chunk<LdCG, LdCG>(make_int2(e.x, e.y & 0xffff), p.g, p.part, p.a.move_to, p.a.from, beg, end, tj,
+                                p.v.ld, p.M, p.Mt, p.v.cld, p.CS, p.dout, p.din, lane);
+      }
+      for (int h = blockIdx.x; h < H; h += gridDim.x) {   // the hubs this CTA proposed for
+        const int j = find_job(s_hp, K, h);
+        const PhaseArgs& p = jobs[j];
+        const int v = __ldg(p.hubs + __ldg(p.batch_hub + s_bi[j]) + (h - static_cast<int>(s_hp[j])));
+        if (__ldcg(p.a.move_to + v) < 0) continue;   // CTA-uniform
+        const int beg = s_bi[j] * p.bs, end = min(p.n, beg + p.bs);
+        DeltaTables tj = dt;
+        tj.tag = j << 24;
+        const int64_t q1 = __ldg(p.chunk_ptr + v + 1);
+        for (int64_t q = __ldg(p.chunk_ptr + v) + wib; q < q1; q += kPWarps)
+          apply_chunk<LdCG, LdCG>(__ldg(p.g.chunks + q), p.g, p.part, p.a.move_to, p.a.from, beg, end, tj, p.v.ld,
+                                  p.M, p.Mt, p.v.cld, p.CS, p.dout, p.din, lane);
+      }
     }
     gang_tables_flush(dt, jobs);
     if (grid_barrier(gc, &target, false, &s_state) < 0) return;

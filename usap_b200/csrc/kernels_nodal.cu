@@ -28,11 +28,15 @@
 // Two schedules run the same device code.  Per batch launches: a proposal
 // kernel (hubs in a second kernel on a side stream) and an apply kernel.
 // Persistent: one cooperative launch runs a stage's whole nodal phase,
-// one 1024-thread CTA per SM, with grid barriers between entropy, sweep
+// one 768-thread CTA per SM, with grid barriers between entropy, sweep
 // start, proposals and apply; it removes the launch gaps that otherwise
-// cost about half of each batch.  State written inside that kernel (the
-// partition, M, degrees, chunk sums, moves) is read through L2 (ld.cg);
-// the non-coherent path is used only for data that no phase writes.
+// cost about half of each batch.  There each CTA applies the moves it
+// accepted itself (listed in shared memory while proposing), and for small
+// B the proposals read a per-batch copy of the tile in shared memory.
+// State written inside that kernel (the partition, M, degrees, chunk sums,
+// moves) is otherwise read through L2 (ld.cg); the non-coherent path is
+// used only for data that no phase writes.  The gang kernel runs the same
+// phase for many jobs at once.
 #include <cmath>
 #include <mutex>
 #include <type_traits>

@@ -90,7 +90,18 @@ typedef struct usap_params {
                           FP32 terms from the rounded log table, compensated sums only (loses
                           accuracy on large counts; kept to measure that).  The description
                           length, the golden-section comparisons and the convergence test stay
-                          FP64 in every mode. */
+                          FP64 in every mode.
+                          3: the reference's own single-precision nodal dS
+                          (graph_parallel.hpp:1066-1215): every term count * logf((float)count /
+                          (float)(d_a * d_b)) in float, added to one float accumulator in the
+                          reference's term order over all B blocks; accept iff it is < 0, and the
+                          accepted float values are what the convergence test sums (:428-444),
+                          as in the reference.  Merges stay exact.  The rounding noise of that
+                          O(B) float sum is part of the reference's behaviour: with it the solve
+                          ends at the reference's block counts and NMI, where exact arithmetic
+                          (mode 0, or the reference itself compiled with double) ends at fewer
+                          blocks on large graphs.  usap_result.fp32_* compare it with the exact
+                          value. */
   int32_t reserved[1];
 } usap_params;
 

@@ -19,6 +19,7 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle_usap.so")
 i32p = C.POINTER(C.c_int32)
 i64p = C.POINTER(C.c_int64)
 u32p = C.POINTER(C.c_uint32)
+f32p = C.POINTER(C.c_float)
 
 
 class OgGraph(C.Structure):
@@ -45,7 +46,8 @@ class OgParams(C.Structure):
                 ("delta_entropy_moving_avg_window", C.c_int32),
                 ("dfs_depth", C.c_int32),
                 ("seed", C.c_uint64),
-                ("init_mode", C.c_int32)]
+                ("init_mode", C.c_int32),
+                ("precision", C.c_int32)]
 
 
 class OgTraceEvent(C.Structure):
@@ -143,6 +145,15 @@ def lib() -> C.CDLL:
                                      C.c_int32, C.c_int32, C.c_int32, C.c_uint64, i32p, i64p,
                                      i32p, i64p, i32p, i64p]
         L.og_nodal_batch.restype = C.c_int64
+        L.og_nodal_batch_p.argtypes = [C.POINTER(OgGraph), i32p, C.POINTER(OgBlocks), C.c_int32,
+                                       C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, i32p,
+                                       i64p, i32p, f32p, i64p, i32p, i64p]
+        L.og_nodal_batch_p.restype = C.c_int64
+        L.og_log_f32.argtypes = [C.c_float]
+        L.og_log_f32.restype = C.c_float
+        L.og_nodal_ds_ref32.argtypes = [C.POINTER(OgGraph), i32p, C.POINTER(OgBlocks), C.c_int32,
+                                        C.c_int32]
+        L.og_nodal_ds_ref32.restype = C.c_float
         L.og_golden_init.argtypes = [C.POINTER(OgGolden)]
         L.og_golden_step.argtypes = [C.POINTER(OgGolden), C.c_int32, C.c_double, C.c_int64, C.c_int32,
                                      C.c_float, i32p, i32p, i32p]
@@ -311,19 +322,25 @@ class OracleBlocks:
                              _p32(best_s), _p64(best_q))
         return best_s, best_q
 
-    def nodal_batch(self, beg: int, end: int, itr: int, stage: int, seed: int):
+    def nodal_ds_ref32(self, v: int, s: int) -> float:
+        """The reference's float nodal dS (precision mode 3) of v moving to s."""
+        return float(lib().og_nodal_ds_ref32(C.byref(self.g.g), _p32(self.part), C.byref(self.b), v, s))
+
+    def nodal_batch(self, beg: int, end: int, itr: int, stage: int, seed: int, precision: int = 0):
         """Runs one batch in place; returns per-vertex proposals and totals."""
         cnt = end - beg
         ps = np.empty(cnt, np.int32)
         pq = np.empty(cnt, np.int64)
         pn = np.empty(cnt, np.int32)
+        pf = np.empty(cnt, np.float32)
         cum_q = C.c_int64(0)
         cum_n = C.c_int32(0)
         near = C.c_int64(0)
-        moves = lib().og_nodal_batch(C.byref(self.g.g), _p32(self.part), C.byref(self.b), beg,
-                                     end, itr, stage, seed, _p32(ps), _p64(pq), _p32(pn),
-                                     C.byref(cum_q), C.byref(cum_n), C.byref(near))
-        return {"prop_s": ps, "prop_q": pq, "prop_ninf": pn, "moves": int(moves),
+        moves = lib().og_nodal_batch_p(C.byref(self.g.g), _p32(self.part), C.byref(self.b), beg,
+                                       end, itr, stage, seed, precision, _p32(ps), _p64(pq), _p32(pn),
+                                       pf.ctypes.data_as(f32p), C.byref(cum_q), C.byref(cum_n),
+                                       C.byref(near))
+        return {"prop_s": ps, "prop_q": pq, "prop_ninf": pn, "prop_f": pf, "moves": int(moves),
                 "cum_q": int(cum_q.value), "cum_ninf": int(cum_n.value),
                 "near": int(near.value)}
 

@@ -584,6 +584,132 @@ int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
   return og_nodal_dq_impl(g, part, b, v, s, neg_inf, NULL);
 }
 
+/* ------------------------------------------------------------------------ */
+/* Precision mode 3: the reference's own single-precision nodal dS.
+ *
+ * The reference evaluates dS in `float` (:1066-1215): every term is
+ * count * std::log((float)count / (long)(d_a * d_b)) -- the long product
+ * converted to float, a float division, logf of the ratio, a float product
+ * -- and the terms are added to one float accumulator in the order of its
+ * loops over all B blocks.  Rounding noise of that O(B) sum decides many
+ * near-zero proposals, and the reference's solve quality depends on it:
+ * the reference compiled with double in place of float ends at far fewer
+ * blocks on the N=50000 workload.  Mode 3 evaluates exactly that
+ * expression, term order included.                                         */
+
+/* log(x) for a float x, rounded to float.  Evaluated in double: x = m * 2^e
+ * with m in [sqrt(1/2), sqrt(2)], log x = e * ln 2 + 2 atanh(z) with
+ * z = (m - 1) / (m + 1) and atanh z = z + z^3/3 + z^5/5 + ... (the
+ * classical series for log((1 + z) / (1 - z)); |z| <= 0.1716, 13 terms,
+ * truncation below 1e-19 relative).  Only IEEE double +, -, *, / are used,
+ * without contraction, so the CUDA kernels' copy of these steps returns the
+ * same bits.  x = 0 gives -inf, x = +inf gives +inf. */
+float og_log_f32(float x) {
+  if (isnan(x) || x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (isinf(x)) return INFINITY;
+  uint32_t u;
+  memcpy(&u, &x, sizeof(u));
+  int e = (int)((u >> 23) & 0xffu);
+  const uint32_t frac = u & 0x7fffffu;
+  double m;
+  if (e == 0) {                      /* subnormal */
+    m = (double)frac * 0x1p-23;
+    e = -126;
+    while (m < 1.0) { m = m * 2.0; e -= 1; }
+  } else {
+    m = 1.0 + (double)frac * 0x1p-23;
+    e -= 127;
+  }
+  if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
+  const double z = (m - 1.0) / (m + 1.0);
+  const double z2 = z * z;
+  double p = 1.0 / 25.0;
+  p = p * z2 + 1.0 / 23.0;
+  p = p * z2 + 1.0 / 21.0;
+  p = p * z2 + 1.0 / 19.0;
+  p = p * z2 + 1.0 / 17.0;
+  p = p * z2 + 1.0 / 15.0;
+  p = p * z2 + 1.0 / 13.0;
+  p = p * z2 + 1.0 / 11.0;
+  p = p * z2 + 1.0 / 9.0;
+  p = p * z2 + 1.0 / 7.0;
+  p = p * z2 + 1.0 / 5.0;
+  p = p * z2 + 1.0 / 3.0;
+  p = p * z2 + 1.0;
+  const double lm = (2.0 * z) * p;
+  return (float)((double)e * 0.69314718055994530942 + lm);
+}
+
+/* count * log((float)count / (float)prod), as the reference rounds it */
+static inline float og_ref_term(int64_t x, int64_t prod) {
+  const float xf = (float)x;
+  const float ratio = xf / (float)prod;
+  return xf * og_log_f32(ratio);
+}
+
+/* _propose_new_partition_nodal's dS (:1066-1215) for v moving to s, in the
+ * reference's float arithmetic and term order: the old terms of rows r, s
+ * and columns r, s (columns skip i in {r, s}) in block order; the deltas of
+ * v's out-edges (rows) and in-edges (columns; the 2x2 row entries are not
+ * adjusted for in-edges, :1135-1142); the four new 2x2 terms; the new terms
+ * of rows and columns for i not in {r, s} in block order.  A term whose
+ * count is 0 is skipped.  Returns 0 when s == part[v]. */
+float og_nodal_ds_ref32(const og_graph* g, const int32_t* part, const og_blocks* b, int32_t v,
+                        int32_t s) {
+  const int32_t B = b->B, r = part[v];
+  if (r == s) return 0.0f;
+  const int64_t* M = b->M;
+  int64_t* rr = malloc(sizeof(int64_t) * 4 * (size_t)B);
+  int64_t *sr = rr + B, *rc = rr + 2 * (size_t)B, *sc = rr + 3 * (size_t)B;
+  for (int32_t i = 0; i < B; i++) {
+    rr[i] = M[(size_t)r * B + i];
+    sr[i] = M[(size_t)s * B + i];
+    rc[i] = M[(size_t)i * B + r];
+    sc[i] = M[(size_t)i * B + s];
+  }
+  const int64_t* din = b->din;
+  const int64_t* dout = b->dout;
+  const int64_t kout = g->kout[v], kin = g->kin[v];
+  const int64_t dor_n = dout[r] - kout, dos_n = dout[s] + kout;
+  const int64_t dir_n = din[r] - kin, dis_n = din[s] + kin;
+  float dS = 0.0f;
+  for (int32_t i = 0; i < B; i++) {                       /* :1096-1114 */
+    if (rr[i] != 0) dS = dS + og_ref_term(rr[i], din[i] * dout[r]);
+    if (sr[i] != 0) dS = dS + og_ref_term(sr[i], din[i] * dout[s]);
+    if (i != r && i != s) {
+      if (rc[i] != 0) dS = dS + og_ref_term(rc[i], dout[i] * din[r]);
+      if (sc[i] != 0) dS = dS + og_ref_term(sc[i], dout[i] * din[s]);
+    }
+  }
+  for (int64_t p = g->out_ptr[v]; p < g->out_ptr[v + 1]; p++) {   /* :1119-1129 */
+    const int32_t bb = part[g->out_idx[p]];
+    rr[bb] -= g->out_w[p];
+    sr[bb] += g->out_w[p];
+  }
+  for (int64_t p = g->in_ptr[v]; p < g->in_ptr[v + 1]; p++) {     /* :1130-1145 */
+    const int32_t bb = part[g->in_idx[p]];
+    rc[bb] -= g->in_w[p];
+    sc[bb] += g->in_w[p];
+  }
+  if (rr[r] != 0) dS = dS - og_ref_term(rr[r], dir_n * dor_n);     /* :1180-1195 */
+  if (rr[s] != 0) dS = dS - og_ref_term(rr[s], dis_n * dor_n);
+  if (sr[r] != 0) dS = dS - og_ref_term(sr[r], dir_n * dos_n);
+  if (sr[s] != 0) dS = dS - og_ref_term(sr[s], dis_n * dos_n);
+  for (int32_t i = 0; i < B; i++) {                       /* :1196-1215 */
+    if (i == r || i == s) continue;
+    if (rr[i] != 0) dS = dS - og_ref_term(rr[i], din[i] * dor_n);
+    if (sr[i] != 0) dS = dS - og_ref_term(sr[i], din[i] * dos_n);
+    if (rc[i] != 0) dS = dS - og_ref_term(rc[i], dout[i] * dir_n);
+    if (sc[i] != 0) dS = dS - og_ref_term(sc[i], dout[i] * dis_n);
+  }
+  free(rr);
+  return dS;
+}
+
+/* Q32 of a float dS (-inf is flagged by the caller) */
+static inline int64_t og_q32_f(float f) { return og_quantize((double)f); }
+
 int64_t og_nodal_dq_f32(const og_graph* g, const int32_t* part, const og_blocks* b,
                         int32_t v, int32_t s, int32_t mode, int32_t* neg_inf, og_fsum* f) {
   f->s = f->c = f->abs = 0.0;
@@ -723,11 +849,15 @@ int32_t og_merge_apply(int32_t n, int32_t* part, int32_t B, const int32_t* best_
   return B - num;
 }
 
-/* nodal_move + update tasks for one batch (:397-443) */
-int64_t og_nodal_batch(const og_graph* g, int32_t* part, og_blocks* b, int32_t beg,
-                       int32_t end, int32_t itr, int32_t stage, uint64_t seed,
-                       int32_t* prop_s, int64_t* prop_q, int32_t* prop_ninf,
-                       int64_t* cum_q, int32_t* cum_ninf, int64_t* near_threshold) {
+/* nodal_move + update tasks for one batch (:397-443).  precision 3: the
+ * accept decision is the reference's float dS < 0 (-inf included), and the
+ * accepted float values are what the convergence sums add (:428-430), in
+ * Q32; the exact value still gives prop_q and the near-threshold count.
+ * prop_f (optional) receives the float dS of each proposal.               */
+int64_t og_nodal_batch_p(const og_graph* g, int32_t* part, og_blocks* b, int32_t beg,
+                         int32_t end, int32_t itr, int32_t stage, uint64_t seed, int32_t precision,
+                         int32_t* prop_s, int64_t* prop_q, int32_t* prop_ninf, float* prop_f,
+                         int64_t* cum_q, int32_t* cum_ninf, int64_t* near_threshold) {
   int32_t cnt = end - beg;
   int32_t* mv = malloc(sizeof(int32_t) * ((size_t)cnt + 1));
   int64_t moves = 0;
@@ -735,21 +865,34 @@ int64_t og_nodal_batch(const og_graph* g, int32_t* part, og_blocks* b, int32_t b
     int32_t s = og_nodal_propose(g, part, b, v, itr, stage, seed);
     int32_t ninf = 0;
     int64_t q = 0;
+    float f = 0.0f;
     int32_t r = part[v];
     int accept = 0;
     if (s != r) {
       q = og_nodal_dq(g, part, b, v, s, &ninf);
-      accept = ninf || q < 0;
       if (!ninf && (q <= OG_NEAR_Q && q >= -OG_NEAR_Q) && near_threshold) (*near_threshold)++;
+      if (precision == 3) {
+        f = og_nodal_ds_ref32(g, part, b, v, s);
+        accept = f < 0.0f;
+      } else {
+        accept = ninf || q < 0;
+      }
     }
     if (prop_s) prop_s[v - beg] = (s != r) ? s : -1;
     if (prop_q) prop_q[v - beg] = q;
     if (prop_ninf) prop_ninf[v - beg] = ninf;
+    if (prop_f) prop_f[v - beg] = f;
     mv[v - beg] = accept ? s : -1;
     if (accept) {
       moves++;
-      if (ninf) *cum_ninf = 1;
-      else *cum_q += q;
+      if (precision == 3) {
+        if (isinf(f)) *cum_ninf = 1;
+        else *cum_q += og_q32_f(f);
+      } else if (ninf) {
+        *cum_ninf = 1;
+      } else {
+        *cum_q += q;
+      }
     }
   }
   for (int32_t v = beg; v < end; v++)
@@ -757,6 +900,14 @@ int64_t og_nodal_batch(const og_graph* g, int32_t* part, og_blocks* b, int32_t b
   og_build(g, part, b);
   free(mv);
   return moves;
+}
+
+int64_t og_nodal_batch(const og_graph* g, int32_t* part, og_blocks* b, int32_t beg,
+                       int32_t end, int32_t itr, int32_t stage, uint64_t seed,
+                       int32_t* prop_s, int64_t* prop_q, int32_t* prop_ninf,
+                       int64_t* cum_q, int32_t* cum_ninf, int64_t* near_threshold) {
+  return og_nodal_batch_p(g, part, b, beg, end, itr, stage, seed, 0, prop_s, prop_q, prop_ninf, NULL,
+                          cum_q, cum_ninf, near_threshold);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -813,6 +964,7 @@ void og_params_default(og_params* p) {
   p->dfs_depth = 20;
   p->seed = 0;
   p->init_mode = 0;
+  p->precision = 0;
 }
 
 static inline int32_t og_reduce(int32_t B, float rate) {
@@ -982,8 +1134,8 @@ static int og_partition_impl(const og_graph* g, const og_params* p, const int32_
       res->sweeps++;
       for (int32_t beg = 0; beg < n; beg += bs) {
         int32_t end = beg + bs < n ? beg + bs : n;
-        int64_t mv = og_nodal_batch(g, part, &blk, beg, end, itr, stage, p->seed, NULL, NULL,
-                                    NULL, &cum_q, &cum_n, &res->near_threshold);
+        int64_t mv = og_nodal_batch_p(g, part, &blk, beg, end, itr, stage, p->seed, p->precision,
+                                      NULL, NULL, NULL, NULL, &cum_q, &cum_n, &res->near_threshold);
         res->batches++;
         res->nodal_proposals += end - beg;
         res->nodal_moves += mv;

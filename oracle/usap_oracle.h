@@ -71,6 +71,7 @@ typedef struct {
   int32_t dfs_depth;                     /* graph_parallel.hpp:51 */
   uint64_t seed;
   int32_t init_mode;                     /* 0: SCC (reference), 1: identity */
+  int32_t precision;                     /* 0: exact Q32 dS; 3: the reference's float nodal dS */
 } og_params;
 
 typedef struct {
@@ -137,6 +138,11 @@ int64_t og_merge_dq_f32(const og_graph* g, const og_blocks* b, int32_t r, int32_
 int64_t og_nodal_dq_f32(const og_graph* g, const int32_t* part, const og_blocks* b,
                         int32_t v, int32_t s, int32_t mode, int32_t* neg_inf, og_fsum* f);
 double og_fsum_value(const og_fsum* f);
+/* precision mode 3: log rounded to float (own evaluation, bit-identical on
+ * the CUDA path) and the reference's float nodal dS in its term order */
+float og_log_f32(float x);
+float og_nodal_ds_ref32(const og_graph* g, const int32_t* part, const og_blocks* b, int32_t v,
+                        int32_t s);
 int32_t og_merge_propose(const og_graph* g, const og_blocks* b, int32_t r, int32_t k,
                          int32_t stage, uint64_t seed);
 int32_t og_nodal_propose(const og_graph* g, const int32_t* part, const og_blocks* b,
@@ -153,6 +159,10 @@ int64_t og_nodal_batch(const og_graph* g, int32_t* part, og_blocks* b, int32_t b
                        int32_t end, int32_t itr, int32_t stage, uint64_t seed,
                        int32_t* prop_s, int64_t* prop_q, int32_t* prop_ninf,
                        int64_t* cum_q, int32_t* cum_ninf, int64_t* near_threshold);
+int64_t og_nodal_batch_p(const og_graph* g, int32_t* part, og_blocks* b, int32_t beg,
+                         int32_t end, int32_t itr, int32_t stage, uint64_t seed, int32_t precision,
+                         int32_t* prop_s, int64_t* prop_q, int32_t* prop_ninf, float* prop_f,
+                         int64_t* cum_q, int32_t* cum_ninf, int64_t* near_threshold);
 
 /* --- golden-section search over B (host-side in the product) ------------- */
 typedef struct { int32_t B; double S; int64_t S_q; int32_t finite; int32_t slot; } og_gpoint;

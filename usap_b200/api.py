@@ -168,8 +168,9 @@ class Context:
 
     def op_nodal_batch(self, part, B: int, beg: int, end: int, itr: int, stage: int, seed: int,
                        dense_max: int = 4096, precision: int = 0):
-        """one nodal batch; in precision mode 1 or 2 the accept decisions are
-        taken on the FP32 dS, returned as prop_f beside the exact prop_q."""
+        """one nodal batch; in precision mode 1, 2 or 3 the accept decisions
+        are taken on the FP32 dS (mode 3: the reference's float expression),
+        returned as prop_f beside the exact prop_q."""
         part = np.ascontiguousarray(part, np.int32).copy()
         cnt = end - beg
         ps = np.empty(cnt, np.int32)

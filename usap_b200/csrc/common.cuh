@@ -195,6 +195,66 @@ __device__ __forceinline__ FF h_term_ff(const float2* __restrict__ T, long long 
   return FF{__fsub_rn(__fadd_rn(a, b), c), 0.0f};
 }
 
+// --- precision mode 3: the reference's own float arithmetic --------------
+// The float-pair terms above exist for modes 1 and 2; mode 3 reproduces the
+// reference's single-precision dS instead.
+template <int P>
+constexpr bool kPairTerms = (P == 1 || P == 2);
+
+// log(x) rounded to float.  x = m * 2^e with m in [sqrt(1/2), sqrt(2)];
+// log x = e * ln 2 + 2 atanh(z), z = (m - 1) / (m + 1), atanh by its series
+// z + z^3/3 + z^5/5 + ... (13 terms; |z| <= 0.1716).  IEEE double +, -, *, /
+// only, in the same order as the oracle's og_log_f32, so host and device
+// agree bit for bit; the result is log x correctly rounded to float except
+// when log x lies within ~1e-16 relative of a rounding boundary.
+__device__ __forceinline__ float ref_logf(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? __int_as_float(0xff800000) : __int_as_float(0x7fc00000);
+  const unsigned u = __float_as_uint(x);
+  if (u >= 0x7f800000u) return x;   // +inf
+  int e = static_cast<int>((u >> 23) & 0xffu);
+  const unsigned frac = u & 0x7fffffu;
+  double m;
+  if (e == 0) {
+    m = __dmul_rn(static_cast<double>(frac), 0x1p-23);
+    e = -126;
+    while (m < 1.0) {
+      m = __dmul_rn(m, 2.0);
+      e -= 1;
+    }
+  } else {
+    m = __dadd_rn(1.0, __dmul_rn(static_cast<double>(frac), 0x1p-23));
+    e -= 127;
+  }
+  if (m > 1.4142135623730951) {
+    m = __dmul_rn(m, 0.5);
+    e += 1;
+  }
+  const double z = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
+  const double z2 = __dmul_rn(z, z);
+  double p = 1.0 / 25.0;
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 23.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 21.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 19.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 17.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 15.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 13.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 11.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 9.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 7.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 5.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 3.0);
+  p = __dadd_rn(__dmul_rn(p, z2), 1.0);
+  const double lm = __dmul_rn(__dmul_rn(2.0, z), p);
+  return __double2float_rn(__dadd_rn(__dmul_rn(static_cast<double>(e), 0.69314718055994530942), lm));
+}
+
+// one term of the reference's dS: count * log((float)count / (float)prod),
+// the long product converted to float, a float division, a float product
+__device__ __forceinline__ float ref_term(long long x, long long prod) {
+  const float xf = __ll2float_rn(x);
+  return __fmul_rn(xf, ref_logf(__fdiv_rn(xf, __ll2float_rn(prod))));
+}
+
 // |dS_fp32 - dS_fp64| of one evaluation; f is the FP32 pair's value, the
 // FP64 value is the exact sum acc / 2^32
 __device__ __forceinline__ double f32_err(double f, long long acc) {

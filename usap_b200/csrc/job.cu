@@ -560,13 +560,14 @@ void Job::merge_phase(const int32_t* part, int32_t B, int32_t K, uint32_t stage,
   a.prop_s = prop_s_;
   a.prop_q = prop_q_;
   a.L2 = g_.logk2;
-  a.prec = prec_;
-  a.prop_x = prec_ ? prop_x_ : nullptr;
-  a.prop_f = prec_ ? prop_f_ : nullptr;
-  a.f32 = prec_ ? f32d_ : nullptr;
+  const int mp = merge_prec();
+  a.prec = mp;
+  a.prop_x = mp ? prop_x_ : nullptr;
+  a.prop_f = mp ? prop_f_ : nullptr;
+  a.f32 = mp ? f32d_ : nullptr;
   if (dense) launch_merge_propose_dense(dense_view(), a, st_);
   else launch_merge_propose(g_, sb_.view(), a, st_);
-  launch_merge_argmin(B, K, prop_s_, prop_q_, a.prop_x, best_s_, best_q_, prec_ ? best_x_ : nullptr, a.f32, st_);
+  launch_merge_argmin(B, K, prop_s_, prop_q_, a.prop_x, best_s_, best_q_, mp ? best_x_ : nullptr, a.f32, st_);
 }
 
 int32_t Job::merge_apply(int32_t* part, int32_t B, int32_t btm) {
@@ -864,7 +865,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
   if (p.delta_entropy_moving_avg_window < 1) throw Error(USAP_ERR_INVALID, "moving average window must be >= 1");
   if (!(p.num_block_reduction_rate > 0.0f && p.num_block_reduction_rate < 1.0f))
     throw Error(USAP_ERR_INVALID, "num_block_reduction_rate must be in (0, 1)");
-  if (p.precision < 0 || p.precision > 2) throw Error(USAP_ERR_INVALID, "precision must be 0, 1 or 2");
+  if (p.precision < 0 || p.precision > 3) throw Error(USAP_ERR_INVALID, "precision must be 0, 1, 2 or 3");
   const int dense_max = p.dense_max > 0 ? p.dense_max : 4096;
   auto t_start = std::chrono::steady_clock::now();
   std::memset(res, 0, sizeof(*res));
@@ -917,7 +918,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
     // beats rebuilding the sorted views, above it does not
     merge_phase(part, B, K, stage, seed, B <= std::min(dense_max, kDenseMergeMax));
     int32_t merged = merge_apply(part, B, btm);
-    if (prec_) launch_order_flips(B, sidx_alt_, best_x_, &f32d_[1].flips, st_);
+    if (merge_prec()) launch_order_flips(B, sidx_alt_, best_x_, &f32d_[1].flips, st_);
     d2h += sizeof(int32_t);
     if (merged < btm) res->merge_shortfall += btm - merged;
     B -= merged;
@@ -1273,7 +1274,7 @@ void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stag
   if (K < 1) throw Error(USAP_ERR_INVALID, "K must be >= 1");
   USAP_CUDA(cudaSetDevice(device_));
   ensure_capacity(B, K, dense_max, 1);
-  if (prec < 0 || prec > 2) throw Error(USAP_ERR_INVALID, "precision must be 0, 1 or 2");
+  if (prec < 0 || prec > 3) throw Error(USAP_ERR_INVALID, "precision must be 0, 1, 2 or 3");
   prec_ = prec;
   if (prec_) USAP_CUDA(cudaMemsetAsync(f32d_, 0, 2 * sizeof(F32Tally), st_));
   USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));
@@ -1283,10 +1284,10 @@ void Job::op_merge_phase(const int32_t* part, int32_t B, int32_t K, int32_t stag
   USAP_CUDA(cudaMemcpyAsync(best_q, best_q_, sizeof(int64_t) * B, cudaMemcpyDeviceToHost, st_));
   if (prop_s) USAP_CUDA(cudaMemcpyAsync(prop_s, prop_s_, sizeof(int32_t) * nk, cudaMemcpyDeviceToHost, st_));
   if (prop_q)
-    USAP_CUDA(cudaMemcpyAsync(prop_q, prec_ ? prop_x_ : prop_q_, sizeof(int64_t) * nk, cudaMemcpyDeviceToHost, st_));
-  if (prec_ && prop_f) USAP_CUDA(cudaMemcpyAsync(prop_f, prop_f_, sizeof(double) * nk, cudaMemcpyDeviceToHost, st_));
+    USAP_CUDA(cudaMemcpyAsync(prop_q, merge_prec() ? prop_x_ : prop_q_, sizeof(int64_t) * nk, cudaMemcpyDeviceToHost, st_));
+  if (merge_prec() && prop_f) USAP_CUDA(cudaMemcpyAsync(prop_f, prop_f_, sizeof(double) * nk, cudaMemcpyDeviceToHost, st_));
   F32Tally m{0, 0, 0, 0.0};
-  if (prec_) USAP_CUDA(cudaMemcpyAsync(&m, f32d_, sizeof(m), cudaMemcpyDeviceToHost, st_));
+  if (merge_prec()) USAP_CUDA(cudaMemcpyAsync(&m, f32d_, sizeof(m), cudaMemcpyDeviceToHost, st_));
   USAP_CUDA(cudaStreamSynchronize(st_));
   if (flips) *flips = static_cast<int64_t>(m.flips);
   prec_ = 0;
@@ -1316,7 +1317,7 @@ void Job::op_nodal_batch(int32_t* part, int32_t B, int32_t dense_max, int32_t be
   if (!loaded()) throw Error(USAP_ERR_STATE, "no graph loaded");
   if (beg < 0 || end > hg_->n || beg > end) throw Error(USAP_ERR_INVALID, "batch range out of bounds");
   USAP_CUDA(cudaSetDevice(device_));
-  if (prec < 0 || prec > 2) throw Error(USAP_ERR_INVALID, "precision must be 0, 1 or 2");
+  if (prec < 0 || prec > 3) throw Error(USAP_ERR_INVALID, "precision must be 0, 1, 2 or 3");
   prec_ = prec;
   ensure_capacity(B, 1, dense_max, 1);
   USAP_CUDA(cudaMemcpyAsync(slots_[0], part, sizeof(int32_t) * hg_->n, cudaMemcpyHostToDevice, st_));

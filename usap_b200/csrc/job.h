@@ -301,6 +301,9 @@ class Job {
   // precision mode of the current solve; with modes 1, 2: [0] merge
   // proposals, [1].flips merge-order inversions
   int prec_ = 0;
+  // the merge phase's mode: mode 3 changes only the nodal dS (the
+  // reference's float merge dS does not move its solve) and keeps merges exact
+  int merge_prec() const { return prec_ == 3 ? 0 : prec_; }
   F32Tally* f32d_ = nullptr;
   unsigned long long *skeys_ = nullptr, *skeys_alt_ = nullptr;
   int32_t *sidx_ = nullptr, *sidx_alt_ = nullptr;

@@ -128,6 +128,10 @@ struct DenseOpsT {
   __device__ __forceinline__ int get(int x, int y) const {
     return LDT::ld(v.M + static_cast<long long>(x) * v.ld + y);
   }
+  // M[y, x], read from row x of the transposed tile (coalesced over y)
+  __device__ __forceinline__ int get_t(int x, int y) const {
+    return LDT::ld(v.Mt + static_cast<long long>(x) * v.ld + y);
+  }
   // first block i (block-id order) whose cumulative M[u,i]+M[i,u] exceeds t:
   // a group scan over the row's chunk sums, then over the 128 entries of the
   // chosen chunk (128 / G per lane, 16-byte loads; rows are padded to ld, a
@@ -201,6 +205,7 @@ struct SortedOpsT {
     int p = find_sorted(v.col, lo, hi, y);
     return p >= 0 ? __ldg(v.val + p) : 0;
   }
+  __device__ __forceinline__ int get_t(int x, int y) const { return get(y, x); }
   template <int G>
   __device__ __forceinline__ int sym_sample(int u, long long t, const Grp<G>&, int* scanned) const {
     int lo = __ldg(v.symptr + u), hi = __ldg(v.symptr + u + 1);
@@ -322,7 +327,7 @@ __device__ __forceinline__ DegLogs deg_logs(const NodalArgs& a, long long dr_out
   const double* __restrict__ L = a.L;
   DegLogs d{__ldg(L + dr_out), __ldg(L + ds_out), __ldg(L + dr_out - kout), __ldg(L + ds_out + kout),
             __ldg(L + dr_in),  __ldg(L + ds_in),  __ldg(L + dr_in - kin),   __ldg(L + ds_in + kin)};
-  if constexpr (P > 0) {
+  if constexpr (kPairTerms<P>) {
     const float2* __restrict__ T = a.L2;
     d.fr_out = ld_ff(T, dr_out);
     d.fs_out = ld_ff(T, ds_out);
@@ -360,7 +365,7 @@ __device__ __forceinline__ void pair_terms(const NodalArgs& a, int X, int Y, int
   ts.acc += q32(g_val(Y, LY, col ? b0 : LD, col ? LD : b0));
   ts.acc -= q32(g_val(X - w, LXn, col ? a1 : LD, col ? LD : a1));
   ts.acc -= q32(g_val(Y + w, LYn, col ? b1 : LD, col ? LD : b1));
-  if constexpr (P > 0) {
+  if constexpr (kPairTerms<P>) {
     const float2* __restrict__ T = a.L2;
     const FF fD = ld_ff(T, D);
     const FF fa0 = col ? dl.fr_in : dl.fr_out, fb0 = col ? dl.fs_in : dl.fs_out;
@@ -449,7 +454,7 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
   long long q = inf ? 0 : q32(t);
   if (neg) q = -q;
   *ninf = g.any(inf) ? 1 : 0;
-  if constexpr (P > 0) {
+  if constexpr (kPairTerms<P>) {
     FF t32{0.0f, 0.0f};
     if (mult != 0 && !inf) {
       const FF A = ld_ff(a.L2, i0), Bv = ld_ff(a.L2, i1);
@@ -459,6 +464,94 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
     *f = ff_value(g.ffsum(fpart));
   }
   return ts.acc + g.sum(q);
+}
+
+// Precision mode 3: the reference's single-precision dS of v (block r)
+// moving to s, _propose_new_partition_nodal (graph_parallel.hpp:1066-1215),
+// in its float arithmetic and term order, by a group of G lanes:
+//  1. the old terms of rows r, s and (i not in {r, s}) columns r, s, block
+//     by block (:1096-1114);
+//  2. the four new 2x2 terms, the row entries adjusted by v's out-edges only
+//     (:1180-1195; the in-edge adjustment is commented out at :1135-1142);
+//  3. the new terms of rows and columns for i not in {r, s} (:1196-1215),
+//     the entries adjusted by v's out-weight (rows) and in-weight (columns)
+//     towards block i, looked up in the group's neighbour-block table.
+// Each lane evaluates the (up to four) terms of one block i of a chunk of
+// G blocks; the terms are then added to one float accumulator in the
+// reference's order, lane after lane (float addition does not
+// reassociate), skipping lanes whose terms are all zero.  Every lane
+// returns the same value.  Rr, Rs, Sr, Ss: M[r,r], M[r,s], M[s,r], M[s,s];
+// wor, wos: v's out-weight to blocks r and s.
+template <class Ops, int G>
+__device__ __forceinline__ float ref32_nodal(const NodalArgs& a, const Ops& ops, const Grp<G>& g, int r, int s,
+                                          long long dr_out, long long dr_in, long long ds_out, long long ds_in,
+                                          long long kout, long long kin, long long Rr, long long Rs,
+                                          long long Sr, long long Ss, long long wor, long long wos,
+                                          const int* key, const int* two, const int* twi, int cap, int lg) {
+  using LDT = typename Ops::LdT;
+  const int B = a.B;
+  float dS = 0.0f;
+  for (int base = 0; base < B; base += G) {
+    const int i = base + g.gl;
+    float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
+    if (i < B) {
+      const long long R = ops.get(r, i), S = ops.get(s, i);
+      const long long di = LDT::ld(a.din + i);
+      if (R) t0 = ref_term(R, di * dr_out);
+      if (S) t1 = ref_term(S, di * ds_out);
+      if (i != r && i != s) {
+        const long long Rc = ops.get_t(r, i), Sc = ops.get_t(s, i);
+        const long long dn = LDT::ld(a.dout + i);
+        if (Rc) t2 = ref_term(Rc, dn * dr_in);
+        if (Sc) t3 = ref_term(Sc, dn * ds_in);
+      }
+    }
+    unsigned m = g.ballot(t0 != 0.0f || t1 != 0.0f || t2 != 0.0f || t3 != 0.0f);
+    while (m) {
+      const int j = __ffs(m) - 1;
+      m &= m - 1;
+      const float a0 = g.shfl(t0, j), a1 = g.shfl(t1, j), a2 = g.shfl(t2, j), a3 = g.shfl(t3, j);
+      dS = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(dS, a0), a1), a2), a3);
+    }
+  }
+  const long long dor_n = dr_out - kout, dos_n = ds_out + kout;
+  const long long dir_n = dr_in - kin, dis_n = ds_in + kin;
+  const long long rr_r = Rr - wor, rr_s = Rs - wos, sr_r = Sr + wor, sr_s = Ss + wos;
+  if (rr_r) dS = __fsub_rn(dS, ref_term(rr_r, dir_n * dor_n));
+  if (rr_s) dS = __fsub_rn(dS, ref_term(rr_s, dis_n * dor_n));
+  if (sr_r) dS = __fsub_rn(dS, ref_term(sr_r, dir_n * dos_n));
+  if (sr_s) dS = __fsub_rn(dS, ref_term(sr_s, dis_n * dos_n));
+  for (int base = 0; base < B; base += G) {
+    const int i = base + g.gl;
+    float u0 = 0.0f, u1 = 0.0f, u2 = 0.0f, u3 = 0.0f;
+    if (i < B && i != r && i != s) {
+      long long R = ops.get(r, i), S = ops.get(s, i), Rc = ops.get_t(r, i), Sc = ops.get_t(s, i);
+      // v's edges towards block i are part of M[r,i] (out) and M[i,r] (in)
+      if (R > 0) {
+        const long long w = table_lookup_wo(key, two, cap, lg, i);
+        R -= w;
+        S += w;
+      }
+      if (Rc > 0) {
+        const long long w = table_lookup_wo(key, twi, cap, lg, i);
+        Rc -= w;
+        Sc += w;
+      }
+      const long long di = LDT::ld(a.din + i), dn = LDT::ld(a.dout + i);
+      if (R) u0 = ref_term(R, di * dor_n);
+      if (S) u1 = ref_term(S, di * dos_n);
+      if (Rc) u2 = ref_term(Rc, dn * dir_n);
+      if (Sc) u3 = ref_term(Sc, dn * dis_n);
+    }
+    unsigned m = g.ballot(u0 != 0.0f || u1 != 0.0f || u2 != 0.0f || u3 != 0.0f);
+    while (m) {
+      const int j = __ffs(m) - 1;
+      m &= m - 1;
+      const float a0 = g.shfl(u0, j), a1 = g.shfl(u1, j), a2 = g.shfl(u2, j), a3 = g.shfl(u3, j);
+      dS = __fsub_rn(__fsub_rn(__fsub_rn(__fsub_rn(dS, a0), a1), a2), a3);
+    }
+  }
+  return dS;
 }
 
 // per-vertex outputs of a decided proposal; returns whether it is accepted
@@ -492,7 +585,7 @@ __device__ __forceinline__ void record_stay(const NodalArgs& a, int v, int r) {
 // accepted dS, moves and near-threshold proposals of one CTA, added to the
 // control block once at the end of the kernel
 // (the accepted dS summed for the convergence test is the exact FP64 value
-// in both precision modes)
+// in precision modes 1 and 2, the reference's float value in mode 3)
 struct CtaTally {
   unsigned long long cum, moves, near;
   int ninf;
@@ -506,11 +599,20 @@ struct CtaTally {
   int own_cap, own_tag;
 };
 
+// the accepted dS that the convergence test sums: the exact value, or in
+// precision mode 3 the reference's float value (its update task sums the
+// float dS it accepted, graph_parallel.hpp:428-434), in Q32
+template <int P>
+__device__ __forceinline__ long long summed_dq(long long acc, double f) {
+  if constexpr (P == 3) return q32(f);
+  return acc;
+}
+
 template <int P>
 __device__ __forceinline__ void tally(CtaTally* t, bool accept, long long acc, double f, int ninf) {
   if (accept) {
     if (ninf) atomicOr(&t->ninf, 1);
-    else atomicAdd(&t->cum, static_cast<unsigned long long>(acc));
+    else atomicAdd(&t->cum, static_cast<unsigned long long>(summed_dq<P>(acc, f)));
     atomicAdd(&t->moves, 1ull);
   }
   if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&t->near, 1ull);
@@ -524,7 +626,7 @@ template <int P>
 __device__ __forceinline__ void tally_ctl(NodalCtl* c, bool accept, long long acc, double f, int ninf) {
   if (accept) {
     if (ninf) atomicOr(&c->cum_ninf, 1);
-    else atomicAdd(&c->cum_q, static_cast<unsigned long long>(acc));
+    else atomicAdd(&c->cum_q, static_cast<unsigned long long>(summed_dq<P>(acc, f)));
     atomicAdd(&c->moves, 1ull);
   }
   if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&c->near, 1ull);
@@ -691,6 +793,9 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
   double f = 0.0;
   const long long acc = finalize_grp<G, Ops::kP>(a, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out,
                                                  ds_in, vi.kout, vi.kin, &ninf, ts.f, &f);
+  if constexpr (Ops::kP == 3)
+    f = ref32_nodal<Ops, G>(a, ops, g, r, s, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin, Rr, Rs, Sr, Ss, wor,
+                            wos, key, two, twi, cap, lg);
   if (g.gl == 0) {
     const bool moved = emit<Ops::kP>(a, v, r, s, acc, f, ninf);
     tally<Ops::kP>(tl, moved, acc, f, ninf);
@@ -847,7 +952,7 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
   ts.sYR = warp_sum_i(ts.sYR);
   ts.sYS = warp_sum_i(ts.sYS);
   nocc = warp_sum_i(nocc);
-  if constexpr (Ops::kP > 0) ts.f = Grp<32>(lane).ffsum(ts.f);
+  if constexpr (kPairTerms<Ops::kP>) ts.f = Grp<32>(lane).ffsum(ts.f);
   if (lane == 0) {
     sh->acc[wib] = ts.acc;
     sh->fhi[wib] = ts.f.hi;
@@ -888,6 +993,9 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
     double f = 0.0;
     const long long acc = finalize_grp<32, Ops::kP>(a, Grp<32>(lane), tot, Rr, Rs, Sr, Ss, wor, wos, dr_out,
                                                     dr_in, ds_out, ds_in, vi.kout, vi.kin, &ninf, fpart, &f);
+    if constexpr (Ops::kP == 3)
+      f = ref32_nodal<Ops, 32>(a, ops, Grp<32>(lane), r, s, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin, Rr, Rs,
+                               Sr, Ss, wor, wos, key, two, twi, cap, lg);
     if (lane == 0) {
       tally_ctl<Ops::kP>(a.ctl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
       if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * occ + 48 + 8ull * sh->scanned;
@@ -2099,6 +2207,7 @@ void nodal_configure(int device) {
     configure(std::integral_constant<int, 0>{});
     configure(std::integral_constant<int, 1>{});
     configure(std::integral_constant<int, 2>{});
+    configure(std::integral_constant<int, 3>{});
     g_phase_grid[device] = coop ? per_phase * sms : 0;
     g_gang_grid[device] = coop ? per_gang * sms : 0;
   });
@@ -2119,10 +2228,11 @@ int nodal_gang_grid(int device) {
 // the apply pass keys a tile cell as x * ld + y in 31 bits
 int nodal_phase_max_blocks() { return 32768; }
 
-// the cooperative kernels of precision mode `prec` (0, 1, 2)
+// the cooperative kernels of precision mode `prec` (0, 1, 2, 3)
 static const void* gang_kernel(int prec) {
   if (prec == 1) return reinterpret_cast<const void*>(k_nodal_gang<1>);
   if (prec == 2) return reinterpret_cast<const void*>(k_nodal_gang<2>);
+  if (prec == 3) return reinterpret_cast<const void*>(k_nodal_gang<3>);
   return reinterpret_cast<const void*>(k_nodal_gang<0>);
 }
 
@@ -2131,10 +2241,12 @@ static const void* phase_kernel(int prec, bool snap) {
   if (snap) {
     if (prec == 1) return reinterpret_cast<const void*>(k_nodal_phase<1, true>);
     if (prec == 2) return reinterpret_cast<const void*>(k_nodal_phase<2, true>);
+    if (prec == 3) return reinterpret_cast<const void*>(k_nodal_phase<3, true>);
     return reinterpret_cast<const void*>(k_nodal_phase<0, true>);
   }
   if (prec == 1) return reinterpret_cast<const void*>(k_nodal_phase<1, false>);
   if (prec == 2) return reinterpret_cast<const void*>(k_nodal_phase<2, false>);
+  if (prec == 3) return reinterpret_cast<const void*>(k_nodal_phase<3, false>);
   return reinterpret_cast<const void*>(k_nodal_phase<0, false>);
 }
 
@@ -2162,6 +2274,7 @@ void launch_nodal_propose_dense(const NodalArgs& a, DenseView v, const HubList& 
                                 const StreamPair& sp) {
   if (a.prec == 1) launch_propose(a, DenseOpsT<LdNC, 1>{v, a.B}, hubs, sp);
   else if (a.prec == 2) launch_propose(a, DenseOpsT<LdNC, 2>{v, a.B}, hubs, sp);
+  else if (a.prec == 3) launch_propose(a, DenseOpsT<LdNC, 3>{v, a.B}, hubs, sp);
   else launch_propose(a, DenseOps{v, a.B}, hubs, sp);
 }
 
@@ -2169,6 +2282,7 @@ void launch_nodal_propose_sorted(const NodalArgs& a, SortedView v, const HubList
                                  const StreamPair& sp) {
   if (a.prec == 1) launch_propose(a, SortedOpsT<1>{v, a.B}, hubs, sp);
   else if (a.prec == 2) launch_propose(a, SortedOpsT<2>{v, a.B}, hubs, sp);
+  else if (a.prec == 3) launch_propose(a, SortedOpsT<3>{v, a.B}, hubs, sp);
   else launch_propose(a, SortedOps{v, a.B}, hubs, sp);
 }
 

@@ -597,13 +597,19 @@ int64_t og_nodal_dq(const og_graph* g, const int32_t* part, const og_blocks* b,
  * blocks on the N=50000 workload.  Mode 3 evaluates exactly that
  * expression, term order included.                                         */
 
-/* log(x) for a float x, rounded to float.  Evaluated in double: x = m * 2^e
- * with m in [sqrt(1/2), sqrt(2)], log x = e * ln 2 + 2 atanh(z) with
- * z = (m - 1) / (m + 1) and atanh z = z + z^3/3 + z^5/5 + ... (the
- * classical series for log((1 + z) / (1 - z)); |z| <= 0.1716, 13 terms,
- * truncation below 1e-19 relative).  Only IEEE double +, -, *, / are used,
- * without contraction, so the CUDA kernels' copy of these steps returns the
- * same bits.  x = 0 gives -inf, x = +inf gives +inf. */
+/* log(x) for a float x, rounded to float.  Evaluated in double with IEEE
+ * +, -, * and fma only, in the same steps as the CUDA kernels' ref_logf, so
+ * both return the same bits: x = m * 2^e with m in [sqrt(1/2), sqrt(2));
+ * k = 128 (m - 1) rounded half up picks r_k = round(1024 / (1 + k/128)) / 1024 and
+ * L_k = -log(r_k) (usap_b200/csrc/ref_log_table.inc, written by
+ * ref_log_table.py with 50-digit logs); u = m r_k - 1 is exact (|u| <
+ * 0.0066), and log x = e ln 2 + L_k + log1p(u), log1p(u) by its series
+ * u - u^2/2 + ... - u^8/8.  x = 0 gives -inf, x = +inf gives +inf.        */
+static const double og_ref_log_tab[][2] = {
+#include "../usap_b200/csrc/ref_log_table.inc"
+};
+#define OG_REF_LOG_K0 38
+
 float og_log_f32(float x) {
   if (isnan(x) || x < 0.0f) return NAN;
   if (x == 0.0f) return -INFINITY;
@@ -611,34 +617,37 @@ float og_log_f32(float x) {
   uint32_t u;
   memcpy(&u, &x, sizeof(u));
   int e = (int)((u >> 23) & 0xffu);
-  const uint32_t frac = u & 0x7fffffu;
-  double m;
-  if (e == 0) {                      /* subnormal */
-    m = (double)frac * 0x1p-23;
-    e = -126;
-    while (m < 1.0) { m = m * 2.0; e -= 1; }
-  } else {
-    m = 1.0 + (double)frac * 0x1p-23;
-    e -= 127;
+  uint32_t frac = u & 0x7fffffu;
+  if (e == 0) {                      /* subnormal: leading one into the hidden bit */
+    int sh = 0;
+    while (!(frac & 0x800000u)) { frac <<= 1; sh++; }
+    frac &= 0x7fffffu;
+    e = 1 - sh;
   }
-  if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
-  const double z = (m - 1.0) / (m + 1.0);
-  const double z2 = z * z;
-  double p = 1.0 / 25.0;
-  p = p * z2 + 1.0 / 23.0;
-  p = p * z2 + 1.0 / 21.0;
-  p = p * z2 + 1.0 / 19.0;
-  p = p * z2 + 1.0 / 17.0;
-  p = p * z2 + 1.0 / 15.0;
-  p = p * z2 + 1.0 / 13.0;
-  p = p * z2 + 1.0 / 11.0;
-  p = p * z2 + 1.0 / 9.0;
-  p = p * z2 + 1.0 / 7.0;
-  p = p * z2 + 1.0 / 5.0;
-  p = p * z2 + 1.0 / 3.0;
-  p = p * z2 + 1.0;
-  const double lm = (2.0 * z) * p;
-  return (float)((double)e * 0.69314718055994530942 + lm);
+  e -= 127;
+  /* m = 1 + frac / 2^23, halved above sqrt(2) (frac >= 0x3504F4); k =
+   * 128 (m - 1) rounded half up, from the bits */
+  double m = 1.0 + (double)frac * 0x1p-23;
+  int k;
+  if (frac >= 0x3504F4u) {
+    m = m * 0.5;
+    e += 1;
+    k = (int)((frac + 0x10000u) >> 17) - 64;
+  } else {
+    k = (int)((frac + 0x8000u) >> 16);
+  }
+  const double* t = og_ref_log_tab[OG_REF_LOG_K0 + k];
+  const double w = m * t[0] - 1.0;
+  double q = -1.0 / 8.0;
+  q = fma(q, w, 1.0 / 7.0);
+  q = fma(q, w, -1.0 / 6.0);
+  q = fma(q, w, 1.0 / 5.0);
+  q = fma(q, w, -1.0 / 4.0);
+  q = fma(q, w, 1.0 / 3.0);
+  q = fma(q, w, -1.0 / 2.0);
+  const double l1p = fma(w * w, q, w);
+  const double hi = fma((double)e, 0.69314718055994530942, t[1]);
+  return (float)(hi + l1p);
 }
 
 /* count * log((float)count / (float)prod), as the reference rounds it */

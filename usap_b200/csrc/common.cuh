@@ -201,57 +201,66 @@ __device__ __forceinline__ FF h_term_ff(const float2* __restrict__ T, long long 
 template <int P>
 constexpr bool kPairTerms = (P == 1 || P == 2);
 
-// log(x) rounded to float.  x = m * 2^e with m in [sqrt(1/2), sqrt(2)];
-// log x = e * ln 2 + 2 atanh(z), z = (m - 1) / (m + 1), atanh by its series
-// z + z^3/3 + z^5/5 + ... (13 terms; |z| <= 0.1716).  IEEE double +, -, *, /
-// only, in the same order as the oracle's og_log_f32, so host and device
-// agree bit for bit; the result is log x correctly rounded to float except
-// when log x lies within ~1e-16 relative of a rounding boundary.
+// log(x) rounded to float, evaluated in double with IEEE +, -, * and fused
+// multiply-add only, in the same steps as the oracle's og_log_f32, so host
+// and device agree bit for bit.  x = m * 2^e with m in [sqrt(1/2), sqrt(2));
+// k = 128 (m - 1) rounded half up picks r_k = round(1024 / (1 + k/128)) / 1024 and
+// L_k = -log(r_k) from ref_log_table.inc (written by ref_log_table.py);
+// u = m r_k - 1 is exact (|u| < 0.0066) and
+//   log x = e ln 2 + L_k + log1p(u),  log1p(u) = u - u^2/2 + ... - u^8/8
+// (the next term is below 3e-21).  The double result is within a few units
+// of 1e-16 of log x, so it rounds to the correctly rounded float except
+// when log x lies that close to a rounding boundary.
+static __device__ const double2 kRefLogTab[] = {
+#include "ref_log_table.inc"
+};
+constexpr int kRefLogK0 = 38;   // table index of k = 0
+
 __device__ __forceinline__ float ref_logf(float x) {
   if (!(x > 0.0f)) return x == 0.0f ? __int_as_float(0xff800000) : __int_as_float(0x7fc00000);
   const unsigned u = __float_as_uint(x);
   if (u >= 0x7f800000u) return x;   // +inf
-  int e = static_cast<int>((u >> 23) & 0xffu);
-  const unsigned frac = u & 0x7fffffu;
-  double m;
-  if (e == 0) {
-    m = __dmul_rn(static_cast<double>(frac), 0x1p-23);
-    e = -126;
-    while (m < 1.0) {
-      m = __dmul_rn(m, 2.0);
-      e -= 1;
-    }
-  } else {
-    m = __dadd_rn(1.0, __dmul_rn(static_cast<double>(frac), 0x1p-23));
-    e -= 127;
+  int e = static_cast<int>(u >> 23);
+  unsigned frac = u & 0x7fffffu;
+  if (e == 0) {   // subnormal: shift the leading one into the hidden bit
+    const int sh = __clz(static_cast<int>(frac)) - 8;
+    frac = (frac << sh) & 0x7fffffu;
+    e = 1 - sh;
   }
-  if (m > 1.4142135623730951) {
-    m = __dmul_rn(m, 0.5);
+  e -= 127;
+  // m = 1 + frac / 2^23, halved above sqrt(2) (frac >= 0x3504F4); k from the
+  // bits: round(frac / 2^16), or round(frac / 2^17) - 64 after halving
+  unsigned long long mbits;
+  int k;
+  if (frac >= 0x3504F4u) {
     e += 1;
+    mbits = (1022ull << 52) | (static_cast<unsigned long long>(frac) << 29);
+    k = static_cast<int>((frac + 0x10000u) >> 17) - 64;
+  } else {
+    mbits = (1023ull << 52) | (static_cast<unsigned long long>(frac) << 29);
+    k = static_cast<int>((frac + 0x8000u) >> 16);
   }
-  const double z = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
-  const double z2 = __dmul_rn(z, z);
-  double p = 1.0 / 25.0;
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 23.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 21.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 19.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 17.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 15.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 13.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 11.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 9.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 7.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 5.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0 / 3.0);
-  p = __dadd_rn(__dmul_rn(p, z2), 1.0);
-  const double lm = __dmul_rn(__dmul_rn(2.0, z), p);
-  return __double2float_rn(__dadd_rn(__dmul_rn(static_cast<double>(e), 0.69314718055994530942), lm));
+  const double m = __longlong_as_double(static_cast<long long>(mbits));
+  const double2 t = __ldg(kRefLogTab + kRefLogK0 + k);
+  const double w = __dsub_rn(__dmul_rn(m, t.x), 1.0);
+  double q = -1.0 / 8.0;
+  q = __fma_rn(q, w, 1.0 / 7.0);
+  q = __fma_rn(q, w, -1.0 / 6.0);
+  q = __fma_rn(q, w, 1.0 / 5.0);
+  q = __fma_rn(q, w, -1.0 / 4.0);
+  q = __fma_rn(q, w, 1.0 / 3.0);
+  q = __fma_rn(q, w, -1.0 / 2.0);
+  const double l1p = __fma_rn(__dmul_rn(w, w), q, w);
+  // e as a double without a conversion instruction: 2^52 + 2^51 + e, minus the offset
+  const double ed = __dsub_rn(__longlong_as_double(0x4338000000000000ll + e), 6755399441055744.0);
+  const double hi = __fma_rn(ed, 0.69314718055994530942, t.y);
+  return __double2float_rn(__dadd_rn(hi, l1p));
 }
 
 // one term of the reference's dS: count * log((float)count / (float)prod),
 // the long product converted to float, a float division, a float product
-__device__ __forceinline__ float ref_term(long long x, long long prod) {
-  const float xf = __ll2float_rn(x);
+__device__ __forceinline__ float ref_term(int x, long long prod) {
+  const float xf = __int2float_rn(x);
   return __fmul_rn(xf, ref_logf(__fdiv_rn(xf, __ll2float_rn(prod))));
 }
 

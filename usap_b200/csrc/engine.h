@@ -216,8 +216,14 @@ struct NodalArgs {
   const int64_t* hi_off;
   int32_t *hkey, *hwo, *hwi;
   int stats;
-  int prec;               // precision mode: 0 FP64; 1, 2 decide on the FP32 dS
+  int prec;               // precision mode: 0 FP64; 1, 2 decide on the FP32 dS; 3 the reference's float dS
   const float2* L2;       // the log table as float pairs (precision modes 1, 2)
+  // precision mode 3, persistent kernel: the reference's old-state terms of
+  // every tile cell, recomputed at each batch start (null: computed per
+  // proposal); row b, column i at b * tld + i
+  float* Trow;            // M[b,i] log(M[b,i] / (d_in[i] d_out[b]))
+  float* Tcol;            // M[i,b] log(M[i,b] / (d_out[i] d_in[b]))
+  int tld;
 };
 
 struct MergeArgs {

@@ -197,6 +197,8 @@ void Job::free_state() {
   batch_hub_cap_ = 0;
   units_cap_ = 0;
   dfree(M_); dfree(Mt_); dfree(CS_);
+  dfree(Trow_); dfree(Tcol_);
+  tcap_ = 0;
   sb_.release(st_);
   dfree(prop_s_); dfree(prop_q_); dfree(prop_x_); dfree(prop_f_); dfree(best_s_); dfree(best_q_); dfree(best_x_);
   dfree(skeys_); dfree(skeys_alt_); dfree(sidx_); dfree(sidx_alt_);
@@ -629,6 +631,9 @@ NodalArgs Job::nodal_args(int32_t* part, int32_t B, int32_t beg, int32_t end, ui
   a.stats = stats;
   a.prec = prec_;
   a.L2 = g_.logk2;
+  a.Trow = nullptr;
+  a.Tcol = nullptr;
+  a.tld = 0;
   if (stats == 2) {   // replay: per-vertex proposals
     a.prop_s = rp_s_;
     a.prop_q = rp_q_;
@@ -755,6 +760,22 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
   pa.model_d = model_d;
   pa.ide_q = ide_q_;
   pa.ide_n = ide_n_;
+  // precision mode 3: the old-state term tables of the single-job kernel
+  // (B <= kRefTabMaxB; above it the per-cell tables cost more than the
+  // proposals' own evaluation)
+  if (prec_ == 3 && !(gang_ && !timed) && B <= kRefTabMaxB) {
+    const size_t cells = static_cast<size_t>(ld_) * ld_;
+    if (cells > tcap_) {
+      dfree(Trow_);
+      dfree(Tcol_);
+      dalloc(&Trow_, cells);
+      dalloc(&Tcol_, cells);
+      tcap_ = cells;
+    }
+    pa.a.Trow = Trow_;
+    pa.a.Tcol = Tcol_;
+    pa.a.tld = ld_;
+  }
   if (gang_ && !timed) {
     gang_->run(pa, st_);
     USAP_CUDA(cudaMemcpyAsync(h_ctl_, ctl_, sizeof(NodalCtl), cudaMemcpyDeviceToHost, st_));

@@ -289,6 +289,10 @@ class Job {
   int32_t batch_hub_cap_ = 0;
   int32_t *dout_ = nullptr, *din_ = nullptr;
   int *M_ = nullptr, *Mt_ = nullptr, *CS_ = nullptr;
+  // precision mode 3: old-state term tables of the persistent kernel (ld_ x ld_ floats each)
+  static constexpr int32_t kRefTabMaxB = 4096;
+  float *Trow_ = nullptr, *Tcol_ = nullptr;
+  size_t tcap_ = 0;
   int ld_ = 0, cld_ = 0;
   SortedBuilder sb_;
   int32_t* prop_s_ = nullptr;

@@ -476,79 +476,168 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
 //  3. the new terms of rows and columns for i not in {r, s} (:1196-1215),
 //     the entries adjusted by v's out-weight (rows) and in-weight (columns)
 //     towards block i, looked up in the group's neighbour-block table.
-// Each lane evaluates the (up to four) terms of one block i of a chunk of
-// G blocks; the terms are then added to one float accumulator in the
-// reference's order, lane after lane (float addition does not
-// reassociate), skipping lanes whose terms are all zero.  Every lane
-// returns the same value.  Rr, Rs, Sr, Ss: M[r,r], M[r,s], M[s,r], M[s,s];
-// wor, wos: v's out-weight to blocks r and s.
-template <class Ops, int G>
-__device__ __forceinline__ float ref32_nodal(const NodalArgs& a, const Ops& ops, const Grp<G>& g, int r, int s,
-                                          long long dr_out, long long dr_in, long long ds_out, long long ds_in,
-                                          long long kout, long long kin, long long Rr, long long Rs,
-                                          long long Sr, long long Ss, long long wor, long long wos,
-                                          const int* key, const int* two, const int* twi, int cap, int lg) {
-  using LDT = typename Ops::LdT;
-  const int B = a.B;
-  float dS = 0.0f;
-  for (int base = 0; base < B; base += G) {
-    const int i = base + g.gl;
-    float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f, t3 = 0.0f;
-    if (i < B) {
-      const long long R = ops.get(r, i), S = ops.get(s, i);
-      const long long di = LDT::ld(a.din + i);
-      if (R) t0 = ref_term(R, di * dr_out);
-      if (S) t1 = ref_term(S, di * ds_out);
-      if (i != r && i != s) {
-        const long long Rc = ops.get_t(r, i), Sc = ops.get_t(s, i);
-        const long long dn = LDT::ld(a.dout + i);
-        if (Rc) t2 = ref_term(Rc, dn * dr_in);
-        if (Sc) t3 = ref_term(Sc, dn * ds_in);
-      }
-    }
-    unsigned m = g.ballot(t0 != 0.0f || t1 != 0.0f || t2 != 0.0f || t3 != 0.0f);
-    while (m) {
-      const int j = __ffs(m) - 1;
-      m &= m - 1;
+// A round covers kRefK * G blocks: lane l loads the entries of blocks
+// base + k G + l (k < kRefK) of the four rows at once, so one round trip
+// serves 4 kRefK loads per lane.  For each k the lanes evaluate the terms
+// of their block, and the terms are then added to one float accumulator in
+// the reference's order -- lane after lane, and within a lane in the
+// reference's term order (float addition does not reassociate).  Zero
+// terms are skipped with branches that are uniform over the group (adding
+// a zero would not change the sum), so the serial chain is as long as the
+// number of non-zero terms.  Every lane returns the same value.  Rr, Rs,
+// Sr, Ss: M[r,r], M[r,s], M[s,r], M[s,s]; wor, wos: v's out-weight to
+// blocks r and s.
+constexpr int kRefK = 4;
+
+template <int G>
+__device__ __forceinline__ float ref32_accumulate(const Grp<G>& g, float dS, float t0, float t1, float t2,
+                                                  float t3, bool sub) {
+  const int nz = (t0 != 0.0f ? 1 : 0) | (t1 != 0.0f ? 2 : 0) | (t2 != 0.0f ? 4 : 0) | (t3 != 0.0f ? 8 : 0);
+  unsigned m = g.ballot(nz != 0);
+  constexpr unsigned kAll = G == 32 ? 0xffffffffu : (1u << G) - 1u;
+  if (m == kAll) {
+    // every lane has a term: a straight chain (adding a zero term changes
+    // nothing), so the shuffles can be issued ahead of the additions
+#pragma unroll
+    for (int j = 0; j < G; j++) {
       const float a0 = g.shfl(t0, j), a1 = g.shfl(t1, j), a2 = g.shfl(t2, j), a3 = g.shfl(t3, j);
-      dS = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(dS, a0), a1), a2), a3);
+      if (sub) dS = __fsub_rn(__fsub_rn(__fsub_rn(__fsub_rn(dS, a0), a1), a2), a3);
+      else dS = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(dS, a0), a1), a2), a3);
+    }
+    return dS;
+  }
+  while (m) {
+    const int j = __ffs(m) - 1;
+    m &= m - 1;
+    const int nzj = g.shfl(nz, j);
+    const float a0 = g.shfl(t0, j), a1 = g.shfl(t1, j), a2 = g.shfl(t2, j), a3 = g.shfl(t3, j);
+    if (sub) {
+      if (nzj & 1) dS = __fsub_rn(dS, a0);
+      if (nzj & 2) dS = __fsub_rn(dS, a1);
+      if (nzj & 4) dS = __fsub_rn(dS, a2);
+      if (nzj & 8) dS = __fsub_rn(dS, a3);
+    } else {
+      if (nzj & 1) dS = __fadd_rn(dS, a0);
+      if (nzj & 2) dS = __fadd_rn(dS, a1);
+      if (nzj & 4) dS = __fadd_rn(dS, a2);
+      if (nzj & 8) dS = __fadd_rn(dS, a3);
     }
   }
-  const long long dor_n = dr_out - kout, dos_n = ds_out + kout;
-  const long long dir_n = dr_in - kin, dis_n = ds_in + kin;
-  const long long rr_r = Rr - wor, rr_s = Rs - wos, sr_r = Sr + wor, sr_s = Ss + wos;
-  if (rr_r) dS = __fsub_rn(dS, ref_term(rr_r, dir_n * dor_n));
-  if (rr_s) dS = __fsub_rn(dS, ref_term(rr_s, dis_n * dor_n));
-  if (sr_r) dS = __fsub_rn(dS, ref_term(sr_r, dir_n * dos_n));
-  if (sr_s) dS = __fsub_rn(dS, ref_term(sr_s, dis_n * dos_n));
-  for (int base = 0; base < B; base += G) {
-    const int i = base + g.gl;
-    float u0 = 0.0f, u1 = 0.0f, u2 = 0.0f, u3 = 0.0f;
-    if (i < B && i != r && i != s) {
-      long long R = ops.get(r, i), S = ops.get(s, i), Rc = ops.get_t(r, i), Sc = ops.get_t(s, i);
-      // v's edges towards block i are part of M[r,i] (out) and M[i,r] (in)
-      if (R > 0) {
-        const long long w = table_lookup_wo(key, two, cap, lg, i);
-        R -= w;
-        S += w;
+  return dS;
+}
+
+// (not inlined: it runs after the group's other work is done, and a call
+// gives it the registers the proposal code held)
+template <class Ops, int G>
+__device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restrict__ din_p,
+                                          const int32_t* __restrict__ dout_p, const float* Trow,
+                                          const float* Tcol, int tld, int r, int s, int dr_out, int dr_in,
+                                          int ds_out, int ds_in, int kout, int kin, int Rr, int Rs, int Sr, int Ss,
+                                          int wor, int wos, const int* key, const int* two, const int* twi, int cap,
+                                          int lg) {
+  using LDT = typename Ops::LdT;
+  const Grp<G> g(static_cast<int>(threadIdx.x & 31));
+  const int B = ops.B;
+  float dS = 0.0f;
+  if (Trow) {
+    // the old-state terms from the batch's tables (written in this launch: L2 loads)
+    const float* tr = Trow + static_cast<long long>(r) * tld;
+    const float* ts = Trow + static_cast<long long>(s) * tld;
+    const float* cr = Tcol + static_cast<long long>(r) * tld;
+    const float* cs = Tcol + static_cast<long long>(s) * tld;
+    for (int base = 0; base < B; base += kRefK * G) {
+      float t[kRefK][4];
+#pragma unroll
+      for (int k = 0; k < kRefK; k++) {
+        const int i = base + k * G + g.gl;
+        const bool in = i < B, col = in && i != r && i != s;
+        t[k][0] = in ? __ldcg(tr + i) : 0.0f;
+        t[k][1] = in ? __ldcg(ts + i) : 0.0f;
+        t[k][2] = col ? __ldcg(cr + i) : 0.0f;
+        t[k][3] = col ? __ldcg(cs + i) : 0.0f;
       }
-      if (Rc > 0) {
-        const long long w = table_lookup_wo(key, twi, cap, lg, i);
-        Rc -= w;
-        Sc += w;
-      }
-      const long long di = LDT::ld(a.din + i), dn = LDT::ld(a.dout + i);
-      if (R) u0 = ref_term(R, di * dor_n);
-      if (S) u1 = ref_term(S, di * dos_n);
-      if (Rc) u2 = ref_term(Rc, dn * dir_n);
-      if (Sc) u3 = ref_term(Sc, dn * dis_n);
+#pragma unroll
+      for (int k = 0; k < kRefK; k++) dS = ref32_accumulate<G>(g, dS, t[k][0], t[k][1], t[k][2], t[k][3], false);
     }
-    unsigned m = g.ballot(u0 != 0.0f || u1 != 0.0f || u2 != 0.0f || u3 != 0.0f);
-    while (m) {
-      const int j = __ffs(m) - 1;
-      m &= m - 1;
-      const float a0 = g.shfl(u0, j), a1 = g.shfl(u1, j), a2 = g.shfl(u2, j), a3 = g.shfl(u3, j);
-      dS = __fsub_rn(__fsub_rn(__fsub_rn(__fsub_rn(dS, a0), a1), a2), a3);
+  }
+  for (int base = 0; !Trow && base < B; base += kRefK * G) {
+    int R[kRefK], S[kRefK], Rc[kRefK], Sc[kRefK];
+#pragma unroll
+    for (int k = 0; k < kRefK; k++) {
+      const int i = base + k * G + g.gl;
+      R[k] = S[k] = Rc[k] = Sc[k] = 0;
+      if (i < B) {
+        R[k] = ops.get(r, i);
+        S[k] = ops.get(s, i);
+        if (i != r && i != s) {   // columns skip i in {r, s}
+          Rc[k] = ops.get_t(r, i);
+          Sc[k] = ops.get_t(s, i);
+        }
+      }
+    }
+    int di[kRefK], dn[kRefK];
+#pragma unroll
+    for (int k = 0; k < kRefK; k++) {
+      const int i = base + k * G + g.gl;
+      di[k] = (R[k] | S[k]) ? LDT::ld(din_p + i) : 0;
+      dn[k] = (Rc[k] | Sc[k]) ? LDT::ld(dout_p + i) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kRefK; k++) {
+      if (!g.any((R[k] | S[k] | Rc[k] | Sc[k]) != 0)) continue;
+      const float t0 = R[k] ? ref_term(R[k], static_cast<long long>(di[k]) * dr_out) : 0.0f;
+      const float t1 = S[k] ? ref_term(S[k], static_cast<long long>(di[k]) * ds_out) : 0.0f;
+      const float t2 = Rc[k] ? ref_term(Rc[k], static_cast<long long>(dn[k]) * dr_in) : 0.0f;
+      const float t3 = Sc[k] ? ref_term(Sc[k], static_cast<long long>(dn[k]) * ds_in) : 0.0f;
+      dS = ref32_accumulate<G>(g, dS, t0, t1, t2, t3, false);
+    }
+  }
+  const int dor_n = dr_out - kout, dos_n = ds_out + kout;
+  const int dir_n = dr_in - kin, dis_n = ds_in + kin;
+  const int rr_r = Rr - wor, rr_s = Rs - wos, sr_r = Sr + wor, sr_s = Ss + wos;
+  if (rr_r) dS = __fsub_rn(dS, ref_term(rr_r, static_cast<long long>(dir_n) * dor_n));
+  if (rr_s) dS = __fsub_rn(dS, ref_term(rr_s, static_cast<long long>(dis_n) * dor_n));
+  if (sr_r) dS = __fsub_rn(dS, ref_term(sr_r, static_cast<long long>(dir_n) * dos_n));
+  if (sr_s) dS = __fsub_rn(dS, ref_term(sr_s, static_cast<long long>(dis_n) * dos_n));
+  for (int base = 0; base < B; base += kRefK * G) {
+    int R[kRefK], S[kRefK], Rc[kRefK], Sc[kRefK];
+#pragma unroll
+    for (int k = 0; k < kRefK; k++) {
+      const int i = base + k * G + g.gl;
+      R[k] = S[k] = Rc[k] = Sc[k] = 0;
+      if (i < B && i != r && i != s) {
+        R[k] = ops.get(r, i);
+        S[k] = ops.get(s, i);
+        Rc[k] = ops.get_t(r, i);
+        Sc[k] = ops.get_t(s, i);
+      }
+    }
+    int di[kRefK], dn[kRefK];
+#pragma unroll
+    for (int k = 0; k < kRefK; k++) {
+      const int i = base + k * G + g.gl;
+      // v's edges towards block i are part of M[r,i] (out) and M[i,r] (in)
+      if (R[k] > 0) {
+        const int w = table_lookup_wo(key, two, cap, lg, i);
+        R[k] -= w;
+        S[k] += w;
+      }
+      if (Rc[k] > 0) {
+        const int w = table_lookup_wo(key, twi, cap, lg, i);
+        Rc[k] -= w;
+        Sc[k] += w;
+      }
+      di[k] = (R[k] | S[k]) ? LDT::ld(din_p + i) : 0;
+      dn[k] = (Rc[k] | Sc[k]) ? LDT::ld(dout_p + i) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kRefK; k++) {
+      if (!g.any((R[k] | S[k] | Rc[k] | Sc[k]) != 0)) continue;
+      const float u0 = R[k] ? ref_term(R[k], static_cast<long long>(di[k]) * dor_n) : 0.0f;
+      const float u1 = S[k] ? ref_term(S[k], static_cast<long long>(di[k]) * dos_n) : 0.0f;
+      const float u2 = Rc[k] ? ref_term(Rc[k], static_cast<long long>(dn[k]) * dir_n) : 0.0f;
+      const float u3 = Sc[k] ? ref_term(Sc[k], static_cast<long long>(dn[k]) * dis_n) : 0.0f;
+      dS = ref32_accumulate<G>(g, dS, u0, u1, u2, u3, true);
     }
   }
   return dS;
@@ -794,8 +883,12 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
   const long long acc = finalize_grp<G, Ops::kP>(a, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out,
                                                  ds_in, vi.kout, vi.kin, &ninf, ts.f, &f);
   if constexpr (Ops::kP == 3)
-    f = ref32_nodal<Ops, G>(a, ops, g, r, s, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin, Rr, Rs, Sr, Ss, wor,
-                            wos, key, two, twi, cap, lg);
+    f = ref32_nodal<Ops, G>(ops, a.din, a.dout, a.Trow, a.Tcol, a.tld, r, s, static_cast<int>(dr_out),
+                            static_cast<int>(dr_in),
+                            static_cast<int>(ds_out), static_cast<int>(ds_in), static_cast<int>(vi.kout),
+                            static_cast<int>(vi.kin), static_cast<int>(Rr), static_cast<int>(Rs),
+                            static_cast<int>(Sr), static_cast<int>(Ss), static_cast<int>(wor),
+                            static_cast<int>(wos), key, two, twi, cap, lg);
   if (g.gl == 0) {
     const bool moved = emit<Ops::kP>(a, v, r, s, acc, f, ninf);
     tally<Ops::kP>(tl, moved, acc, f, ninf);
@@ -994,8 +1087,12 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
     const long long acc = finalize_grp<32, Ops::kP>(a, Grp<32>(lane), tot, Rr, Rs, Sr, Ss, wor, wos, dr_out,
                                                     dr_in, ds_out, ds_in, vi.kout, vi.kin, &ninf, fpart, &f);
     if constexpr (Ops::kP == 3)
-      f = ref32_nodal<Ops, 32>(a, ops, Grp<32>(lane), r, s, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin, Rr, Rs,
-                               Sr, Ss, wor, wos, key, two, twi, cap, lg);
+      f = ref32_nodal<Ops, 32>(ops, a.din, a.dout, a.Trow, a.Tcol, a.tld, r, s, static_cast<int>(dr_out),
+                               static_cast<int>(dr_in),
+                               static_cast<int>(ds_out), static_cast<int>(ds_in), static_cast<int>(vi.kout),
+                               static_cast<int>(vi.kin), static_cast<int>(Rr), static_cast<int>(Rs),
+                               static_cast<int>(Sr), static_cast<int>(Ss), static_cast<int>(wor),
+                               static_cast<int>(wos), key, two, twi, cap, lg);
     if (lane == 0) {
       tally_ctl<Ops::kP>(a.ctl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
       if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * occ + 48 + 8ull * sh->scanned;
@@ -1637,6 +1734,29 @@ __device__ __forceinline__ void unit_vertices(const NodalArgs& a, const Ops& ops
   }
 }
 
+// Precision mode 3: the reference's old-state dS terms of every tile cell
+// for the batch about to be proposed (grid-collective; they depend on the
+// cell and its blocks' degrees only, not on the proposing vertex):
+//   Trow[b, i] = M[b,i] log(M[b,i] / (d_in[i] d_out[b]))
+//   Tcol[b, i] = M[i,b] log(M[i,b] / (d_out[i] d_in[b]))
+// in the reference's float arithmetic (ref_term), 0 for empty cells.
+__device__ __forceinline__ void ref32_tables_pass(int B, int ld, const int* M, const int* Mt, const int32_t* din,
+                                                  const int32_t* dout, float* Trow, float* Tcol) {
+  const long long cells = static_cast<long long>(B) * ld;
+  for (long long c = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; c < cells;
+       c += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int b = static_cast<int>(c / ld), i = static_cast<int>(c - static_cast<long long>(b) * ld);
+    float tr = 0.0f, tc = 0.0f;
+    if (i < B) {
+      const int x = __ldcg(M + c), y = __ldcg(Mt + c);
+      if (x) tr = ref_term(x, static_cast<long long>(__ldcg(din + i)) * __ldcg(dout + b));
+      if (y) tc = ref_term(y, static_cast<long long>(__ldcg(dout + i)) * __ldcg(din + b));
+    }
+    __stcg(Trow + c, tr);
+    __stcg(Tcol + c, tc);
+  }
+}
+
 template <int P, bool kSnap>
 __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
   extern __shared__ int dyn[];
@@ -1712,6 +1832,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       a.beg = bi * p.bs;
       a.end = a.beg + p.bs < p.n ? a.beg + p.bs : p.n;
       const int count = a.end - a.beg;
+      if constexpr (P == 3) {
+        if (p.a.Trow) {   // the batch's old-state terms, before anyone proposes
+          ref32_tables_pass(B, p.a.tld, p.v.M, p.v.Mt, p.din, p.dout, p.a.Trow, p.a.Tcol);
+          if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+        }
+      }
       if (kSnap) {
         // the tile as the previous batch left it (rows padded to ld with
         // zeros; cld = 1)

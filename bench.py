@@ -294,35 +294,64 @@ def precision_sample(ctx, G, local_rank: int, seeds=(0, 1, 2, 3, 4)) -> dict:
     return out
 
 
+def nmi_numpy(truth, given) -> float:
+    """Normalised mutual information 2 MI / (H_truth + H_given) of two
+    labelings, in plain numpy (the reference arm loads none of this
+    project's libraries)."""
+    import numpy as np
+    t = np.unique(np.asarray(truth), return_inverse=True)[1]
+    g = np.unique(np.asarray(given), return_inverse=True)[1]
+    n = t.size
+    cell = np.unique(t.astype(np.int64) * (int(g.max()) + 1) + g, return_counts=True)[1] / n
+    pt = np.bincount(t) / n
+    pg = np.bincount(g) / n
+    h_t = -float(np.sum(pt * np.log(pt)))
+    h_g = -float(np.sum(pg * np.log(pg)))
+    mi = h_t + h_g + float(np.sum(cell * np.log(cell)))
+    return 2.0 * mi / (h_t + h_g) if h_t + h_g > 0 else 1.0
+
+
+def bench_config(world: int) -> dict:
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "graph_seed": 0 if world == 1 else "rank",
+            "num_batch_nodal_update": 10, "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MiB write) before each step",
+            "init": "SCC/DFS initial blocks (dfs_depth 20)"}
+
+
 def run_reference_arm(args, rank: int, world: int):
+    """The reference's own partition() (oracle/_ref/ref_main, compiled from
+    its sources) on rank 0's graph, K full solves after W warm-up solves of
+    the N=5000 graph.  NMI per step is scored in numpy; nothing of this
+    project's CUDA library is loaded."""
     if rank != 0:
         return
     from usap_b200 import generator as gen
-    from usap_b200.api import evaluate
     threads = os.cpu_count() or 1
     G = graph_for(0)
     Gw = gen.generate(gen.config_c1())
     for _ in range(args.warmup):      # warm the binary and page cache (untimed, N=5000)
         reference_solve(Gw, threads)
-    times, B, nmi = [], None, None
+    times, Bs, nmis = [], [], []
     for k in range(args.steps):
         t, B, part = reference_solve(G, threads)
         times.append(t)
-        log(f"reference step {k}: {t:.2f} s, B={B}")
-    nmi = evaluate(G.truth, part)["nmi"]
+        Bs.append(int(B))
+        nmis.append(nmi_numpy(G.truth, part))
+        log(f"reference step {k}: {t:.2f} s, B={B}, NMI={nmis[-1]:.4f}")
     v = statistics.mean(times)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1000,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded DC-SBM generator)",
-        "config": {"workload": WORKLOAD, "graph_seed": 0, "num_batch_nodal_update": 10,
-                   "threads": threads},
+        "config": bench_config(world),
         "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "reference",
                          "sample": "full partition() of the N=50k graph per step (timed as "
                                    "main.cpp:54-60 does), reference sources + Taskflow-API shim"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "B": B, "nmi": nmi, "step_seconds": times,
+        "B": Bs[-1], "nmi": nmis[-1], "step_B": Bs, "step_nmi": nmis,
+        "mean_nmi": statistics.mean(nmis), "step_seconds": times,
     }
     print(json.dumps(line), flush=True)
 
@@ -493,9 +522,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         "warmup": args.warmup, "ms_per_step": value * 1000, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32 counts, f64 entropy (Q32 sums)",
         "data": "synthetic (seeded DC-SBM generator)",
-        "config": {"workload": WORKLOAD, "graph_seed": "rank", "num_batch_nodal_update": 10,
-                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) before each step",
-                   "init": "SCC/DFS initial blocks (dfs_depth 20)"},
+        "config": bench_config(world),
         "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": int(e2e_res["h2d_bytes"]),
                 "d2h_bytes_per_step": int(e2e_res["d2h_bytes"])},
         "gpu_launches": launches,

@@ -109,3 +109,62 @@ def test_static_limits_and_bad_ids(env):
     assert rc == 0
     torch.cuda.synchronize()
     assert abs(int(out.item()) - want) <= TOL_Q32
+
+
+def test_static_calls_allocate_nothing(env):
+    """After the first call on a device (which sets up the log table and
+    loads the kernels), further calls leave the device's free memory
+    unchanged: the entry point allocates nothing."""
+    torch, api, native = env
+    G = gen.generate(gen.config_c0(seed=3))
+    src, dst = _dev(torch, G.src), _dev(torch, G.dst)
+    part = _dev(torch, G.truth)
+    Bt = int(G.truth.max()) + 1
+    outs = [torch.zeros(1, dtype=torch.int64, device="cuda") for _ in range(8)]
+    assert _call(torch, native, src, dst, None, G.n, part, Bt, outs[0]) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for out in outs:
+        assert _call(torch, native, src, dst, None, G.n, part, Bt, out) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    vals = {int(o.item()) for o in outs}
+    assert len(vals) == 1
+
+
+_FRESH = r"""
+import ctypes as C, sys
+import numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from usap_b200 import api, generator as gen, native
+G = gen.generate(gen.config_c0(seed=5))
+Bt = int(G.truth.max()) + 1
+ctx = api.Context(0); ctx.load(G.src, G.dst, None, G.n)
+want = ctx.op_entropy(G.truth.astype(np.int32), Bt); ctx.close()
+st = torch.cuda.Stream()          # non-blocking with respect to the legacy stream
+with torch.cuda.stream(st):
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.int32)).cuda()
+    src, dst, part = d(G.src), d(G.dst), d(G.truth)
+    out = torch.zeros(1, dtype=torch.int64, device="cuda")
+    st.synchronize()
+    rc = native.lib().usap_entropy_static(C.c_void_p(src.data_ptr()), C.c_void_p(dst.data_ptr()), None,
+                                          src.numel(), G.n, C.c_void_p(part.data_ptr()), Bt,
+                                          C.c_void_p(out.data_ptr()), C.c_void_p(st.cuda_stream))
+    assert rc == 0, native.lib().usap_last_error()
+st.synchronize()
+assert int(out.item()) == want, (int(out.item()), want)
+print("fresh ok")
+"""
+
+
+def test_static_first_call_on_nonblocking_stream(env):
+    """In a fresh process, the very first call (the one that sets up the
+    log table) runs on a non-blocking stream and is already exact."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    p = subprocess.run([sys.executable, "-c", _FRESH, root], capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert "fresh ok" in p.stdout

@@ -112,7 +112,9 @@ class Server {
     if (n <= 0) {
       const int32_t base = g.one_based ? 1 : 0;
       int64_t m = -1;
-      for (int64_t i = 0; i < g.e; i++) m = std::max<int64_t>(m, static_cast<int64_t>(g.src[i]) - base);
+      // the largest id over both endpoints, as Job::load sizes the graph
+      for (int64_t i = 0; i < g.e; i++)
+        m = std::max<int64_t>(m, static_cast<int64_t>(std::max(g.src[i], g.dst[i])) - base);
       n = m + 1;
     }
     r->bytes = solve_footprint_bytes(n, g.e, p.dense_max > 0 ? p.dense_max : 4096, g.weight != nullptr);
@@ -140,7 +142,8 @@ class Server {
     std::shared_ptr<Request> r = it->second;
     if (block) cv_done_.wait(lk, [&] { return r->done; });
     if (!r->done) return false;
-    requests_.erase(it);
+    // another thread waiting on the same ticket may have taken it meanwhile
+    if (requests_.erase(ticket) == 0) throw Error(USAP_ERR_INVALID, "ticket " + std::to_string(ticket) + " was already taken");
     lk.unlock();
     if (timing) {
       auto ms = [](Clock::time_point a, Clock::time_point b) {

@@ -174,6 +174,9 @@ unsigned char* scratch_for(int dev) {
     USAP_CUDA(cudaMemcpy(base + kLogOff + sizeof(double) * k0, buf, sizeof(double) * (k1 - k0),
                          cudaMemcpyHostToDevice));
   }
+  // a copy from pageable memory may return before it lands; the first call's
+  // kernels can run on a non-blocking stream, so wait for the table here
+  USAP_CUDA(cudaDeviceSynchronize());
   g_scratch_ptr[dev] = base;
   return base;
 }

@@ -7,12 +7,66 @@
 #include "usap_oracle.h"
 
 #include <math.h>
+#include <pthread.h>
+#include <stdatomic.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 #define OG_TAG_MERGE 0x4D455247u /* 'MERG' */
 #define OG_TAG_NODAL 0x4E4F4441u /* 'NODA' */
 #define OG_NEAR_Q 4              /* |dS| <= 1e-9 in Q32 units */
+
+/* ------------------------------------------------------------------------ */
+/* A parallel loop over [0, n) on host threads (items handed out in chunks by
+ * an atomic counter).  Used only where the reference itself runs items in
+ * parallel from one snapshot (a batch's nodal proposals, a merge phase's
+ * blocks); every result is written per item or summed as integers, so the
+ * outcome does not depend on the thread count.  OG_THREADS overrides the
+ * thread count (1: sequential).                                            */
+typedef void (*og_item_fn)(void* ctx, int32_t item, int32_t worker);
+typedef struct {
+  og_item_fn fn;
+  void* ctx;
+  int32_t n, chunk, worker;
+  atomic_int* next;
+} og_pf_arg;
+
+static void* og_pf_run(void* p) {
+  og_pf_arg* a = (og_pf_arg*)p;
+  for (;;) {
+    int32_t i0 = atomic_fetch_add(a->next, a->chunk);
+    if (i0 >= a->n) break;
+    int32_t i1 = i0 + a->chunk < a->n ? i0 + a->chunk : a->n;
+    for (int32_t i = i0; i < i1; i++) a->fn(a->ctx, i, a->worker);
+  }
+  return NULL;
+}
+
+#define OG_MAX_WORKERS 64
+static int32_t og_workers(void) {
+  const char* e = getenv("OG_THREADS");
+  long t = e ? atol(e) : sysconf(_SC_NPROCESSORS_ONLN);
+  if (t < 1) t = 1;
+  if (t > OG_MAX_WORKERS) t = OG_MAX_WORKERS;
+  return (int32_t)t;
+}
+
+static void og_parallel_for(int32_t n, og_item_fn fn, void* ctx) {
+  int32_t nt = og_workers();
+  if (nt > n / 8) nt = n / 8 > 0 ? n / 8 : 1;
+  atomic_int next = 0;
+  og_pf_arg args[OG_MAX_WORKERS];
+  pthread_t th[OG_MAX_WORKERS];
+  for (int32_t t = 0; t < nt; t++)
+    args[t] = (og_pf_arg){fn, ctx, n, 8, t, &next};
+  int32_t started = 0;
+  for (int32_t t = 1; t < nt; t++)
+    if (pthread_create(&th[t], NULL, og_pf_run, &args[t]) == 0) started = t;
+    else break;
+  og_pf_run(&args[0]);
+  for (int32_t t = 1; t <= started; t++) pthread_join(th[t], NULL);
+}
 
 /* ------------------------------------------------------------------------ */
 /* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11).                         */
@@ -802,20 +856,35 @@ int32_t og_nodal_propose(const og_graph* g, const int32_t* part, const og_blocks
 }
 
 /* block_merge task (:349-368): K proposals per block, first strict minimum */
-void og_merge_phase(const og_graph* g, const og_blocks* b, int32_t K, int32_t stage,
-                    uint64_t seed, int32_t* best_s, int64_t* best_q) {
-  for (int32_t r = 0; r < b->B; r++) {
-    best_s[r] = -1;
-    best_q[r] = INT64_MAX;
-    for (int32_t k = 0; k < K; k++) {
-      int32_t s = og_merge_propose(g, b, r, k, stage, seed);
-      int64_t q = og_merge_dq(g, b, r, s);
-      if (q < best_q[r]) {
-        best_q[r] = q;
-        best_s[r] = s;
-      }
+typedef struct {
+  const og_graph* g;
+  const og_blocks* b;
+  int32_t K, stage;
+  uint64_t seed;
+  int32_t* best_s;
+  int64_t* best_q;
+} og_merge_task;
+
+static void og_merge_block(void* ctx, int32_t r, int32_t worker) {
+  (void)worker;
+  og_merge_task* t = (og_merge_task*)ctx;
+  t->best_s[r] = -1;
+  t->best_q[r] = INT64_MAX;
+  for (int32_t k = 0; k < t->K; k++) {
+    int32_t s = og_merge_propose(t->g, t->b, r, k, t->stage, t->seed);
+    int64_t q = og_merge_dq(t->g, t->b, r, s);
+    if (q < t->best_q[r]) {
+      t->best_q[r] = q;
+      t->best_s[r] = s;
     }
   }
+}
+
+void og_merge_phase(const og_graph* g, const og_blocks* b, int32_t K, int32_t stage,
+                    uint64_t seed, int32_t* best_s, int64_t* best_q) {
+  og_merge_task t = {g, b, K, stage, seed, best_s, best_q};
+  /* blocks are independent (the block_merge task runs them in parallel) */
+  og_parallel_for(b->B, og_merge_block, &t);
 }
 
 /* _carry_out_best_merges (:1225-1279), sequential as in the reference, with
@@ -863,51 +932,83 @@ int32_t og_merge_apply(int32_t n, int32_t* part, int32_t B, const int32_t* best_
  * accepted float values are what the convergence sums add (:428-430), in
  * Q32; the exact value still gives prop_q and the near-threshold count.
  * prop_f (optional) receives the float dS of each proposal.               */
+typedef struct {
+  const og_graph* g;
+  const int32_t* part;
+  const og_blocks* b;
+  int32_t beg, itr, stage, precision;
+  uint64_t seed;
+  int32_t *prop_s, *prop_ninf, *mv;
+  int64_t* prop_q;
+  float* prop_f;
+  /* per worker: moves, accepted sum (Q32), near-threshold count, -inf flag */
+  int64_t moves[OG_MAX_WORKERS], cq[OG_MAX_WORKERS], nnear[OG_MAX_WORKERS];
+  int32_t cn[OG_MAX_WORKERS];
+} og_nodal_task;
+
+static void og_nodal_item(void* ctx, int32_t i, int32_t w) {
+  og_nodal_task* t = (og_nodal_task*)ctx;
+  const int32_t v = t->beg + i;
+  int32_t s = og_nodal_propose(t->g, t->part, t->b, v, t->itr, t->stage, t->seed);
+  int32_t ninf = 0;
+  int64_t q = 0;
+  float f = 0.0f;
+  int32_t r = t->part[v];
+  int accept = 0;
+  if (s != r) {
+    q = og_nodal_dq(t->g, t->part, t->b, v, s, &ninf);
+    if (!ninf && (q <= OG_NEAR_Q && q >= -OG_NEAR_Q)) t->nnear[w]++;
+    if (t->precision == 3) {
+      f = og_nodal_ds_ref32(t->g, t->part, t->b, v, s);
+      accept = f < 0.0f;
+    } else {
+      accept = ninf || q < 0;
+    }
+  }
+  if (t->prop_s) t->prop_s[i] = (s != r) ? s : -1;
+  if (t->prop_q) t->prop_q[i] = q;
+  if (t->prop_ninf) t->prop_ninf[i] = ninf;
+  if (t->prop_f) t->prop_f[i] = f;
+  t->mv[i] = accept ? s : -1;
+  if (accept) {
+    t->moves[w]++;
+    if (t->precision == 3) {
+      if (isinf(f)) t->cn[w] = 1;
+      else t->cq[w] += og_q32_f(f);
+    } else if (ninf) {
+      t->cn[w] = 1;
+    } else {
+      t->cq[w] += q;
+    }
+  }
+}
+
+/* one batch (:397-443): every proposal reads the batch-start state (the
+ * reference runs them in parallel, so this loop does too), then the
+ * accepted moves are applied and M rebuilt */
 int64_t og_nodal_batch_p(const og_graph* g, int32_t* part, og_blocks* b, int32_t beg,
                          int32_t end, int32_t itr, int32_t stage, uint64_t seed, int32_t precision,
                          int32_t* prop_s, int64_t* prop_q, int32_t* prop_ninf, float* prop_f,
                          int64_t* cum_q, int32_t* cum_ninf, int64_t* near_threshold) {
   int32_t cnt = end - beg;
-  int32_t* mv = malloc(sizeof(int32_t) * ((size_t)cnt + 1));
+  og_nodal_task* t = calloc(1, sizeof(og_nodal_task));
+  t->g = g; t->part = part; t->b = b; t->beg = beg; t->itr = itr; t->stage = stage;
+  t->precision = precision; t->seed = seed;
+  t->prop_s = prop_s; t->prop_q = prop_q; t->prop_ninf = prop_ninf; t->prop_f = prop_f;
+  t->mv = malloc(sizeof(int32_t) * ((size_t)cnt + 1));
+  og_parallel_for(cnt, og_nodal_item, t);
   int64_t moves = 0;
-  for (int32_t v = beg; v < end; v++) {
-    int32_t s = og_nodal_propose(g, part, b, v, itr, stage, seed);
-    int32_t ninf = 0;
-    int64_t q = 0;
-    float f = 0.0f;
-    int32_t r = part[v];
-    int accept = 0;
-    if (s != r) {
-      q = og_nodal_dq(g, part, b, v, s, &ninf);
-      if (!ninf && (q <= OG_NEAR_Q && q >= -OG_NEAR_Q) && near_threshold) (*near_threshold)++;
-      if (precision == 3) {
-        f = og_nodal_ds_ref32(g, part, b, v, s);
-        accept = f < 0.0f;
-      } else {
-        accept = ninf || q < 0;
-      }
-    }
-    if (prop_s) prop_s[v - beg] = (s != r) ? s : -1;
-    if (prop_q) prop_q[v - beg] = q;
-    if (prop_ninf) prop_ninf[v - beg] = ninf;
-    if (prop_f) prop_f[v - beg] = f;
-    mv[v - beg] = accept ? s : -1;
-    if (accept) {
-      moves++;
-      if (precision == 3) {
-        if (isinf(f)) *cum_ninf = 1;
-        else *cum_q += og_q32_f(f);
-      } else if (ninf) {
-        *cum_ninf = 1;
-      } else {
-        *cum_q += q;
-      }
-    }
+  for (int32_t w = 0; w < OG_MAX_WORKERS; w++) {
+    moves += t->moves[w];
+    *cum_q += t->cq[w];
+    if (t->cn[w]) *cum_ninf = 1;
+    if (near_threshold) *near_threshold += t->nnear[w];
   }
   for (int32_t v = beg; v < end; v++)
-    if (mv[v - beg] >= 0) part[v] = mv[v - beg];
+    if (t->mv[v - beg] >= 0) part[v] = t->mv[v - beg];
   og_build(g, part, b);
-  free(mv);
+  free(t->mv);
+  free(t);
   return moves;
 }
 

@@ -1,4 +1,4 @@
-/* Oracle: a plain-C, single-threaded restatement of uSAP's stochastic block
+/* Oracle: a plain-C restatement of uSAP's stochastic block
  * partitioning path (include/graph_parallel.hpp of chih-chun-chang/uSAP).
  *
  * TEST INFRASTRUCTURE ONLY.  It is what the CUDA path is compared

@@ -80,7 +80,8 @@ typedef struct usap_params {
                           when the tile is dense and B <= 4096; 0: one launch per batch.
                           usap_batch_partition always uses per-batch launches. */
   int32_t persistent_ctas; /* CTAs of the cooperative kernel (one per SM); 0 = every SM */
-  int32_t precision;   /* 0 (default): every dS term in FP64, rounded to Q32 and summed exactly.
+  int32_t precision;   /* 3 (default): the reference's float nodal dS, below.
+                          0: every dS term in FP64, rounded to Q32 and summed exactly.
                           1 and 2: dS also evaluated with single-precision operations only, and
                           the nodal accept and merge choices taken on that value; the exact FP64
                           value is computed beside it to count flipped decisions
@@ -91,7 +92,7 @@ typedef struct usap_params {
                           accuracy on large counts; kept to measure that).  The description
                           length, the golden-section comparisons and the convergence test stay
                           FP64 in every mode.
-                          3: the reference's own single-precision nodal dS
+                          3 (default): the reference's own single-precision nodal dS
                           (graph_parallel.hpp:1066-1215): every term count * logf((float)count /
                           (float)(d_a * d_b)) in float, added to one float accumulator in the
                           reference's term order over all B blocks; accept iff it is < 0, and the
@@ -150,7 +151,8 @@ typedef struct usap_scores {
 
 /* Trace events for replay harnesses: one after each merge application
  * (kind 1), each nodal batch (kind 2) and each finished stage (kind 3),
- * with checksums of the partition, of M's non-zeros and of the degrees. */
+ * with checksums of the partition, of M's non-zeros and of the degrees.
+ * itr: the sweep of a batch (kind 2), the sweeps the stage ran (kind 3). */
 typedef struct usap_trace_event {
   int32_t kind, stage, itr, batch_beg, B;
   int64_t S_q;     /* kind 2: data term of the running S (Q32; S = model term + S_q / 2^32);
@@ -224,6 +226,12 @@ usap_status usap_ctx_evaluate(usap_ctx* ctx, const int32_t* truth, usap_scores* 
 usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out_assign,
                                usap_result* out);
 usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user);
+/* Failure injection for tests (no counterpart in the reference): in the next
+ * cooperative nodal-phase launch of this context, CTA `hold_cta` never
+ * arrives at its grid barriers and every barrier wait gives up after
+ * timeout_ns (> 0; at most 10 s), so that solve returns USAP_ERR_INTERNAL
+ * ("a grid barrier timed out").  One launch only; the context stays usable. */
+usap_status usap_ctx_test_barrier_timeout(usap_ctx* ctx, int32_t hold_cta, int64_t timeout_ns);
 
 /* --- batched form: many independent jobs on one GPU ---------------------- */
 /* One job solves graphs[graph] with its own Philox seed (several jobs on the

@@ -1074,7 +1074,7 @@ void og_params_default(og_params* p) {
   p->dfs_depth = 20;
   p->seed = 0;
   p->init_mode = 0;
-  p->precision = 0;
+  p->precision = 3;   /* the reference's float nodal dS, as usap_params_default */
 }
 
 static inline int32_t og_reduce(int32_t B, float rate) {
@@ -1229,6 +1229,7 @@ static int og_partition_impl(const og_graph* g, const og_params* p, const int32_
     double thr = isf ? p->delta_entropy_threshold2 : p->delta_entropy_threshold1;
     int converged = 0;
     const double model = og_model_S(n, g->e, B);
+    int32_t stage_sweeps = 0;
     for (int32_t itr = 0; itr < maxitr && !converged; itr++) {
       int64_t S_q = og_data_q(g, &blk);   /* data term; S = model + S_q / 2^32 */
       int32_t S_n = 0;
@@ -1242,6 +1243,7 @@ static int og_partition_impl(const og_graph* g, const og_params* p, const int32_
       int64_t cum_q = 0;
       int32_t cum_n = 0;
       res->sweeps++;
+      stage_sweeps++;
       for (int32_t beg = 0; beg < n; beg += bs) {
         int32_t end = beg + bs < n ? beg + bs : n;
         int64_t mv = og_nodal_batch_p(g, part, &blk, beg, end, itr, stage, p->seed, p->precision,
@@ -1267,7 +1269,7 @@ static int og_partition_impl(const og_graph* g, const og_params* p, const int32_
     const double S_fin = og_desc_length(model, data_fin);
     const int64_t S_fin_q = og_add_sat(og_quantize(model), data_fin);
     memset(&ev, 0, sizeof(ev));
-    ev.kind = 3; ev.stage = stage; ev.B = B; ev.S_q = S_fin_q;
+    ev.kind = 3; ev.stage = stage; ev.itr = stage_sweeps; ev.B = B; ev.S_q = S_fin_q;
     og_emit(trace, user, &ev, g, part, &blk);
     res->stages++;
     stage++;

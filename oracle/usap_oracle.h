@@ -71,7 +71,7 @@ typedef struct {
   int32_t dfs_depth;                     /* graph_parallel.hpp:51 */
   uint64_t seed;
   int32_t init_mode;                     /* 0: SCC (reference), 1: identity */
-  int32_t precision;                     /* 0: exact Q32 dS; 3: the reference's float nodal dS */
+  int32_t precision;                     /* 3 (default): the reference's float nodal dS; 0: exact Q32 dS */
 } og_params;
 
 typedef struct {

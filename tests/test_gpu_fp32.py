@@ -153,7 +153,7 @@ def test_fp32_solve_close_to_fp64(api, oracle, mode, persistent):
     ctx = api.Context(0)
     ctx.load(G.src, G.dst, None, G.n)
     base = dict(num_batch_nodal_update=10, seed=7, persistent=persistent)
-    p64, r64 = ctx.partition(nat.default_params(**base))
+    p64, r64 = ctx.partition(nat.default_params(precision=0, **base))
     p32, r32 = ctx.partition(nat.default_params(precision=mode, **base))
     p32b, r32b = ctx.partition(nat.default_params(precision=mode, **base))
     ctx.close()

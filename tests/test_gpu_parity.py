@@ -287,14 +287,20 @@ def test_persistent_move_list_overflow(api, oracle):
     assert np.array_equal(part_b, part_o) and res_b["S_q"] == res_o["S_q"]
 
 
-@pytest.mark.parametrize("within,alpha,seed", [(0.8, 10.0, 0), (0.5, 1.0, 1), (0.8, 1.0, 2),
-                                               (0.5, 10.0, 3)])
-def test_c1_solve_exact(api, oracle, within, alpha, seed):
-    """N=5000, 19 planted blocks, the four {within, alpha} variants: the
-    final partition, B and S equal the oracle's."""
+C1_VARIANTS = [(0.8, 10.0), (0.5, 10.0), (0.8, 1.0), (0.5, 1.0)]
+
+
+@pytest.mark.parametrize("precision", [3, 0])
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+@pytest.mark.parametrize("within,alpha", C1_VARIANTS)
+def test_c1_solve_exact(api, oracle, within, alpha, seed, precision):
+    """N=5000, 19 planted blocks: each of the four {within, alpha} variants
+    with graph and chain seeds 0..3, in the default precision (the
+    reference's float nodal dS) and in exact FP64: the final partition, B, S
+    and sweeps equal the oracle's."""
     from usap_b200 import native as nat
     G = gen.generate(gen.config_c1(within=within, alpha=alpha, seed=seed))
-    params = {"num_batch_nodal_update": 10, "seed": seed}
+    params = {"num_batch_nodal_update": 10, "seed": seed, "precision": precision}
     ctx = api.Context(0)
     ctx.load(G.src, G.dst, None, G.n)
     part_g, res_g = ctx.partition(nat.default_params(**params))
@@ -305,26 +311,10 @@ def test_c1_solve_exact(api, oracle, within, alpha, seed):
     assert (res_g["B"], res_g["S_q"], res_g["sweeps"]) == (res_o["B"], res_o["S_q"], res_o["sweeps"])
 
 
-def test_quality_matches_reference_runs(api, oracle, ref_fixtures):
-    """NMI of GPU solves on the C0 graph against the recorded reference runs
-    (the reference seeds from std::random_device: compared by distribution)."""
-    from usap_b200 import native as nat
-    g = ref_fixtures["graphs"]["c0"]
-    truth = np.array(g["truth"])
-    ref = [oracle.evaluate(truth, np.array(r["part"]))["nmi"] for r in ref_fixtures["c0_runs"]]
-    ctx = api.Context(0)
-    ctx.load(np.array(g["src"]), np.array(g["dst"]), None, g["n"])
-    mine = []
-    for seed in range(8):
-        part, _ = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=seed))
-        mine.append(api.evaluate(truth, part)["nmi"])
-    ctx.close()
-    assert abs(np.mean(mine) - np.mean(ref)) < 0.06, (mine, ref)
-
-
 def test_c2_scale_properties(api):
-    """N=50000, 44 blocks, ~780k edges (too large for the oracle): the result
-    is self-consistent and reproducible.  S reported equals S recomputed from
+    """N=50000, 44 blocks, ~780k edges (the oracle comparison of this graph
+    is in test_gpu_c2_quality.py): the result is self-consistent and
+    reproducible.  S reported equals S recomputed from
     the returned partition; labels are compact in [0, B); a second solve with
     the same seed is identical; the dense/sparse switch point does not change
     the answer."""
@@ -355,7 +345,8 @@ def test_identity_init_large_B(api):
     G = gen.generate(gen.config_c2())
     ctx = api.Context(0)
     ctx.load(G.src, G.dst, None, G.n)
-    part, res = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=0, init_mode=1))
+    # exact FP64 dS: the float mode's O(B) sums make the B ~ N stages slow
+    part, res = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=0, init_mode=1, precision=0))
     B = res["B"]
     assert 1 <= B < 1000 and part.max() < B
     assert res["S"] > 0 and res["S_q"] == ctx.op_entropy(part, B)

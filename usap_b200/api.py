@@ -100,6 +100,12 @@ class Context:
         nat.check(nat.lib().usap_ctx_evaluate(self._h, nat.p32(t), C.byref(s)))
         return nat.scores_dict(s)
 
+    def test_barrier_timeout(self, hold_cta: int, timeout_ns: int) -> None:
+        """Failure injection: the next cooperative nodal-phase launch has CTA
+        ``hold_cta`` withhold its grid-barrier arrivals and waits limited to
+        ``timeout_ns``, so that solve raises UsapError(-6)."""
+        nat.check(nat.lib().usap_ctx_test_barrier_timeout(self._h, int(hold_cta), int(timeout_ns)))
+
     def set_trace(self, fn: Optional[Callable[[dict], None]]) -> None:
         if fn is None:
             self._trace_fn = nat.TRACE_FN()

@@ -106,6 +106,7 @@ void usap_params_default(usap_params* p) {
   p->device = 0;
   p->stats = 0;
   p->persistent = 1;
+  p->precision = 3;   // the reference's own float nodal dS (graph_parallel.hpp:1066-1215)
 }
 
 usap_status usap_partition(const usap_graph* g, const usap_params* p, int32_t* out_assign,
@@ -236,6 +237,16 @@ usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user) {
   return guarded([&] {
     check_ctx(ctx);
     ctx->job->set_trace(fn, user);
+  });
+}
+
+usap_status usap_ctx_test_barrier_timeout(usap_ctx* ctx, int32_t hold_cta, int64_t timeout_ns) {
+  return guarded([&] {
+    check_ctx(ctx);
+    if (hold_cta < 0) throw usap::Error(USAP_ERR_INVALID, "hold_cta must be >= 0");
+    if (timeout_ns <= 0 || timeout_ns > 10000000000ll)
+      throw usap::Error(USAP_ERR_INVALID, "timeout_ns must be in (0, 10 s]");
+    ctx->job->arm_barrier_test(hold_cta, static_cast<unsigned long long>(timeout_ns));
   });
 }
 

@@ -259,6 +259,8 @@ struct PhaseArgs {
   double model_d;           // model term of S for this stage's B
   long long* ide_q;
   int* ide_n;
+  unsigned long long bar_timeout_ns;  // wait limit of the grid barriers (0: 200 ms)
+  int bar_hold;             // failure injection: this CTA never arrives at a barrier (-1: none)
 };
 
 // Control block of a gang launch (several jobs' nodal phases at once).

@@ -760,6 +760,10 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
   pa.model_d = model_d;
   pa.ide_q = ide_q_;
   pa.ide_n = ide_n_;
+  pa.bar_timeout_ns = bar_test_timeout_ns_;
+  pa.bar_hold = bar_test_hold_;
+  bar_test_hold_ = -1;   // one launch only
+  bar_test_timeout_ns_ = 0;
   // precision mode 3: the old-state term tables of the single-job kernel
   // (B <= kRefTabMaxB; above it the per-cell tables cost more than the
   // proposals' own evaluation)
@@ -1094,7 +1098,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
     const long long S_fin_q = add_sat(q32_host(model_d), data_fin);
     auto tn1 = std::chrono::steady_clock::now();
     ms_nodal += std::chrono::duration<double, std::milli>(tn1 - tm1).count();
-    if (trace_on(3)) emit_trace(3, stage, 0, 0, B, part, dense, S_fin_q, 0, 0, 0, 0);
+    if (trace_on(3)) emit_trace(3, stage, static_cast<int>(h_ctl_->sweeps), 0, B, part, dense, S_fin_q, 0, 0, 0, 0);
     res->stages++;
     stage++;
 

@@ -194,6 +194,13 @@ class Job {
     trace_ = fn;
     trace_user_ = user;
   }
+  // failure injection for tests: the next cooperative nodal-phase launch
+  // has CTA `hold` withhold its barrier arrivals and waits limited to
+  // timeout_ns, so the launch ends with USAP_ERR_INTERNAL
+  void arm_barrier_test(int hold, unsigned long long timeout_ns) {
+    bar_test_hold_ = hold;
+    bar_test_timeout_ns_ = timeout_ns;
+  }
   // init (n labels >= 0, renumbered 0..B-1 in ascending order) replaces
   // the SCC pass as the initial partition when given
   void partition(const usap_params& p, int32_t* out_assign, usap_result* res, const int32_t* init = nullptr);
@@ -278,6 +285,8 @@ class Job {
   int64_t hcap_ = 0;          // hub scratch slots
   size_t units_cap_ = 0;      // ints of units_
   int32_t bs_ = 1;   // nodal batch size of the current solve
+  int bar_test_hold_ = -1;                 // arm_barrier_test
+  unsigned long long bar_test_timeout_ns_ = 0;
   int32_t* slots_[4] = {nullptr, nullptr, nullptr, nullptr};
   int32_t* move_to_ = nullptr;
   int32_t* from_ = nullptr;

@@ -898,7 +898,11 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
       for (int c = 0; c < nch; c++)
         if (i0 + c < tl->own_cap) tl->own[i0 + c] = make_int2(v, tl->own_tag | c);
     }
-    if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * noccupied + 48 + 8ull * scanned;
+    // precision 3 also reads, for the old-state and again for the new-state
+    // terms, rows r and s and columns r and s of M and both degree arrays:
+    // 2 x 24 bytes per block, as the reference's O(B) loops do
+    if (a.stats)
+      *my_bytes += 8 + 8ull * deg + 48ull * noccupied + 48 + 8ull * scanned + (Ops::kP == 3 ? 48ull * a.B : 0ull);
   }
   g.sync();
 }
@@ -1095,7 +1099,8 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
                                static_cast<int>(wos), key, two, twi, cap, lg);
     if (lane == 0) {
       tally_ctl<Ops::kP>(a.ctl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
-      if (a.stats) *my_bytes += 8 + 8ull * deg + 48ull * occ + 48 + 8ull * sh->scanned;
+      if (a.stats)
+        *my_bytes += 8 + 8ull * deg + 48ull * occ + 48 + 8ull * sh->scanned + (Ops::kP == 3 ? 48ull * a.B : 0ull);
     }
   }
   __syncthreads();
@@ -1656,13 +1661,24 @@ constexpr unsigned long long kBarOvf = 1ull << 48;    // bits 48..63: overflow a
 // receives the overflow count.  A wait gives up after kBarrierTimeoutNs and
 // sets bar_err.  Returns -1 on error (every CTA then leaves at its next
 // barrier), else 1 if kBarDone is set, else 0.
+// Wait limit of a grid barrier and the failure-injection switch: a CTA
+// with `hold` set never arrives, so every wait of the launch runs out.
+struct BarrierOpts {
+  unsigned long long timeout_ns = kBarrierTimeoutNs;
+  bool hold = false;
+};
+
 template <class CtlT>
 __device__ __forceinline__ int grid_barrier(CtlT* ctl, unsigned* target, bool publish_done, int* s_state,
-                                            bool publish_ovf = false, unsigned* s_ovf = nullptr) {
+                                            bool publish_ovf = false, unsigned* s_ovf = nullptr,
+                                            BarrierOpts bo = BarrierOpts{}) {
   *target += gridDim.x;
   __syncthreads();
   if (threadIdx.x == 0) {
-    red_release_add64(&ctl->bar, (publish_done ? 1ull + kBarDone : 1ull) + (publish_ovf ? kBarOvf : 0ull));
+    // a CTA told to withhold its arrival (failure injection) still waits,
+    // so that every CTA leaves through the timeout below
+    if (!bo.hold)
+      red_release_add64(&ctl->bar, (publish_done ? 1ull + kBarDone : 1ull) + (publish_ovf ? kBarOvf : 0ull));
     const unsigned long long t0 = global_ns();
     unsigned spins = 0;
     int st;
@@ -1678,7 +1694,7 @@ __device__ __forceinline__ int grid_barrier(CtlT* ctl, unsigned* target, bool pu
           st = -1;
           break;
         }
-        if (global_ns() - t0 > kBarrierTimeoutNs) {
+        if (global_ns() - t0 > bo.timeout_ns) {
           atomicExch(&ctl->bar_err, 1);
           st = -1;
           break;
@@ -1789,6 +1805,9 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
     vs.CS = sCS;
   }
   const Ops ops{vs, p.a.B};
+  BarrierOpts bo;
+  bo.timeout_ns = p.bar_timeout_ns ? p.bar_timeout_ns : kBarrierTimeoutNs;
+  bo.hold = static_cast<int>(blockIdx.x) == p.bar_hold;
   // dense deltas in the first 2 * kPHubSlots ints, chunk-sum deltas (B <= 128: B entries) after them
   const int mode = p.a.B >= kDeltaGlobalMinB ? kDeltaGlobal
                    : (p.a.B * p.a.B <= 2 * kPHubSlots ? kDeltaDense : kDeltaHashed);
@@ -1820,12 +1839,12 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       acc = warp_sum_ll(acc);
       if (lane == 0 && acc) atomicAdd(&ctl->entropy_acc, static_cast<unsigned long long>(acc));
     }
-    if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+    if (grid_barrier(ctl, &target, false, &s_state, false, nullptr, bo) < 0) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       ctl_sweep_start(ctl, p.W, p.ide_q, p.ide_n);
       ctl->entropy_acc = 0;
     }
-    if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+    if (grid_barrier(ctl, &target, false, &s_state, false, nullptr, bo) < 0) return;
     const uint32_t itr = static_cast<uint32_t>(sw);   // ctl->sweeps before this sweep started
     for (int bi = 0; bi * p.bs < p.n; bi++) {
       NodalArgs a = p.a;
@@ -1835,7 +1854,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       if constexpr (P == 3) {
         if (p.a.Trow) {   // the batch's old-state terms, before anyone proposes
           ref32_tables_pass(B, p.a.tld, p.v.M, p.v.Mt, p.din, p.dout, p.a.Trow, p.a.Tcol);
-          if (grid_barrier(ctl, &target, false, &s_state) < 0) return;
+          if (grid_barrier(ctl, &target, false, &s_state, false, nullptr, bo) < 0) return;
         }
       }
       if (kSnap) {
@@ -1888,7 +1907,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       __syncthreads();
       if (threadIdx.x == 0) tally_flush(&s_tally, ctl);
       const int nown = s_nown;
-      if (grid_barrier(ctl, &target, false, &s_state, nown > kOwnCap, &s_ovf) < 0) return;
+      if (grid_barrier(ctl, &target, false, &s_state, nown > kOwnCap, &s_ovf, bo) < 0) return;
       // every CTA reads the same count here: the next overflow arrivals come
       // after the next proposal pass, which no CTA starts before all passed
       // the apply barrier below
@@ -1933,7 +1952,7 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
       }
       if (dt.mode == kDeltaDense) dense_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
       else if (dt.mode == kDeltaHashed) tables_flush(dt, p.M, p.Mt, p.CS, p.v.ld, p.v.cld);
-      const int st = grid_barrier(ctl, &target, done, &s_state);
+      const int st = grid_barrier(ctl, &target, done, &s_state, false, nullptr, bo);
       if (st < 0) return;   // a barrier failed
       if (st > 0) {         // converged
         converged = true;

@@ -477,8 +477,10 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
 //     the entries adjusted by v's out-weight (rows) and in-weight (columns)
 //     towards block i, looked up in the group's neighbour-block table.
 // A round covers kRefK * G blocks: lane l loads the entries of blocks
-// base + k G + l (k < kRefK) of the four rows at once, so one round trip
-// serves 4 kRefK loads per lane.  For each k the lanes evaluate the terms
+// base + k G + l (k < kRefK) of the four rows at once.  kRefK = 1 measured
+// fastest on the N=50000 solve (450 ms against 657 ms with 4 and 591 ms
+// with 2): deeper rounds hold registers that the persistent kernel's 80 per
+// thread cannot spare.  For each k the lanes evaluate the terms
 // of their block, and the terms are then added to one float accumulator in
 // the reference's order -- lane after lane, and within a lane in the
 // reference's term order (float addition does not reassociate).  Zero
@@ -487,7 +489,7 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
 // number of non-zero terms.  Every lane returns the same value.  Rr, Rs,
 // Sr, Ss: M[r,r], M[r,s], M[s,r], M[s,s]; wor, wos: v's out-weight to
 // blocks r and s.
-constexpr int kRefK = 4;
+constexpr int kRefK = 1;
 
 template <int G>
 __device__ __forceinline__ float ref32_accumulate(const Grp<G>& g, float dS, float t0, float t1, float t2,

@@ -226,6 +226,13 @@ usap_status usap_ctx_evaluate(usap_ctx* ctx, const int32_t* truth, usap_scores* 
 usap_status usap_ctx_partition(usap_ctx* ctx, const usap_params* p, int32_t* out_assign,
                                usap_result* out);
 usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user);
+/* The resident graph's adjacency (graph_parallel.hpp:285-290, insertion order
+ * = file order inside each list): out_ptr/in_ptr n + 1 entries, out_idx,
+ * in_idx, out_w, in_w e entries (weights 1 for an unweighted graph), kout,
+ * kin the weighted degrees (n).  Any pointer may be NULL.  A graph loaded
+ * with usap_ctx_load_tsv has these lists built on the device. */
+usap_status usap_ctx_adjacency(usap_ctx* ctx, int32_t* out_ptr, int32_t* out_idx, int32_t* out_w,
+                               int32_t* in_ptr, int32_t* in_idx, int32_t* in_w, int32_t* kout, int32_t* kin);
 /* Failure injection for tests (no counterpart in the reference): in the next
  * cooperative nodal-phase launch of this context, CTA `hold_cta` never
  * arrives at its grid barriers and every barrier wait gives up after

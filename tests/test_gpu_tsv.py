@@ -109,3 +109,39 @@ def test_tsv_c2_parse(api):
           f"numpy loadtxt of 100k lines {1e3 * (t2 - t1):.1f} ms")
     a.close()
     b.close()
+
+
+def _shuffled(G, seed=9):
+    """the same edges in a random file order (not grouped by source)"""
+    perm = np.random.default_rng(seed).permutation(G.num_edges)
+    return G.src[perm], G.dst[perm]
+
+
+@pytest.mark.parametrize("case", ["c2", "c2_shuffled", "weighted_crlf", "weighted_shuffled"])
+def test_device_adjacency_equals_host(api, case):
+    """usap_ctx_load_tsv builds the out- and in-lists on the device (stable
+    counting sort by source and by target, file order kept inside each
+    list); they equal, byte for byte, the lists the host builds from the
+    same edges as arrays (usap_ctx_load), with the weights and weighted
+    degrees."""
+    if case.startswith("c2"):
+        G = gen.generate(gen.config_c2(seed=0))
+    else:
+        G = gen.generate(gen.config_c1(within=0.5, alpha=1.0, seed=2))
+    src, dst = _shuffled(G) if case.endswith("shuffled") else (G.src, G.dst)
+    w = np.random.default_rng(5).integers(1, 4, src.size).astype(np.int32) if case.startswith("weighted") else None
+    n = int(max(src.max(), dst.max())) + 1
+    a = api.Context(0)
+    a.load(src, dst, w, n)
+    b = api.Context(0)
+    b.load_tsv(_tsv(src, dst, w, "\r\n" if case.endswith("crlf") else "\n"), n)
+    ha, hb = a.adjacency(), b.adjacency()
+    for k in ha:
+        assert ha[k].dtype == hb[k].dtype and np.array_equal(ha[k], hb[k]), (case, k)
+    # file order inside the lists: the in-list of a vertex lists its sources
+    # in the order their edges appear in the input
+    v = int(np.argmax(np.bincount(dst, minlength=n)))
+    lo, hi = hb["in_ptr"][v], hb["in_ptr"][v + 1]
+    assert np.array_equal(hb["in_idx"][lo:hi], src[dst == v])
+    a.close()
+    b.close()

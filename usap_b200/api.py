@@ -100,6 +100,17 @@ class Context:
         nat.check(nat.lib().usap_ctx_evaluate(self._h, nat.p32(t), C.byref(s)))
         return nat.scores_dict(s)
 
+    def adjacency(self) -> dict:
+        """The resident graph's out/in lists (file order inside each list),
+        weights and weighted degrees (usap_ctx_adjacency)."""
+        n, e = self.n, self.e
+        out = {k: np.empty(n + 1, np.int32) for k in ("out_ptr", "in_ptr")}
+        out.update({k: np.empty(e, np.int32) for k in ("out_idx", "out_w", "in_idx", "in_w")})
+        out.update({k: np.empty(n, np.int32) for k in ("kout", "kin")})
+        nat.check(nat.lib().usap_ctx_adjacency(self._h, *(nat.p32(out[k]) for k in (
+            "out_ptr", "out_idx", "out_w", "in_ptr", "in_idx", "in_w", "kout", "kin"))))
+        return out
+
     def test_barrier_timeout(self, hold_cta: int, timeout_ns: int) -> None:
         """Failure injection: the next cooperative nodal-phase launch has CTA
         ``hold_cta`` withhold its grid-barrier arrivals and waits limited to

@@ -162,16 +162,12 @@ usap_status usap_ctx_load_tsv(usap_ctx* ctx, const char* text, int64_t len, int3
     check_ctx(ctx);
     if (!text && len > 0) throw usap::Error(USAP_ERR_INVALID, "null text");
     if (n < 0) throw usap::Error(USAP_ERR_INVALID, "n must be >= 0");
-    usap::TsvEdges t = usap::parse_tsv_device(ctx->job->device(), text ? text : "", len);
+    // parse and adjacency lists on the device; the host keeps a copy of the
+    // lists for its own passes (initial blocks, work units)
+    usap::HostGraph h;
+    usap::TsvEdges t = usap::parse_tsv_device(ctx->job->device(), text ? text : "", len, n, &h);
     if (t.src.empty()) throw usap::Error(USAP_ERR_INVALID, "graph needs at least one edge");
-    usap_graph g{};
-    g.n = n > 0 ? n : t.max_src;   // N = the largest source id (graph_parallel.hpp:276)
-    g.e = static_cast<int64_t>(t.src.size());
-    g.src = t.src.data();
-    g.dst = t.dst.data();
-    g.weight = t.w.empty() ? nullptr : t.w.data();
-    g.one_based = 0;
-    ctx->job->load(g);
+    ctx->job->load_host(std::move(h));
   });
 }
 
@@ -237,6 +233,30 @@ usap_status usap_ctx_set_trace(usap_ctx* ctx, usap_trace_fn fn, void* user) {
   return guarded([&] {
     check_ctx(ctx);
     ctx->job->set_trace(fn, user);
+  });
+}
+
+usap_status usap_ctx_adjacency(usap_ctx* ctx, int32_t* out_ptr, int32_t* out_idx, int32_t* out_w,
+                               int32_t* in_ptr, int32_t* in_idx, int32_t* in_w, int32_t* kout, int32_t* kin) {
+  return guarded([&] {
+    check_ctx(ctx);
+    const usap::HostGraph& h = ctx->job->host_graph();
+    auto copy = [](int32_t* dst, const std::vector<int32_t>& v) {
+      if (dst && !v.empty()) std::memcpy(dst, v.data(), sizeof(int32_t) * v.size());
+    };
+    auto weights = [&](int32_t* dst, const std::vector<int32_t>& v) {
+      if (!dst) return;
+      if (h.unit) std::fill(dst, dst + h.e, 1);
+      else copy(dst, v);
+    };
+    copy(out_ptr, h.out_ptr);
+    copy(out_idx, h.out_idx);
+    weights(out_w, h.out_w);
+    copy(in_ptr, h.in_ptr);
+    copy(in_idx, h.in_idx);
+    weights(in_w, h.in_w);
+    copy(kout, h.kout);
+    copy(kin, h.kin);
   });
 }
 

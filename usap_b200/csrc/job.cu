@@ -210,11 +210,16 @@ void Job::free_state() {
 }
 
 // --- graph load -----------------------------------------------------------------
-std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
+std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in, HostGraph* pre) {
   USAP_CUDA(cudaSetDevice(device));
+  HostGraph h;
+  int64_t wtot = 0;
+  if (pre) {
+    h = std::move(*pre);
+    wtot = h.wtot;
+  } else {
   if (in.e <= 0 || !in.src || !in.dst) throw Error(USAP_ERR_INVALID, "graph needs at least one edge");
   if (in.e >= (1ll << 30)) throw Error(USAP_ERR_LIMIT, "more than 2^30 edges");
-  HostGraph h;
   h.e = in.e;
   const int32_t base = in.one_based ? 1 : 0;
   h.src.resize(in.e);
@@ -252,7 +257,6 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   if (maxid >= h.n)
     throw Error(USAP_ERR_INVALID, "vertex id " + std::to_string(maxid) + " >= n = " + std::to_string(h.n));
   h.unit = true;
-  int64_t wtot = 0;
   if (in.weight) {
     h.w.resize(in.e);
     for (int64_t i = 0; i < in.e; i++) {
@@ -267,8 +271,9 @@ std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in) {
   }
   if (wtot >= (1ll << 24)) throw Error(USAP_ERR_LIMIT, "total edge weight must be below 2^24");
   h.wtot = wtot;
+  }
   const int32_t n = h.n;
-  build_csr(h);
+  if (!h.csr_built) build_csr(h);
   scc_prepare(h);
   // per-vertex global hash regions for degrees beyond the shared-memory table
   std::vector<int64_t> hi_off(n, -1);
@@ -406,6 +411,12 @@ GraphResident::~GraphResident() {
 void Job::load(const usap_graph& in) {
   USAP_CUDA(cudaSetDevice(device_));
   attach(load_graph(device_, in));
+}
+
+void Job::load_host(HostGraph&& h) {
+  USAP_CUDA(cudaSetDevice(device_));
+  const usap_graph none{};
+  attach(load_graph(device_, none, &h));
 }
 
 void Job::attach(std::shared_ptr<GraphResident> gr) {

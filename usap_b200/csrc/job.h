@@ -2,7 +2,9 @@
 #pragma once
 
 #include <chrono>
+#include <functional>
 #include <future>
+#include <memory>
 #include <condition_variable>
 #include <mutex>
 #include <string>
@@ -32,6 +34,9 @@ struct HostGraph {
   bool transpose_is_in = false;
   // first 32-edge chunk of each vertex (n + 1 entries; GraphDev::chunks)
   std::vector<int64_t> chunk_ptr;
+  // the out/in lists and weighted degrees are filled already (built on the
+  // device from a parsed TSV, build_csr_device)
+  bool csr_built = false;
 };
 
 // _scc + _dfs_itr (graph_parallel.hpp:514-603), host side; scc_prepare
@@ -55,7 +60,15 @@ struct TsvEdges {
   std::vector<int32_t> src, dst, w;
   int32_t max_src = 0, max_id = 0;
 };
-TsvEdges parse_tsv_device(int device, const char* text, int64_t len);
+// With `graph` given, the parsed edges (0-based, n = the given n or else the
+// largest source id) and their out/in lists, built on the device by
+// build_csr_device, are also returned there.
+TsvEdges parse_tsv_device(int device, const char* text, int64_t len, int32_t n = 0, HostGraph* graph = nullptr);
+// out/in lists and weighted degrees of h's edges (h.n, h.e, h.src, h.unit
+// set) from the same edges in device memory (kernels_csr.cu); alloc
+// returns stream-ordered device memory freed by the caller
+void build_csr_device(const int32_t* d_src, const int32_t* d_dst, const int32_t* d_w, HostGraph& h,
+                      cudaStream_t st, const std::function<void*(size_t)>& alloc);
 
 // the same scores from device arrays on `device` (kernels_eval.cu)
 void evaluate_device(const int32_t* truth, const int32_t* given, int64_t n, int device, usap_scores* out);
@@ -121,7 +134,9 @@ struct GraphResident {
 };
 
 // Graph_P constructor / load_graph_from_tsv (graph_parallel.hpp:251-317)
-std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in);
+// (pre: a graph whose edges and lists are already on the host, e.g. from
+// parse_tsv_device; `in` is then ignored)
+std::shared_ptr<GraphResident> load_graph(int device, const usap_graph& in, HostGraph* pre = nullptr);
 
 // Runs the dense nodal phases of concurrent solves together in single
 // cooperative launches (k_nodal_gang); see gang.cpp.
@@ -178,6 +193,8 @@ class Job {
   Job& operator=(const Job&) = delete;
 
   void load(const usap_graph& g);
+  // a graph whose adjacency lists are built already (parse_tsv_device)
+  void load_host(HostGraph&& h);
   // solve a graph that is already resident (shared with other jobs)
   void attach(std::shared_ptr<GraphResident> gr);
   bool loaded() const { return hg_ != nullptr; }

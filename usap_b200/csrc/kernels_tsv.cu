@@ -160,7 +160,7 @@ __global__ void k_tsv_parse(const char* __restrict__ text, int64_t len, const in
 
 }  // namespace
 
-TsvEdges parse_tsv_device(int device, const char* text, int64_t len) {
+TsvEdges parse_tsv_device(int device, const char* text, int64_t len, int32_t n, HostGraph* graph) {
   if (!text || len < 0) throw Error(USAP_ERR_INVALID, "null text");
   // line counts and offsets are int32: at most 2^31 - 1 bytes of text
   if (len > static_cast<int64_t>(INT_MAX)) throw Error(USAP_ERR_LIMIT, "tsv text above 2^31 - 1 bytes");
@@ -240,6 +240,25 @@ TsvEdges parse_tsv_device(int device, const char* text, int64_t len) {
   USAP_CUDA(cudaStreamSynchronize(st));
   out.max_src = hs.max_src;
   out.max_id = hs.max_id;
+  if (graph) {
+    // the graph of load_graph_from_tsv: N = the largest source id (:276),
+    // or the caller's n; adjacency lists built here, on the device copy
+    HostGraph& h = *graph;
+    h.n = n > 0 ? n : out.max_src;
+    if (out.max_id > h.n)
+      throw Error(USAP_ERR_INVALID, "vertex id " + std::to_string(out.max_id - 1) + " >= n = " + std::to_string(h.n));
+    if (lines >= (1ll << 30)) throw Error(USAP_ERR_LIMIT, "more than 2^30 edges");
+    h.e = lines;
+    h.unit = !hs.nonunit;
+    h.wtot = 0;
+    for (int32_t x : out.w) h.wtot += x;
+    if (h.unit) h.wtot = lines;
+    if (h.wtot >= (1ll << 24)) throw Error(USAP_ERR_LIMIT, "total edge weight must be below 2^24");
+    h.src = out.src;
+    h.dst = out.dst;
+    h.w = out.w;
+    build_csr_device(dv, dv + lines, dv + 2 * lines, h, st, alloc);
+  }
   return out;
 }
 

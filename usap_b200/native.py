@@ -115,7 +115,7 @@ EXPORTS = ("usap_version", "usap_last_error", "usap_params_default", "usap_parti
            "usap_evaluate", "usap_evaluate_device", "usap_ctx_evaluate", "usap_ctx_create",
            "usap_ctx_destroy", "usap_ctx_load", "usap_ctx_load_tsv", "usap_ctx_add_edges",
            "usap_ctx_partition_from",
-           "usap_ctx_num_nodes", "usap_ctx_partition", "usap_ctx_set_trace", "usap_ctx_test_barrier_timeout", "usap_op_scc",
+           "usap_ctx_num_nodes", "usap_ctx_partition", "usap_ctx_set_trace", "usap_ctx_test_barrier_timeout", "usap_ctx_adjacency", "usap_op_scc",
            "usap_op_build", "usap_op_entropy", "usap_op_merge_phase", "usap_op_merge_apply",
            "usap_op_nodal_batch", "usap_op_merge_phase_prec", "usap_op_nodal_batch_prec",
            "usap_batch_partition", "usap_entropy_static",
@@ -152,6 +152,7 @@ def lib() -> C.CDLL:
     L.usap_ctx_partition.argtypes = [C.c_void_p, C.POINTER(Params), i32p, C.POINTER(Result)]
     L.usap_ctx_set_trace.argtypes = [C.c_void_p, TRACE_FN, C.c_void_p]
     L.usap_ctx_test_barrier_timeout.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
+    L.usap_ctx_adjacency.argtypes = [C.c_void_p] + [i32p] * 8
     L.usap_op_scc.argtypes = [C.c_void_p, C.c_int32, i32p, i32p]
     L.usap_op_build.argtypes = [C.c_void_p, i32p, C.c_int32, C.c_int32, i32p, i32p, i32p]
     L.usap_op_entropy.argtypes = [C.c_void_p, i32p, C.c_int32, C.c_int32, i64p]

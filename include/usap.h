@@ -70,7 +70,10 @@ typedef struct usap_params {
   int32_t t_block_num;                      /* 20 */
   /* B200 build */
   uint64_t seed;       /* Philox key of every proposal draw */
-  int32_t init_mode;   /* 0: SCC/DFS initial blocks (reference); 1: one block per vertex */
+  int32_t init_mode;   /* 0: SCC/DFS initial blocks on the host (the reference's, exact);
+                          1: one block per vertex; 2: a device stand-in for the SCC pass
+                          (the cells of a multi-source breadth-first search from one
+                          vertex in eight; different blocks of the same kind, no host pass) */
   int32_t dense_max;   /* dense int32 tile for B <= dense_max (default 4096), sorted views above */
   int32_t device;      /* CUDA device for usap_partition (ignored by contexts) */
   int32_t stats;       /* 1: per-kernel CUDA-event timings and algorithmic byte counts */
@@ -124,8 +127,8 @@ typedef struct usap_result {
   int64_t cub_calls;          /* CUB sort/scan/reduce calls during the call */
   int64_t h2d_bytes, d2h_bytes;  /* host<->device traffic of the call */
   int64_t sweep_graph_launches;  /* nodal sweeps replayed from a captured CUDA graph */
-  /* precision 1 or 2: the FP32 values and decisions against the FP64 values
-   * of the same evaluations (zero with precision = 0) */
+  /* precision 1, 2 or 3: the FP32 values and decisions against the FP64
+   * values of the same evaluations (zero with precision = 0) */
   int64_t fp32_nodal_evals;  /* nodal dS evaluations with a finite FP64 value */
   int64_t fp32_nodal_flips;  /* ... whose FP32 accept decision differs from FP64's */
   int64_t fp32_merge_evals;  /* merge proposals */
@@ -137,6 +140,7 @@ typedef struct usap_result {
   int64_t apply_scans;       /* nodal batches of the cooperative kernel whose moves were applied by
                                 scanning all of the batch's edges (a CTA accepted more moves than its
                                 shared-memory list holds) instead of each CTA's own list */
+  int64_t B_init;            /* blocks of the initial partition (before the first merge phase) */
 } usap_result;
 
 typedef struct usap_scores {

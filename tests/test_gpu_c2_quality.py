@@ -28,6 +28,8 @@ QUALITY = os.path.join(ROOT, "tests", "golden", "ref_quality.json")
 TOL_NMI = 0.01
 NO_STRUCTURE = 0.2
 SEEDS = 16
+B0_BAND = 0.10   # device initial blocks: within 10% of the SCC pass's count
+MAX_NO_STRUCTURE = 2
 
 
 @pytest.fixture(scope="module")
@@ -94,3 +96,39 @@ def test_quality_matches_reference_runs(api, name):
     ref_ok = ref[ref >= NO_STRUCTURE]
     assert ref_ok.size >= ref.size - 1
     assert abs(nmi.mean() - ref_ok.mean()) <= TOL_NMI, (name, nmi.mean(), ref_ok.mean())
+
+
+@pytest.mark.parametrize("name", ["c1_f0.5_a1", "c2"])
+def test_device_initial_blocks(api, name):
+    """init_mode 2, the device stand-in for the host SCC pass (multi-source
+    breadth-first cells from one vertex in eight): as many initial blocks
+    as the SCC pass within B0_BAND and a deterministic partition.  Over 16
+    seeds, the runs that find structure reach a mean NMI within TOL_NMI of
+    the reference's runs, as the default path must.  Unlike the default
+    path, this start sometimes keeps a large B and finds no structure, as
+    the reference itself does (1 of 16 runs at N=50000 here, 1 of 20 in an
+    earlier sample): at most MAX_NO_STRUCTURE of 16 may."""
+    from usap_b200 import native as nat
+    rec = _ref_runs()[name]
+    c = rec["config"]
+    G = gen.generate(gen.SBMConfig(n=c["n"], blocks=c["blocks"], within=c["within"], alpha=c["alpha"],
+                                   seed=c["seed"]))
+    ctx = api.Context(0)
+    ctx.load(G.src, G.dst, None, G.n)
+    _, scc = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=0))
+    nmi, first = [], None
+    for seed in range(SEEDS):
+        part, res = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=seed, init_mode=2))
+        assert abs(res["B_init"] - scc["B_init"]) <= B0_BAND * scc["B_init"], (res["B_init"], scc["B_init"])
+        if first is None:
+            first = (part, res)
+        nmi.append(api.evaluate(G.truth, part)["nmi"])
+    again, res2 = ctx.partition(nat.default_params(num_batch_nodal_update=10, seed=0, init_mode=2))
+    assert np.array_equal(again, first[0]) and res2["S_q"] == first[1]["S_q"]
+    ctx.close()
+    ref = np.array([r["nmi"] for r in rec["runs"]])
+    ref_ok = ref[ref >= NO_STRUCTURE]
+    nmi = np.array(nmi)
+    ok = nmi[nmi >= NO_STRUCTURE]
+    assert ok.size >= SEEDS - MAX_NO_STRUCTURE, nmi
+    assert abs(ok.mean() - ref_ok.mean()) <= TOL_NMI, (name, ok.mean(), ref_ok.mean())

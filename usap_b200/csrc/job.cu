@@ -921,10 +921,15 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
   F32Tally nodal32{0, 0, 0, 0.0};   // summed over the stages' nodal phases
   if (prec_) USAP_CUDA(cudaMemsetAsync(f32d_, 0, 2 * sizeof(F32Tally), st_));
 
-  // initial blocks (host): depth-limited DFS on the transpose, or identity
+  // initial blocks: the host's depth-limited DFS on the transpose (the
+  // reference's), one block per vertex, or the device's matching stand-in
   std::vector<int32_t> part0(n);
   int32_t B;
-  if (init) {
+  int32_t* dpart0 = nullptr;
+  if (!init && p.init_mode == 2) {
+    dpart0 = static_cast<int32_t*>(dev_alloc(sizeof(int32_t) * n, st_));
+    B = device_initial_blocks(g_, dpart0, st_, nullptr);
+  } else if (init) {
     B = compact_labels(init, n, part0.data());
   } else if (p.init_mode == 1) {
     for (int32_t v = 0; v < n; v++) part0[v] = v;
@@ -934,11 +939,17 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
   }
   ensure_capacity(B, K, dense_max, std::max(maxitr, 1));
   int32_t work = 0;
-  USAP_CUDA(cudaMemcpyAsync(slots_[work], part0.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st_));
+  if (dpart0) {
+    USAP_CUDA(cudaMemcpyAsync(slots_[work], dpart0, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st_));
+    dev_free(dpart0, st_);
+  } else {
+    USAP_CUDA(cudaMemcpyAsync(slots_[work], part0.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, st_));
+  }
   wait();
   auto t_init = std::chrono::steady_clock::now();
   res->ms_init = std::chrono::duration<double, std::milli>(t_init - t_start).count();
 
+  res->B_init = B;
   int32_t btm = reduce_blocks(B, p.num_block_reduction_rate);
   Golden gs;
   uint32_t stage = 0;

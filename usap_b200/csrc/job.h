@@ -69,6 +69,11 @@ TsvEdges parse_tsv_device(int device, const char* text, int64_t len, int32_t n =
 // returns stream-ordered device memory freed by the caller
 void build_csr_device(const int32_t* d_src, const int32_t* d_dst, const int32_t* d_w, HostGraph& h,
                       cudaStream_t st, const std::function<void*(size_t)>& alloc);
+void scan_exclusive_i32(const int32_t* in, int64_t m, int32_t* out, cudaStream_t st,
+                        const std::function<void*(size_t)>& alloc);
+// initial blocks on the device (init_mode 2, kernels_init.cu): compact
+// labels of n vertices into part (device), returns B; *rounds: matching rounds
+int32_t device_initial_blocks(const GraphDev& g, int32_t* part, cudaStream_t st, int* rounds);
 
 // the same scores from device arrays on `device` (kernels_eval.cu)
 void evaluate_device(const int32_t* truth, const int32_t* given, int64_t n, int device, usap_scores* out);

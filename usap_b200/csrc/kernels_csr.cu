@@ -130,9 +130,11 @@ int grid_for(int64_t work, int per_block) {
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16)));
 }
 
-// exclusive scan of n + 1 counts in place into ptr (ptr[n] = total)
-void scan_counts(const int32_t* cnt, int64_t m, int32_t* ptr, cudaStream_t st,
-                 const std::function<void*(size_t)>& alloc) {
+}  // namespace
+
+// exclusive scan of m int32 values (out[m - 1] + in[m - 1] = the total)
+void scan_exclusive_i32(const int32_t* cnt, int64_t m, int32_t* ptr, cudaStream_t st,
+                        const std::function<void*(size_t)>& alloc) {
   const int64_t tiles = (m + kScanTile - 1) / kScanTile;
   int32_t* sums = static_cast<int32_t*>(alloc(sizeof(int32_t) * tiles));
   k_scan_tile<<<static_cast<unsigned>(tiles), kScanTile, 0, st>>>(cnt, m, ptr, sums);
@@ -142,6 +144,8 @@ void scan_counts(const int32_t* cnt, int64_t m, int32_t* ptr, cudaStream_t st,
   k_scan_add<<<static_cast<unsigned>((m + kThreads - 1) / kThreads), kThreads, 0, st>>>(ptr, m, sums);
   USAP_LAUNCHED();
 }
+
+namespace {
 
 // one side (keyed by `key`): ptr (n + 1), idx and optional weights (e), the
 // weighted degree per key
@@ -161,7 +165,7 @@ void csr_side(const int32_t* key, const int32_t* val, const int32_t* w, int64_t 
   USAP_CUDA(cudaMemsetAsync(cursor, 0, sizeof(int32_t) * m, st));
   k_csr_count<<<grid_for(e, kThreads), kThreads, 0, st>>>(key, w, e, cnt, deg);
   USAP_LAUNCHED();
-  scan_counts(cnt, m, ptr, st, alloc);
+  scan_exclusive_i32(cnt, m, ptr, st, alloc);
   k_csr_scatter<<<grid_for(e, kThreads), kThreads, 0, st>>>(key, val, e, ptr, cursor, tmp);
   USAP_LAUNCHED();
   k_csr_rank<<<grid_for(static_cast<int64_t>(n) * 32, kThreads), kThreads, 0, st>>>(ptr, n, tmp, val, w, idx, wo);

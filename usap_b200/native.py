@@ -62,7 +62,7 @@ class Result(C.Structure):
                 ("fp32_merge_evals", C.c_int64), ("fp32_merge_flips", C.c_int64),
                 ("fp32_order_flips", C.c_int64), ("fp32_flip_rate", C.c_double),
                 ("fp32_err_max", C.c_double), ("fp32_err_mean", C.c_double),
-                ("apply_scans", C.c_int64)]
+                ("apply_scans", C.c_int64), ("B_init", C.c_int64)]
 
 
 class Scores(C.Structure):

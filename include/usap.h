@@ -74,7 +74,8 @@ typedef struct usap_params {
                           1: one block per vertex; 2: a device stand-in for the SCC pass
                           (the cells of a multi-source breadth-first search from one
                           vertex in eight; different blocks of the same kind, no host pass) */
-  int32_t dense_max;   /* dense int32 tile for B <= dense_max (default 4096), sorted views above */
+  int32_t dense_max;   /* dense int32 tile for B <= dense_max, sorted views above; 0 (default):
+                          16384 with precision 3 (its proposals read whole tile rows), else 4096 */
   int32_t device;      /* CUDA device for usap_partition (ignored by contexts) */
   int32_t stats;       /* 1: per-kernel CUDA-event timings and algorithmic byte counts */
   int32_t trace_kinds; /* trace events to emit: bit k-1 for kind k; 0 = all kinds */

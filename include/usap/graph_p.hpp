@@ -52,7 +52,7 @@ class Graph_P {
   // B200 build
   uint64_t seed = 0;
   int init_mode = 0;
-  int dense_max = 4096;
+  int dense_max = 0;   // 0: automatic (usap_params.dense_max)
   int device = 0;
 
   explicit Graph_P(const std::string& FileName, size_t num_threads = 16) {

@@ -102,7 +102,7 @@ void usap_params_default(usap_params* p) {
   p->t_block_num = 20;
   p->seed = 0;
   p->init_mode = 0;
-  p->dense_max = 4096;
+  p->dense_max = 0;   // automatic: 4096, or 16384 with the float nodal dS (effective_dense_max)
   p->device = 0;
   p->stats = 0;
   p->persistent = 1;
@@ -322,12 +322,12 @@ usap_status usap_batch_partition(const usap_graph* graphs, int32_t ngraphs, cons
     // pool while other solves' kernels run, which is slow: reserve it now
     {
       int64_t want = 0;
-      const int64_t dmax = base.dense_max > 0 ? base.dense_max : 4096;
+      const int64_t dmax = usap::effective_dense_max(base);
       for (int32_t k = 0; k < std::min<int32_t>(W, njobs); k++) {
         const usap::HostGraph& hg = res[jobs[order[k]].graph]->hg;
         // initial blocks: one per vertex, or about N/7 from the SCC pass
         const int64_t b0 = base.init_mode == 1 ? hg.n : std::max<int64_t>(1, hg.n / 4);
-        want += usap::solve_footprint_bytes(hg.n, hg.e, std::min<int64_t>(dmax, b0), !hg.unit);
+        want += usap::solve_footprint_bytes(hg.n, hg.e, std::min<int64_t>(dmax, b0), !hg.unit, base.precision == 3);
       }
       usap::pool_reserve(device, want);
     }

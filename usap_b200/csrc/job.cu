@@ -902,7 +902,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
   if (!(p.num_block_reduction_rate > 0.0f && p.num_block_reduction_rate < 1.0f))
     throw Error(USAP_ERR_INVALID, "num_block_reduction_rate must be in (0, 1)");
   if (p.precision < 0 || p.precision > 3) throw Error(USAP_ERR_INVALID, "precision must be 0, 1, 2 or 3");
-  const int dense_max = p.dense_max > 0 ? p.dense_max : 4096;
+  const int dense_max = effective_dense_max(p);
   auto t_start = std::chrono::steady_clock::now();
   std::memset(res, 0, sizeof(*res));
   const int32_t n = hg_->n;

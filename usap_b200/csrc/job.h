@@ -17,7 +17,14 @@
 namespace usap {
 
 // upper estimate of the device memory one solve holds (server.cpp)
-int64_t solve_footprint_bytes(int64_t n, int64_t e, int64_t dense_max, bool weighted);
+int64_t solve_footprint_bytes(int64_t n, int64_t e, int64_t dense_max, bool weighted, bool float_ds);
+// the largest B held as a dense tile: the caller's dense_max, or by default
+// 4096 (exact and FP32 modes) and 16384 with the float nodal dS, whose
+// proposals read whole rows (on sorted views that is a binary search per
+// block); 16384 blocks is a 2 GB tile pair
+inline int32_t effective_dense_max(const usap_params& p) {
+  return p.dense_max > 0 ? p.dense_max : (p.precision == 3 ? 16384 : 4096);
+}
 
 struct HostGraph {
   int32_t n = 0;

@@ -50,13 +50,16 @@ struct Request {
 // Upper estimate of the device memory one solve of a graph with n vertices
 // and e edges holds: the graph (edge list, both adjacency lists, edge
 // chunks, log table), the partition slots and per-vertex state, the sorted
-// views' sort buffers, and the dense tile for B <= dense_max.
-int64_t solve_footprint_bytes(int64_t n, int64_t e, int64_t dense_max, bool weighted) {
+// views' sort buffers, the dense tile for B <= dense_max, and with the
+// float nodal dS its per-batch term tables (two floats per cell, B <= 4096).
+int64_t solve_footprint_bytes(int64_t n, int64_t e, int64_t dense_max, bool weighted, bool float_ds) {
   const int64_t d = std::min(n, std::max<int64_t>(dense_max, 1));
   const int64_t graph = (weighted ? 48 : 32) * e + 64 * n + 8 * (e + 1);
   const int64_t state = 72 * n + 160 * n + 112 * e;
   const int64_t tile = 8 * (d + 4) * (d + 4) + 4 * d * ((d + 127) / 128 + 1);
-  return graph + state + tile + (8ll << 20);
+  const int64_t dt = std::min<int64_t>(d, 4096);
+  const int64_t tables = float_ds ? 8 * (dt + 4) * (dt + 4) : 0;
+  return graph + state + tile + tables + (8ll << 20);
 }
 
 class Server {
@@ -117,7 +120,7 @@ class Server {
         m = std::max<int64_t>(m, static_cast<int64_t>(std::max(g.src[i], g.dst[i])) - base);
       n = m + 1;
     }
-    r->bytes = solve_footprint_bytes(n, g.e, p.dense_max > 0 ? p.dense_max : 4096, g.weight != nullptr);
+    r->bytes = solve_footprint_bytes(n, g.e, effective_dense_max(p), g.weight != nullptr, p.precision == 3);
     if (r->bytes > budget_)
       throw Error(USAP_ERR_LIMIT, "request needs about " + std::to_string(r->bytes >> 20) +
                                       " MiB of device memory, more than the server's budget of " +

@@ -63,7 +63,9 @@ def test_served_budget_bounds_admission(api):
     them one by one and still finishes all; poll reports progress."""
     from usap_b200 import native as nat
     G = gen.generate(gen.config_c1(seed=1))
-    srv = api.Server(workers=4, memory_budget=250 << 20)
+    # one request's estimate is about 340 MiB in the default precision (its
+    # dense tile may reach 16384 blocks, here N=5000): one fits, two do not
+    srv = api.Server(workers=4, memory_budget=500 << 20)
     ts = [srv.submit(G.src, G.dst, None, G.n, params=nat.default_params(num_batch_nodal_update=10, seed=s))
           for s in range(3)]
     seen = None

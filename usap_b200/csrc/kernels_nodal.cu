@@ -483,48 +483,35 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
 // thread cannot spare.  For each k the lanes evaluate the terms
 // of their block, and the terms are then added to one float accumulator in
 // the reference's order -- lane after lane, and within a lane in the
-// reference's term order (float addition does not reassociate).  Zero
-// terms are skipped with branches that are uniform over the group (adding
-// a zero would not change the sum), so the serial chain is as long as the
-// number of non-zero terms.  Every lane returns the same value.  Rr, Rs,
+// reference's term order (float addition does not reassociate), through the
+// group's shared-memory buffer `buf` (ref32_accumulate).  Rounds whose four
+// rows are empty in every lane are skipped.  Every lane returns the same
+// value.  Rr, Rs,
 // Sr, Ss: M[r,r], M[r,s], M[s,r], M[s,s]; wor, wos: v's out-weight to
 // blocks r and s.
 constexpr int kRefK = 1;
 
+// One round of the chain: lane l's four terms (0 where the reference skips
+// a zero count) are staged in buf[4 l .. 4 l + 3] (buf: 4 G floats of the
+// group's shared memory, 16-byte aligned), and every lane then adds (or
+// subtracts) all 4 G of them to its copy of the accumulator in that order.
+// Adding a zero term leaves the float sum unchanged: the accumulator starts
+// at +0 and round-to-nearest never makes it -0, so x + 0 = x holds for every
+// value it takes (infinities and NaN included).  The loop has the same trip
+// count in every group, so the two half-warp groups of a warp run it in
+// step, one shared-memory broadcast load per four terms.
 template <int G>
 __device__ __forceinline__ float ref32_accumulate(const Grp<G>& g, float dS, float t0, float t1, float t2,
-                                                  float t3, bool sub) {
-  const int nz = (t0 != 0.0f ? 1 : 0) | (t1 != 0.0f ? 2 : 0) | (t2 != 0.0f ? 4 : 0) | (t3 != 0.0f ? 8 : 0);
-  unsigned m = g.ballot(nz != 0);
-  constexpr unsigned kAll = G == 32 ? 0xffffffffu : (1u << G) - 1u;
-  if (m == kAll) {
-    // every lane has a term: a straight chain (adding a zero term changes
-    // nothing), so the shuffles can be issued ahead of the additions
-#pragma unroll
-    for (int j = 0; j < G; j++) {
-      const float a0 = g.shfl(t0, j), a1 = g.shfl(t1, j), a2 = g.shfl(t2, j), a3 = g.shfl(t3, j);
-      if (sub) dS = __fsub_rn(__fsub_rn(__fsub_rn(__fsub_rn(dS, a0), a1), a2), a3);
-      else dS = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(dS, a0), a1), a2), a3);
-    }
-    return dS;
+                                                  float t3, bool sub, float* buf) {
+  reinterpret_cast<float4*>(buf)[g.gl] = make_float4(t0, t1, t2, t3);
+  g.sync();
+#pragma unroll 4
+  for (int j = 0; j < G; j++) {
+    const float4 q = reinterpret_cast<const float4*>(buf)[j];
+    if (sub) dS = __fsub_rn(__fsub_rn(__fsub_rn(__fsub_rn(dS, q.x), q.y), q.z), q.w);
+    else dS = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(dS, q.x), q.y), q.z), q.w);
   }
-  while (m) {
-    const int j = __ffs(m) - 1;
-    m &= m - 1;
-    const int nzj = g.shfl(nz, j);
-    const float a0 = g.shfl(t0, j), a1 = g.shfl(t1, j), a2 = g.shfl(t2, j), a3 = g.shfl(t3, j);
-    if (sub) {
-      if (nzj & 1) dS = __fsub_rn(dS, a0);
-      if (nzj & 2) dS = __fsub_rn(dS, a1);
-      if (nzj & 4) dS = __fsub_rn(dS, a2);
-      if (nzj & 8) dS = __fsub_rn(dS, a3);
-    } else {
-      if (nzj & 1) dS = __fadd_rn(dS, a0);
-      if (nzj & 2) dS = __fadd_rn(dS, a1);
-      if (nzj & 4) dS = __fadd_rn(dS, a2);
-      if (nzj & 8) dS = __fadd_rn(dS, a3);
-    }
-  }
+  g.sync();   // the next round overwrites buf
   return dS;
 }
 
@@ -536,7 +523,7 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
                                           const float* Tcol, int tld, int r, int s, int dr_out, int dr_in,
                                           int ds_out, int ds_in, int kout, int kin, int Rr, int Rs, int Sr, int Ss,
                                           int wor, int wos, const int* key, const int* two, const int* twi, int cap,
-                                          int lg) {
+                                          int lg, float* buf) {
   using LDT = typename Ops::LdT;
   const Grp<G> g(static_cast<int>(threadIdx.x & 31));
   const int B = ops.B;
@@ -559,7 +546,7 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
         t[k][3] = col ? __ldcg(cs + i) : 0.0f;
       }
 #pragma unroll
-      for (int k = 0; k < kRefK; k++) dS = ref32_accumulate<G>(g, dS, t[k][0], t[k][1], t[k][2], t[k][3], false);
+      for (int k = 0; k < kRefK; k++) dS = ref32_accumulate<G>(g, dS, t[k][0], t[k][1], t[k][2], t[k][3], false, buf);
     }
   }
   for (int base = 0; !Trow && base < B; base += kRefK * G) {
@@ -591,7 +578,7 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
       const float t1 = S[k] ? ref_term(S[k], static_cast<long long>(di[k]) * ds_out) : 0.0f;
       const float t2 = Rc[k] ? ref_term(Rc[k], static_cast<long long>(dn[k]) * dr_in) : 0.0f;
       const float t3 = Sc[k] ? ref_term(Sc[k], static_cast<long long>(dn[k]) * ds_in) : 0.0f;
-      dS = ref32_accumulate<G>(g, dS, t0, t1, t2, t3, false);
+      dS = ref32_accumulate<G>(g, dS, t0, t1, t2, t3, false, buf);
     }
   }
   const int dor_n = dr_out - kout, dos_n = ds_out + kout;
@@ -639,7 +626,7 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
       const float u1 = S[k] ? ref_term(S[k], static_cast<long long>(di[k]) * dos_n) : 0.0f;
       const float u2 = Rc[k] ? ref_term(Rc[k], static_cast<long long>(dn[k]) * dir_n) : 0.0f;
       const float u3 = Sc[k] ? ref_term(Sc[k], static_cast<long long>(dn[k]) * dis_n) : 0.0f;
-      dS = ref32_accumulate<G>(g, dS, u0, u1, u2, u3, true);
+      dS = ref32_accumulate<G>(g, dS, u0, u1, u2, u3, true, buf);
     }
   }
   return dS;
@@ -890,7 +877,7 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
                             static_cast<int>(ds_out), static_cast<int>(ds_in), static_cast<int>(vi.kout),
                             static_cast<int>(vi.kin), static_cast<int>(Rr), static_cast<int>(Rs),
                             static_cast<int>(Sr), static_cast<int>(Ss), static_cast<int>(wor),
-                            static_cast<int>(wos), key, two, twi, cap, lg);
+                            static_cast<int>(wos), key, two, twi, cap, lg, reinterpret_cast<float*>(list));
   if (g.gl == 0) {
     const bool moved = emit<Ops::kP>(a, v, r, s, acc, f, ninf);
     tally<Ops::kP>(tl, moved, acc, f, ninf);
@@ -916,7 +903,7 @@ __global__ void __launch_bounds__(kThreads, 5) k_nodal_propose(NodalArgs a, Ops 
   __shared__ int s_key[kWarps][kHCap];
   __shared__ int s_wo[kWarps][kHCap];
   __shared__ int s_wi[kWarps][kHCap];
-  __shared__ int s_list[kWarps][kHubDegree];   // occupied slots other than r, s
+  __shared__ __align__(16) int s_list[kWarps][kHubDegree];   // occupied slots other than r, s; then the float dS's terms
   __shared__ CtaTally s_tally;
   if (a.ctl->done) return;   // written by earlier launches only
   const uint32_t itr = static_cast<uint32_t>(a.ctl->itr);
@@ -939,6 +926,7 @@ struct HubShared {
   int sum[5][NW];
   float fhi[NW], flo[NW];   // FP32 partial sums (precision modes 1, 2)
   int target, scanned;
+  __align__(16) float chain[128];   // precision 3: the float dS's staged terms (warp 0)
 };
 
 // Proposal for one vertex of degree > kHubDegree by a whole CTA of NT
@@ -1098,7 +1086,7 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
                                static_cast<int>(ds_out), static_cast<int>(ds_in), static_cast<int>(vi.kout),
                                static_cast<int>(vi.kin), static_cast<int>(Rr), static_cast<int>(Rs),
                                static_cast<int>(Sr), static_cast<int>(Ss), static_cast<int>(wor),
-                               static_cast<int>(wos), key, two, twi, cap, lg);
+                               static_cast<int>(wos), key, two, twi, cap, lg, sh->chain);
     if (lane == 0) {
       tally_ctl<Ops::kP>(a.ctl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
       if (a.stats)
@@ -1113,7 +1101,7 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
 template <class Ops>
 __global__ void __launch_bounds__(kHubThreads) k_nodal_propose_hub(NodalArgs a, Ops ops, const int32_t* hubs,
                                                                   int hub_lo, int hub_hi, int smem_cap) {
-  extern __shared__ int dyn[];
+  extern __shared__ __align__(16) int dyn[];
   __shared__ HubShared<kHubWarps> sh;
   if (a.ctl->done) return;
   const uint32_t itr = static_cast<uint32_t>(a.ctl->itr);
@@ -1777,7 +1765,7 @@ __device__ __forceinline__ void ref32_tables_pass(int B, int ld, const int* M, c
 
 template <int P, bool kSnap>
 __global__ void __launch_bounds__(kPThreads, 1) k_nodal_phase(PhaseArgs p) {
-  extern __shared__ int dyn[];
+  extern __shared__ __align__(16) int dyn[];
   __shared__ CtaTally s_tally;
   __shared__ HubShared<kPWarps> sh;
   __shared__ int s_base, s_state;
@@ -2056,7 +2044,7 @@ __device__ __forceinline__ void job_prefix(long long v, long long* tmp, long lon
 template <int P>
 __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __restrict__ jobs, int K, GangCtl* gc,
                                                              int exit_below) {
-  extern __shared__ int dyn[];
+  extern __shared__ __align__(16) int dyn[];
   __shared__ CtaTally s_tally[kGangMax];
   __shared__ HubShared<kPWarps> sh;
   __shared__ int s_bi[kGangMax], s_sw[kGangMax], s_act[kGangMax], s_nb[kGangMax];

@@ -282,7 +282,10 @@ def precision_sample(ctx, G, local_rank: int, seeds16=tuple(range(16)), seeds5=(
     for mode, seeds in ((3, seeds16), (0, seeds16), (1, seeds5), (2, seeds5)):
         runs = []
         for seed in seeds:
-            p = nat.default_params(num_batch_nodal_update=10, seed=seed, precision=mode, device=local_rank)
+            # (mode 3 with its FP64 shadow on, for the flip counts: the
+            # same solve, the shadow decides nothing)
+            p = nat.default_params(num_batch_nodal_update=10, seed=seed, precision=mode, device=local_rank,
+                                   fp64_shadow=1 if mode == 3 else 0)
             part, r = ctx.partition(p)
             run = {"seed": seed, "ms": r["ms_total"], "B": r["B"], "S": r["S"],
                    "nmi": api.evaluate(G.truth, part)["nmi"], "sweeps": r["sweeps"]}

@@ -107,7 +107,11 @@ typedef struct usap_params {
                           (mode 0, or the reference itself compiled with double) ends at fewer
                           blocks on large graphs.  usap_result.fp32_* compare it with the exact
                           value. */
-  int32_t reserved[1];
+  int32_t fp64_shadow; /* precision 3 only: 1 = also evaluate the exact FP64 value of every nodal
+                          dS beside the float one and report the flipped decisions and errors in
+                          usap_result.fp32_*; 0 (default) = skip that evaluation (it decides
+                          nothing in precision 3) and leave fp32_* at 0.  The other precisions
+                          always evaluate it. */
 } usap_params;
 
 typedef struct usap_result {
@@ -117,7 +121,8 @@ typedef struct usap_result {
   int64_t S_q;             /* the same in Q32 fixed point, saturated beyond +-2^31 */
   int64_t sweeps, batches;
   int64_t nodal_proposals, nodal_moves;
-  int64_t near_threshold;  /* nodal proposals with |dS| <= 1e-9 */
+  int64_t near_threshold;  /* nodal proposals with |dS| <= 1e-9 (the deciding value: exact, or
+                              the float dS in precision 3) */
   int64_t merge_shortfall; /* merges the merge order could not supply */
   int64_t edge_visits;     /* sum over proposing vertices of in+out degree */
   double ms_total, ms_init, ms_merge, ms_nodal, ms_h2d, ms_d2h;

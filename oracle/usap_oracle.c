@@ -930,7 +930,9 @@ int32_t og_merge_apply(int32_t n, int32_t* part, int32_t B, const int32_t* best_
 /* nodal_move + update tasks for one batch (:397-443).  precision 3: the
  * accept decision is the reference's float dS < 0 (-inf included), and the
  * accepted float values are what the convergence sums add (:428-430), in
- * Q32; the exact value still gives prop_q and the near-threshold count.
+ * Q32; the exact value still gives prop_q.  The near-threshold count is
+ * of the deciding value: |dS| <= 1e-9 exactly, or the float dS in
+ * precision 3.
  * prop_f (optional) receives the float dS of each proposal.               */
 typedef struct {
   const og_graph* g;
@@ -957,12 +959,13 @@ static void og_nodal_item(void* ctx, int32_t i, int32_t w) {
   int accept = 0;
   if (s != r) {
     q = og_nodal_dq(t->g, t->part, t->b, v, s, &ninf);
-    if (!ninf && (q <= OG_NEAR_Q && q >= -OG_NEAR_Q)) t->nnear[w]++;
     if (t->precision == 3) {
       f = og_nodal_ds_ref32(t->g, t->part, t->b, v, s);
       accept = f < 0.0f;
+      if (!isinf(f) && fabs((double)f) <= 1e-9) t->nnear[w]++;
     } else {
       accept = ninf || q < 0;
+      if (!ninf && (q <= OG_NEAR_Q && q >= -OG_NEAR_Q)) t->nnear[w]++;
     }
   }
   if (t->prop_s) t->prop_s[i] = (s != r) ? s : -1;

@@ -99,24 +99,28 @@ def _solve_pair(api, oracle, n, src, dst, w, params, persistent=1):
     ctx.set_trace(None)
     ctx.close()
     og = oracle.OracleGraph(n, src, dst, w)
-    oparams = {k: v for k, v in params.items() if k != "dense_max"}
+    oparams = {k: v for k, v in params.items() if k not in ("dense_max", "fp64_shadow")}
     part_o, res_o, ev_o = og.partition(oparams, trace=True)
     return part_g, res_g, ev_gpu, part_o, res_o, ev_o
 
 
 @pytest.mark.parametrize("graph,params,persistent", [
     ("c0", {"num_batch_nodal_update": 10, "seed": 0}, 1),
+    ("c0", {"num_batch_nodal_update": 10, "seed": 0, "fp64_shadow": 1}, 1),
     ("c0", {"num_batch_nodal_update": 10, "seed": 0}, 0),
     ("c0", {"num_batch_nodal_update": 4, "seed": 3, "dense_max": 16}, 1),
     ("weighted", {"num_batch_nodal_update": 7, "seed": 2}, 1),
     ("hub", {"num_batch_nodal_update": 10, "seed": 9}, 1),
+    ("hub", {"num_batch_nodal_update": 10, "seed": 9, "fp64_shadow": 1}, 1),
     ("hub", {"num_batch_nodal_update": 10, "seed": 9, "dense_max": 32}, 0),
+    ("hub", {"num_batch_nodal_update": 10, "seed": 9, "dense_max": 32, "fp64_shadow": 1}, 0),
 ])
 def test_ref32_full_solve_trace_exact(api, oracle, graph, params, persistent):
     """Whole solves in mode 3: every trace event (after each merge, batch
     and stage), the final partition, B, S and the counters equal the
     oracle's; persistent and per-batch schedules, dense tile and sorted
-    views."""
+    views, with and without the FP64 shadow evaluation (which decides
+    nothing in mode 3 and only adds the flip counts)."""
     params = dict(params, precision=3)
     n, src, dst, w = GRAPHS[graph]()
     part_g, res_g, ev_g, part_o, res_o, ev_o = _solve_pair(api, oracle, n, src, dst, w, params, persistent)
@@ -128,9 +132,13 @@ def test_ref32_full_solve_trace_exact(api, oracle, graph, params, persistent):
         assert a == b, (graph, i, a, b)
     assert np.array_equal(part_g, part_o)
     for k in ("B", "S_q", "stages", "sweeps", "batches", "nodal_proposals", "nodal_moves",
-              "merge_shortfall"):
+              "merge_shortfall", "near_threshold"):
         assert res_g[k] == res_o[k], k
-    assert res_g["fp32_nodal_evals"] > 0
+    if params.get("fp64_shadow"):
+        assert res_g["fp32_nodal_evals"] > 0
+        assert res_g["fp32_flip_rate"] == res_g["fp32_nodal_flips"] / res_g["fp32_nodal_evals"]
+    else:
+        assert res_g["fp32_nodal_evals"] == 0 and res_g["fp32_nodal_flips"] == 0
 
 
 @pytest.mark.parametrize("within,alpha,seed", [(0.8, 10.0, 0), (0.5, 1.0, 1), (0.8, 1.0, 2),

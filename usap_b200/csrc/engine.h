@@ -217,6 +217,7 @@ struct NodalArgs {
   int32_t *hkey, *hwo, *hwi;
   int stats;
   int prec;               // precision mode: 0 FP64; 1, 2 decide on the FP32 dS; 3 the reference's float dS
+  int shadow;             // precision 3: also evaluate the exact FP64 dS (flip counts, replay)
   const float2* L2;       // the log table as float pairs (precision modes 1, 2)
   // precision mode 3, persistent kernel: the reference's old-state terms of
   // every tile cell, recomputed at each batch start (null: computed per

@@ -641,6 +641,7 @@ NodalArgs Job::nodal_args(int32_t* part, int32_t B, int32_t beg, int32_t end, ui
   a.hwi = g_.hwi;
   a.stats = stats;
   a.prec = prec_;
+  a.shadow = prec_ != 3 || shadow_ || stats == 2 ? 1 : 0;
   a.L2 = g_.logk2;
   a.Trow = nullptr;
   a.Tcol = nullptr;
@@ -918,6 +919,7 @@ void Job::partition(const usap_params& p, int32_t* out_assign, usap_result* res,
   const LaunchCount lc0 = launch_count();
   long long d2h = 0;
   prec_ = p.precision;
+  shadow_ = p.fp64_shadow != 0;
   F32Tally nodal32{0, 0, 0, 0.0};   // summed over the stages' nodal phases
   if (prec_) USAP_CUDA(cudaMemsetAsync(f32d_, 0, 2 * sizeof(F32Tally), st_));
 

@@ -343,6 +343,7 @@ class Job {
   // precision mode of the current solve; with modes 1, 2: [0] merge
   // proposals, [1].flips merge-order inversions
   int prec_ = 0;
+  bool shadow_ = false;   // precision 3: evaluate the exact FP64 dS beside the float one
   // the merge phase's mode: mode 3 changes only the nodal dS (the
   // reference's float merge dS does not move its solve) and keeps merges exact
   int merge_prec() const { return prec_ == 3 ? 0 : prec_; }

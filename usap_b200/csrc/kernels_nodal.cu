@@ -680,6 +680,14 @@ struct CtaTally {
 // the accepted dS that the convergence test sums: the exact value, or in
 // precision mode 3 the reference's float value (its update task sums the
 // float dS it accepted, graph_parallel.hpp:428-434), in Q32
+// |dS| <= 1e-9 for the value that decides: the exact one (Q32), or in
+// precision 3 the float one
+template <int P>
+__device__ __forceinline__ bool near_threshold(long long acc, double f, int ninf) {
+  if constexpr (P == 3) return !isinf(f) && fabs(f) <= 1e-9;
+  return !ninf && acc <= kNearQ && acc >= -kNearQ;
+}
+
 template <int P>
 __device__ __forceinline__ long long summed_dq(long long acc, double f) {
   if constexpr (P == 3) return q32(f);
@@ -687,29 +695,30 @@ __device__ __forceinline__ long long summed_dq(long long acc, double f) {
 }
 
 template <int P>
-__device__ __forceinline__ void tally(CtaTally* t, bool accept, long long acc, double f, int ninf) {
+__device__ __forceinline__ void tally(CtaTally* t, bool accept, long long acc, double f, int ninf, bool shadow) {
   if (accept) {
     if (ninf) atomicOr(&t->ninf, 1);
     else atomicAdd(&t->cum, static_cast<unsigned long long>(summed_dq<P>(acc, f)));
     atomicAdd(&t->moves, 1ull);
   }
-  if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&t->near, 1ull);
+  if (near_threshold<P>(acc, f, ninf)) atomicAdd(&t->near, 1ull);
   if constexpr (P > 0) {
-    if (!ninf) f32_tally(&t->f32, f, acc);
+    if (shadow && !ninf) f32_tally(&t->f32, f, acc);
   }
 }
 
 // the same straight into the control block (one proposal per CTA)
 template <int P>
-__device__ __forceinline__ void tally_ctl(NodalCtl* c, bool accept, long long acc, double f, int ninf) {
+__device__ __forceinline__ void tally_ctl(NodalCtl* c, bool accept, long long acc, double f, int ninf,
+                                          bool shadow) {
   if (accept) {
     if (ninf) atomicOr(&c->cum_ninf, 1);
     else atomicAdd(&c->cum_q, static_cast<unsigned long long>(summed_dq<P>(acc, f)));
     atomicAdd(&c->moves, 1ull);
   }
-  if (!ninf && acc <= kNearQ && acc >= -kNearQ) atomicAdd(&c->near, 1ull);
+  if (near_threshold<P>(acc, f, ninf)) atomicAdd(&c->near, 1ull);
   if constexpr (P > 0) {
-    if (!ninf) f32_tally(&c->f32, f, acc);
+    if (shadow && !ninf) f32_tally(&c->f32, f, acc);
   }
 }
 
@@ -813,74 +822,90 @@ __device__ __forceinline__ void group_vertex(const NodalArgs& a, const Ops& ops,
   const long long ds_out = LDT::ld(a.dout + s), ds_in = LDT::ld(a.din + s);
   int e4 = 0;
   if (g.gl < 4) e4 = ops.get(g.gl < 2 ? r : s, (g.gl & 1) ? s : r);
-  const DegLogs dl = deg_logs<Ops::kP>(a, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
-  // compact the occupied slots so that each lane takes about one block
-  int nlist = 0, noccupied = 0;
-  for (int base = 0; base < cap; base += G) {
-    const int i = base + g.gl;
-    const int b = i < cap ? key[i] : -1;
-    const unsigned occ = g.ballot(b >= 0);
-    const bool use = b >= 0 && b != r && b != s;
-    const unsigned mu = g.ballot(use);
-    if (use) list[nlist + __popc(mu & lanes_below)] = i;
-    nlist += __popc(mu);
-    noccupied += __popc(occ);
-  }
-  g.sync();
-  // each lane has at most four slots (nlist <= 4 * G): their M entries
-  // and degrees are loaded in two rounds of two, then the log terms
-  TermSums ts{0, 0, 0, 0, 0};
+  // the exact FP64 dS (decides in precision 0; in the others the shadow
+  // value the FP32 decision is compared with, skipped in precision 3
+  // unless asked for)
+  const bool shadow = Ops::kP != 3 || a.shadow;
+  int ninf = 0, noccupied = 0;
+  double f = 0.0;
+  long long acc = 0;
+  if (shadow) {
+    const DegLogs dl = deg_logs<Ops::kP>(a, dr_out, dr_in, ds_out, ds_in, vi.kout, vi.kin);
+    // compact the occupied slots so that each lane takes about one block
+    int nlist = 0;
+    for (int base = 0; base < cap; base += G) {
+      const int i = base + g.gl;
+      const int b = i < cap ? key[i] : -1;
+      const unsigned occ = g.ballot(b >= 0);
+      const bool use = b >= 0 && b != r && b != s;
+      const unsigned mu = g.ballot(use);
+      if (use) list[nlist + __popc(mu & lanes_below)] = i;
+      nlist += __popc(mu);
+      noccupied += __popc(occ);
+    }
+    g.sync();
+    // each lane has at most four slots (nlist <= 4 * G): their M entries
+    // and degrees are loaded in two rounds of two, then the log terms
+    TermSums ts{0, 0, 0, 0, 0};
 #pragma unroll
-  for (int k0 = 0; k0 < 4; k0 += 2) {
-    int R[2], S[2], Rc[2], Sc[2], Di[2], Do[2], wo[2], wi[2];
+    for (int k0 = 0; k0 < 4; k0 += 2) {
+      int R[2], S[2], Rc[2], Sc[2], Di[2], Do[2], wo[2], wi[2];
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-      const int t = g.gl + G * (k0 + k);
-      R[k] = S[k] = Rc[k] = Sc[k] = Di[k] = Do[k] = wo[k] = wi[k] = 0;
-      if (t < nlist) {
-        const int i = list[t];
-        const int b = key[i];
-        wo[k] = two[i];
-        wi[k] = twi[i];
-        if (wo[k] > 0) {
-          R[k] = ops.get(r, b);
-          S[k] = ops.get(s, b);
-          Di[k] = LDT::ld(a.din + b);
-        }
-        if (wi[k] > 0) {
-          Rc[k] = ops.get(b, r);
-          Sc[k] = ops.get(b, s);
-          Do[k] = LDT::ld(a.dout + b);
+      for (int k = 0; k < 2; k++) {
+        const int t = g.gl + G * (k0 + k);
+        R[k] = S[k] = Rc[k] = Sc[k] = Di[k] = Do[k] = wo[k] = wi[k] = 0;
+        if (t < nlist) {
+          const int i = list[t];
+          const int b = key[i];
+          wo[k] = two[i];
+          wi[k] = twi[i];
+          if (wo[k] > 0) {
+            R[k] = ops.get(r, b);
+            S[k] = ops.get(s, b);
+            Di[k] = LDT::ld(a.din + b);
+          }
+          if (wi[k] > 0) {
+            Rc[k] = ops.get(b, r);
+            Sc[k] = ops.get(b, s);
+            Do[k] = LDT::ld(a.dout + b);
+          }
         }
       }
-    }
 #pragma unroll
-    for (int k = 0; k < 2; k++)
-      slot_terms_vals<Ops::kP>(a, R[k], S[k], Rc[k], Sc[k], Di[k], Do[k], wo[k], wi[k], dl, ts);
+      for (int k = 0; k < 2; k++)
+        slot_terms_vals<Ops::kP>(a, R[k], S[k], Rc[k], Sc[k], Di[k], Do[k], wo[k], wi[k], dl, ts);
+    }
+    ts.acc = g.sum(ts.acc);
+    ts.sXR = g.sum(ts.sXR);
+    ts.sXS = g.sum(ts.sXS);
+    ts.sYR = g.sum(ts.sYR);
+    ts.sYS = g.sum(ts.sYS);
+    const long long Rr = g.shfl(e4, 0), Rs = g.shfl(e4, 1);
+    const long long Sr = g.shfl(e4, 2), Ss = g.shfl(e4, 3);
+    const long long wor = table_lookup_wo(key, two, cap, lg, r);
+    const long long wos = table_lookup_wo(key, two, cap, lg, s);
+    acc = finalize_grp<G, Ops::kP>(a, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out, ds_in, vi.kout,
+                                   vi.kin, &ninf, ts.f, &f);
   }
-  ts.acc = g.sum(ts.acc);
-  ts.sXR = g.sum(ts.sXR);
-  ts.sXS = g.sum(ts.sXS);
-  ts.sYR = g.sum(ts.sYR);
-  ts.sYS = g.sum(ts.sYS);
-  const long long Rr = g.shfl(e4, 0), Rs = g.shfl(e4, 1);
-  const long long Sr = g.shfl(e4, 2), Ss = g.shfl(e4, 3);
-  const long long wor = table_lookup_wo(key, two, cap, lg, r);
-  const long long wos = table_lookup_wo(key, two, cap, lg, s);
-  int ninf;
-  double f = 0.0;
-  const long long acc = finalize_grp<G, Ops::kP>(a, g, ts, Rr, Rs, Sr, Ss, wor, wos, dr_out, dr_in, ds_out,
-                                                 ds_in, vi.kout, vi.kin, &ninf, ts.f, &f);
-  if constexpr (Ops::kP == 3)
+  if constexpr (Ops::kP == 3) {
+    const int Rr = g.shfl(e4, 0), Rs = g.shfl(e4, 1);
+    const int Sr = g.shfl(e4, 2), Ss = g.shfl(e4, 3);
+    const int wor = table_lookup_wo(key, two, cap, lg, r);
+    const int wos = table_lookup_wo(key, two, cap, lg, s);
     f = ref32_nodal<Ops, G>(ops, a.din, a.dout, a.Trow, a.Tcol, a.tld, r, s, static_cast<int>(dr_out),
                             static_cast<int>(dr_in),
                             static_cast<int>(ds_out), static_cast<int>(ds_in), static_cast<int>(vi.kout),
                             static_cast<int>(vi.kin), static_cast<int>(Rr), static_cast<int>(Rs),
                             static_cast<int>(Sr), static_cast<int>(Ss), static_cast<int>(wor),
                             static_cast<int>(wos), key, two, twi, cap, lg, reinterpret_cast<float*>(list));
+    // without the shadow the -inf of a new-state term x log(x / 0) comes
+    // from the float sum itself (the term is +inf there, and every new-state
+    // term is subtracted)
+    if (!shadow) ninf = isinf(f) && f < 0.0 ? 1 : 0;
+  }
   if (g.gl == 0) {
     const bool moved = emit<Ops::kP>(a, v, r, s, acc, f, ninf);
-    tally<Ops::kP>(tl, moved, acc, f, ninf);
+    tally<Ops::kP>(tl, moved, acc, f, ninf, shadow);
     if (moved && tl->own) {
       const int nch = deg > 32 ? (deg + 31) >> 5 : 1;   // the vertex's chunks (one even without edges)
       const int i0 = atomicAdd(tl->nown, nch);
@@ -1087,8 +1112,13 @@ __device__ __forceinline__ void hub_vertex(const NodalArgs& a, const Ops& ops, i
                                static_cast<int>(vi.kin), static_cast<int>(Rr), static_cast<int>(Rs),
                                static_cast<int>(Sr), static_cast<int>(Ss), static_cast<int>(wor),
                                static_cast<int>(wos), key, two, twi, cap, lg, sh->chain);
+    // (a hub's exact value is a CTA-parallel sum over its slots and is
+    // always evaluated; without the shadow it is not reported, as for the
+    // other vertices)
+    const bool shadow = Ops::kP != 3 || a.shadow;
+    if (!shadow) ninf = isinf(f) && f < 0.0 ? 1 : 0;
     if (lane == 0) {
-      tally_ctl<Ops::kP>(a.ctl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf);
+      tally_ctl<Ops::kP>(a.ctl, emit<Ops::kP>(a, v, r, s, acc, f, ninf), acc, f, ninf, shadow);
       if (a.stats)
         *my_bytes += 8 + 8ull * deg + 48ull * occ + 48 + 8ull * sh->scanned + (Ops::kP == 3 ? 48ull * a.B : 0ull);
     }

@@ -44,7 +44,7 @@ class Params(C.Structure):
                 ("init_mode", C.c_int32), ("dense_max", C.c_int32), ("device", C.c_int32),
                 ("stats", C.c_int32), ("trace_kinds", C.c_int32), ("sweep_graphs", C.c_int32),
                 ("persistent", C.c_int32), ("persistent_ctas", C.c_int32),
-                ("precision", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("precision", C.c_int32), ("fp64_shadow", C.c_int32)]
 
 
 class Result(C.Structure):

@@ -476,12 +476,10 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
 //  3. the new terms of rows and columns for i not in {r, s} (:1196-1215),
 //     the entries adjusted by v's out-weight (rows) and in-weight (columns)
 //     towards block i, looked up in the group's neighbour-block table.
-// A round covers kRefK * G blocks: lane l loads the entries of blocks
-// base + k G + l (k < kRefK) of the four rows at once.  kRefK = 1 measured
-// fastest on the N=50000 solve (450 ms against 657 ms with 4 and 591 ms
-// with 2): deeper rounds hold registers that the persistent kernel's 80 per
-// thread cannot spare.  For each k the lanes evaluate the terms
-// of their block, and the terms are then added to one float accumulator in
+// A round covers G blocks: lane l loads the entries of block base + l of
+// the four rows (the next round's loads are issued before this round's
+// terms are evaluated).  The lanes evaluate the terms of their block, and
+// the terms are then added to one float accumulator in
 // the reference's order -- lane after lane, and within a lane in the
 // reference's term order (float addition does not reassociate), through the
 // group's shared-memory buffer `buf` (ref32_accumulate).  Rounds whose four
@@ -489,8 +487,6 @@ __device__ __forceinline__ long long finalize_grp(const NodalArgs& a, const Grp<
 // value.  Rr, Rs,
 // Sr, Ss: M[r,r], M[r,s], M[s,r], M[s,s]; wor, wos: v's out-weight to
 // blocks r and s.
-constexpr int kRefK = 1;
-
 // One round of the chain: lane l's four terms (0 where the reference skips
 // a zero count) are staged in buf[4 l .. 4 l + 3] (buf: 4 G floats of the
 // group's shared memory, 16-byte aligned), and every lane then adds (or
@@ -528,56 +524,56 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
   const Grp<G> g(static_cast<int>(threadIdx.x & 31));
   const int B = ops.B;
   float dS = 0.0f;
+  // Every round first issues the loads of the next round (pure reads of the
+  // batch-start state), so that their L2 latency overlaps this round's
+  // terms and chain.
   if (Trow) {
     // the old-state terms from the batch's tables (written in this launch: L2 loads)
     const float* tr = Trow + static_cast<long long>(r) * tld;
     const float* ts = Trow + static_cast<long long>(s) * tld;
     const float* cr = Tcol + static_cast<long long>(r) * tld;
     const float* cs = Tcol + static_cast<long long>(s) * tld;
-    for (int base = 0; base < B; base += kRefK * G) {
-      float t[kRefK][4];
-#pragma unroll
-      for (int k = 0; k < kRefK; k++) {
-        const int i = base + k * G + g.gl;
-        const bool in = i < B, col = in && i != r && i != s;
-        t[k][0] = in ? __ldcg(tr + i) : 0.0f;
-        t[k][1] = in ? __ldcg(ts + i) : 0.0f;
-        t[k][2] = col ? __ldcg(cr + i) : 0.0f;
-        t[k][3] = col ? __ldcg(cs + i) : 0.0f;
-      }
-#pragma unroll
-      for (int k = 0; k < kRefK; k++) dS = ref32_accumulate<G>(g, dS, t[k][0], t[k][1], t[k][2], t[k][3], false, buf);
+    float n0, n1, n2, n3;
+    auto tload = [&](int i) {
+      const bool in = i < B, col = in && i != r && i != s;
+      n0 = in ? __ldcg(tr + i) : 0.0f;
+      n1 = in ? __ldcg(ts + i) : 0.0f;
+      n2 = col ? __ldcg(cr + i) : 0.0f;
+      n3 = col ? __ldcg(cs + i) : 0.0f;
+    };
+    tload(g.gl);
+    for (int base = 0; base < B; base += G) {
+      const float t0 = n0, t1 = n1, t2 = n2, t3 = n3;
+      tload(base + G + g.gl);
+      dS = ref32_accumulate<G>(g, dS, t0, t1, t2, t3, false, buf);
     }
   }
-  for (int base = 0; !Trow && base < B; base += kRefK * G) {
-    int R[kRefK], S[kRefK], Rc[kRefK], Sc[kRefK];
-#pragma unroll
-    for (int k = 0; k < kRefK; k++) {
-      const int i = base + k * G + g.gl;
-      R[k] = S[k] = Rc[k] = Sc[k] = 0;
+  // a round's entries of rows r, s (R, S), columns r, s (Rc, Sc) and the
+  // degrees of its block (d_in: di, d_out: dn)
+  int nR, nS, nRc, nSc, ndi, ndn;
+  if (!Trow) {
+    auto oload = [&](int i) {
+      nR = nS = nRc = nSc = ndi = ndn = 0;
       if (i < B) {
-        R[k] = ops.get(r, i);
-        S[k] = ops.get(s, i);
+        nR = ops.get(r, i);
+        nS = ops.get(s, i);
         if (i != r && i != s) {   // columns skip i in {r, s}
-          Rc[k] = ops.get_t(r, i);
-          Sc[k] = ops.get_t(s, i);
+          nRc = ops.get_t(r, i);
+          nSc = ops.get_t(s, i);
         }
+        ndi = LDT::ld(din_p + i);
+        ndn = LDT::ld(dout_p + i);
       }
-    }
-    int di[kRefK], dn[kRefK];
-#pragma unroll
-    for (int k = 0; k < kRefK; k++) {
-      const int i = base + k * G + g.gl;
-      di[k] = (R[k] | S[k]) ? LDT::ld(din_p + i) : 0;
-      dn[k] = (Rc[k] | Sc[k]) ? LDT::ld(dout_p + i) : 0;
-    }
-#pragma unroll
-    for (int k = 0; k < kRefK; k++) {
-      if (!g.any((R[k] | S[k] | Rc[k] | Sc[k]) != 0)) continue;
-      const float t0 = R[k] ? ref_term(R[k], static_cast<long long>(di[k]) * dr_out) : 0.0f;
-      const float t1 = S[k] ? ref_term(S[k], static_cast<long long>(di[k]) * ds_out) : 0.0f;
-      const float t2 = Rc[k] ? ref_term(Rc[k], static_cast<long long>(dn[k]) * dr_in) : 0.0f;
-      const float t3 = Sc[k] ? ref_term(Sc[k], static_cast<long long>(dn[k]) * ds_in) : 0.0f;
+    };
+    oload(g.gl);
+    for (int base = 0; base < B; base += G) {
+      const int R = nR, S = nS, Rc = nRc, Sc = nSc, di = ndi, dn = ndn;
+      oload(base + G + g.gl);
+      if (!g.any((R | S | Rc | Sc) != 0)) continue;
+      const float t0 = R ? ref_term(R, static_cast<long long>(di) * dr_out) : 0.0f;
+      const float t1 = S ? ref_term(S, static_cast<long long>(di) * ds_out) : 0.0f;
+      const float t2 = Rc ? ref_term(Rc, static_cast<long long>(dn) * dr_in) : 0.0f;
+      const float t3 = Sc ? ref_term(Sc, static_cast<long long>(dn) * ds_in) : 0.0f;
       dS = ref32_accumulate<G>(g, dS, t0, t1, t2, t3, false, buf);
     }
   }
@@ -588,46 +584,40 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
   if (rr_s) dS = __fsub_rn(dS, ref_term(rr_s, static_cast<long long>(dis_n) * dor_n));
   if (sr_r) dS = __fsub_rn(dS, ref_term(sr_r, static_cast<long long>(dir_n) * dos_n));
   if (sr_s) dS = __fsub_rn(dS, ref_term(sr_s, static_cast<long long>(dis_n) * dos_n));
-  for (int base = 0; base < B; base += kRefK * G) {
-    int R[kRefK], S[kRefK], Rc[kRefK], Sc[kRefK];
-#pragma unroll
-    for (int k = 0; k < kRefK; k++) {
-      const int i = base + k * G + g.gl;
-      R[k] = S[k] = Rc[k] = Sc[k] = 0;
-      if (i < B && i != r && i != s) {
-        R[k] = ops.get(r, i);
-        S[k] = ops.get(s, i);
-        Rc[k] = ops.get_t(r, i);
-        Sc[k] = ops.get_t(s, i);
-      }
+  auto nload = [&](int i) {
+    nR = nS = nRc = nSc = ndi = ndn = 0;
+    if (i < B && i != r && i != s) {
+      nR = ops.get(r, i);
+      nS = ops.get(s, i);
+      nRc = ops.get_t(r, i);
+      nSc = ops.get_t(s, i);
+      ndi = LDT::ld(din_p + i);
+      ndn = LDT::ld(dout_p + i);
     }
-    int di[kRefK], dn[kRefK];
-#pragma unroll
-    for (int k = 0; k < kRefK; k++) {
-      const int i = base + k * G + g.gl;
-      // v's edges towards block i are part of M[r,i] (out) and M[i,r] (in)
-      if (R[k] > 0) {
-        const int w = table_lookup_wo(key, two, cap, lg, i);
-        R[k] -= w;
-        S[k] += w;
-      }
-      if (Rc[k] > 0) {
-        const int w = table_lookup_wo(key, twi, cap, lg, i);
-        Rc[k] -= w;
-        Sc[k] += w;
-      }
-      di[k] = (R[k] | S[k]) ? LDT::ld(din_p + i) : 0;
-      dn[k] = (Rc[k] | Sc[k]) ? LDT::ld(dout_p + i) : 0;
+  };
+  nload(g.gl);
+  for (int base = 0; base < B; base += G) {
+    int R = nR, S = nS, Rc = nRc, Sc = nSc;
+    const int di = ndi, dn = ndn;
+    nload(base + G + g.gl);
+    const int i = base + g.gl;
+    // v's edges towards block i are part of M[r,i] (out) and M[i,r] (in)
+    if (R > 0) {
+      const int w = table_lookup_wo(key, two, cap, lg, i);
+      R -= w;
+      S += w;
     }
-#pragma unroll
-    for (int k = 0; k < kRefK; k++) {
-      if (!g.any((R[k] | S[k] | Rc[k] | Sc[k]) != 0)) continue;
-      const float u0 = R[k] ? ref_term(R[k], static_cast<long long>(di[k]) * dor_n) : 0.0f;
-      const float u1 = S[k] ? ref_term(S[k], static_cast<long long>(di[k]) * dos_n) : 0.0f;
-      const float u2 = Rc[k] ? ref_term(Rc[k], static_cast<long long>(dn[k]) * dir_n) : 0.0f;
-      const float u3 = Sc[k] ? ref_term(Sc[k], static_cast<long long>(dn[k]) * dis_n) : 0.0f;
-      dS = ref32_accumulate<G>(g, dS, u0, u1, u2, u3, true, buf);
+    if (Rc > 0) {
+      const int w = table_lookup_wo(key, twi, cap, lg, i);
+      Rc -= w;
+      Sc += w;
     }
+    if (!g.any((R | S | Rc | Sc) != 0)) continue;
+    const float u0 = R ? ref_term(R, static_cast<long long>(di) * dor_n) : 0.0f;
+    const float u1 = S ? ref_term(S, static_cast<long long>(di) * dos_n) : 0.0f;
+    const float u2 = Rc ? ref_term(Rc, static_cast<long long>(dn) * dir_n) : 0.0f;
+    const float u3 = Sc ? ref_term(Sc, static_cast<long long>(dn) * dis_n) : 0.0f;
+    dS = ref32_accumulate<G>(g, dS, u0, u1, u2, u3, true, buf);
   }
   return dS;
 }

@@ -257,6 +257,45 @@ __device__ __forceinline__ float ref_logf(float x) {
   return __double2float_rn(__dadd_rn(hi, l1p));
 }
 
+// ref_logf for x > 0 (+inf included) without branches: the same operations
+// on the same values, the special cases chosen by selects, so that several
+// evaluations can be interleaved by the compiler.
+__device__ __forceinline__ float ref_logf_pos(float x) {
+  const unsigned u = __float_as_uint(x);
+  int e = static_cast<int>(u >> 23);
+  unsigned frac = u & 0x7fffffu;
+  const bool sub = e == 0;   // subnormal: shift the leading one into the hidden bit
+  const int sh = sub ? __clz(static_cast<int>(frac)) - 8 : 0;
+  frac = (frac << sh) & 0x7fffffu;
+  e = (sub ? 1 - sh : e) - 127;
+  const bool half = frac >= 0x3504F4u;
+  e += half ? 1 : 0;
+  const unsigned long long mbits = ((half ? 1022ull : 1023ull) << 52) | (static_cast<unsigned long long>(frac) << 29);
+  const int k = half ? static_cast<int>((frac + 0x10000u) >> 17) - 64 : static_cast<int>((frac + 0x8000u) >> 16);
+  const double m = __longlong_as_double(static_cast<long long>(mbits));
+  const double2 t = __ldg(kRefLogTab + kRefLogK0 + (u >= 0x7f800000u ? 0 : k));
+  const double w = __dsub_rn(__dmul_rn(m, t.x), 1.0);
+  double q = -1.0 / 8.0;
+  q = __fma_rn(q, w, 1.0 / 7.0);
+  q = __fma_rn(q, w, -1.0 / 6.0);
+  q = __fma_rn(q, w, 1.0 / 5.0);
+  q = __fma_rn(q, w, -1.0 / 4.0);
+  q = __fma_rn(q, w, 1.0 / 3.0);
+  q = __fma_rn(q, w, -1.0 / 2.0);
+  const double l1p = __fma_rn(__dmul_rn(w, w), q, w);
+  const double ed = __dsub_rn(__longlong_as_double(0x4338000000000000ll + e), 6755399441055744.0);
+  const double hi = __fma_rn(ed, 0.69314718055994530942, t.y);
+  const float r = __double2float_rn(__dadd_rn(hi, l1p));
+  return u >= 0x7f800000u ? x : r;   // +inf
+}
+
+// ref_term(x, prod) where x != 0, else 0, without branches (x, prod >= 0)
+__device__ __forceinline__ float ref_term_nz(int x, long long prod) {
+  const float xf = __int2float_rn(x ? x : 1);
+  const float t = __fmul_rn(xf, ref_logf_pos(__fdiv_rn(xf, __ll2float_rn(x ? prod : 1))));
+  return x ? t : 0.0f;
+}
+
 // one term of the reference's dS: count * log((float)count / (float)prod),
 // the long product converted to float, a float division, a float product
 __device__ __forceinline__ float ref_term(int x, long long prod) {

@@ -570,10 +570,10 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
       const int R = nR, S = nS, Rc = nRc, Sc = nSc, di = ndi, dn = ndn;
       oload(base + G + g.gl);
       if (!g.any((R | S | Rc | Sc) != 0)) continue;
-      const float t0 = R ? ref_term(R, static_cast<long long>(di) * dr_out) : 0.0f;
-      const float t1 = S ? ref_term(S, static_cast<long long>(di) * ds_out) : 0.0f;
-      const float t2 = Rc ? ref_term(Rc, static_cast<long long>(dn) * dr_in) : 0.0f;
-      const float t3 = Sc ? ref_term(Sc, static_cast<long long>(dn) * ds_in) : 0.0f;
+      const float t0 = ref_term_nz(R, static_cast<long long>(di) * dr_out);
+      const float t1 = ref_term_nz(S, static_cast<long long>(di) * ds_out);
+      const float t2 = ref_term_nz(Rc, static_cast<long long>(dn) * dr_in);
+      const float t3 = ref_term_nz(Sc, static_cast<long long>(dn) * ds_in);
       dS = ref32_accumulate<G>(g, dS, t0, t1, t2, t3, false, buf);
     }
   }
@@ -613,10 +613,12 @@ __device__ __noinline__ float ref32_nodal(const Ops ops, const int32_t* __restri
       Sc += w;
     }
     if (!g.any((R | S | Rc | Sc) != 0)) continue;
-    const float u0 = R ? ref_term(R, static_cast<long long>(di) * dor_n) : 0.0f;
-    const float u1 = S ? ref_term(S, static_cast<long long>(di) * dos_n) : 0.0f;
-    const float u2 = Rc ? ref_term(Rc, static_cast<long long>(dn) * dir_n) : 0.0f;
-    const float u3 = Sc ? ref_term(Sc, static_cast<long long>(dn) * dis_n) : 0.0f;
+    // (all four evaluated, the empty ones discarded: no branches, so the
+    // four evaluations overlap)
+    const float u0 = ref_term_nz(R, static_cast<long long>(di) * dor_n);
+    const float u1 = ref_term_nz(S, static_cast<long long>(di) * dos_n);
+    const float u2 = ref_term_nz(Rc, static_cast<long long>(dn) * dir_n);
+    const float u3 = ref_term_nz(Sc, static_cast<long long>(dn) * dis_n);
     dS = ref32_accumulate<G>(g, dS, u0, u1, u2, u3, true, buf);
   }
   return dS;

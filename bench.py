@@ -22,9 +22,11 @@ e2e    the same metric through the one-shot C ABI call usap_partition with
 roofline  the persistent nodal-phase kernel (k_nodal_phase: one launch per
        stage runs every sweep's entropy pass, proposals and apply), the
        dominant kernel: algorithmic bytes (per proposing vertex
-       8 + 8 deg + 48 |distinct neighbour blocks| + 48 + 8 * sampled
-       entries, plus 48 B for the float dS's reads of rows and columns r, s
-       of M and the degrees, twice; per entropy pass 4 B^2 + 8 nnz(M); per edge of a moved
+       8 + 8 deg + 48 + 8 * sampled entries, plus 48 B for the float dS's
+       reads of rows and columns r, s of M and the degrees, twice, and
+       48 |distinct neighbour blocks| where the exact FP64 value is also
+       evaluated (hubs; every vertex with the FP64 shadow on); per entropy
+       pass 4 B^2 + 8 nnz(M); per edge of a moved
        vertex 24) over its CUDA-event time, against the measured copy
        bandwidth of this B200 pool;
 cpu_baseline  the reference's own partition() (compiled from its sources

@@ -501,7 +501,7 @@ __device__ __forceinline__ float ref32_accumulate(const Grp<G>& g, float dS, flo
                                                   float t3, bool sub, float* buf) {
   reinterpret_cast<float4*>(buf)[g.gl] = make_float4(t0, t1, t2, t3);
   g.sync();
-#pragma unroll 4
+#pragma unroll 8
   for (int j = 0; j < G; j++) {
     const float4 q = reinterpret_cast<const float4*>(buf)[j];
     if (sub) dS = __fsub_rn(__fsub_rn(__fsub_rn(__fsub_rn(dS, q.x), q.y), q.z), q.w);

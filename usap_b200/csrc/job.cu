@@ -776,10 +776,10 @@ float Job::nodal_phase(int32_t* part, int32_t B, uint32_t stage, uint64_t seed, 
   pa.bar_hold = bar_test_hold_;
   bar_test_hold_ = -1;   // one launch only
   bar_test_timeout_ns_ = 0;
-  // precision mode 3: the old-state term tables of the single-job kernel
-  // (B <= kRefTabMaxB; above it the per-cell tables cost more than the
-  // proposals' own evaluation)
-  if (prec_ == 3 && !(gang_ && !timed) && B <= kRefTabMaxB) {
+  // precision mode 3: the old-state term tables of the persistent kernels,
+  // single-job and gang (B <= kRefTabMaxB; above it the per-cell tables
+  // cost more than the proposals' own evaluation)
+  if (prec_ == 3 && B <= kRefTabMaxB) {
     const size_t cells = static_cast<size_t>(ld_) * ld_;
     if (cells > tcap_) {
       dfree(Trow_);

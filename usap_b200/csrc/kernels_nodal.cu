@@ -2153,6 +2153,36 @@ __global__ void __launch_bounds__(kPThreads, 1) k_nodal_gang(const PhaseArgs* __
       }
     }
     if (leaving) break;
+    if constexpr (P == 3) {
+      // precision 3: the old-state term tables of every unfinished job's
+      // batch (as the single-job kernel's ref32_tables_pass), before anyone
+      // proposes
+      {
+        long long cells = 0;
+        if (mine && jobs[threadIdx.x].a.Trow) cells = static_cast<long long>(jobs[threadIdx.x].a.B) * jobs[threadIdx.x].a.tld;
+        job_prefix(cells, s_tmp, s_cp);
+      }
+      const long long total = s_cp[K];
+      if (total > 0) {
+        for (long long c = static_cast<long long>(blockIdx.x) * kPThreads + threadIdx.x; c < total;
+             c += static_cast<long long>(gridDim.x) * kPThreads) {
+          const int j = find_job(s_cp, K, c);
+          const PhaseArgs& p = jobs[j];
+          const long long cc = c - s_cp[j];
+          const int ld = p.a.tld, B = p.a.B;
+          const int b = static_cast<int>(cc / ld), i = static_cast<int>(cc - static_cast<long long>(b) * ld);
+          float tr = 0.0f, tc = 0.0f;
+          if (i < B) {
+            const int x = __ldcg(p.v.M + cc), y = __ldcg(p.v.Mt + cc);
+            if (x) tr = ref_term(x, static_cast<long long>(__ldcg(p.din + i)) * __ldcg(p.dout + b));
+            if (y) tc = ref_term(y, static_cast<long long>(__ldcg(p.dout + i)) * __ldcg(p.din + b));
+          }
+          __stcg(p.a.Trow + cc, tr);
+          __stcg(p.a.Tcol + cc, tc);
+        }
+        if (grid_barrier(gc, &target, false, &s_state) < 0) return;
+      }
+    }
     // proposals of every unfinished job's current batch
     if (threadIdx.x < K) {
       s_tally[threadIdx.x] = CtaTally{0, 0, 0, 0};
